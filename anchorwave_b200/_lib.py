@@ -1,0 +1,92 @@
+"""ctypes binding of libaw_b200.so (the C ABI declared in include/anchorwave_b200.h).
+
+There is no fallback: if the shared library is missing or cannot be loaded, importing
+this module raises, so no caller can silently run a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaw_b200.so")
+
+
+class KswExtz(C.Structure):
+    """ksw_extz_t (minimap2/ksw2.h:40-50); identical layout in include/anchorwave_b200.h."""
+    _fields_ = [("max", C.c_uint32, 31), ("zdropped", C.c_uint32, 1),
+                ("max_q", C.c_int), ("max_t", C.c_int), ("mqe", C.c_int), ("mqe_t", C.c_int),
+                ("mte", C.c_int), ("mte_q", C.c_int), ("score", C.c_int),
+                ("m_cigar", C.c_int), ("n_cigar", C.c_int), ("reach_end", C.c_int),
+                ("stopped", C.c_int), ("cigar", C.POINTER(C.c_uint32))]
+
+
+# Every symbol the header declares; tests check that the library exports each one.
+EXPORTS = [
+    "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "aw_ksw_extd2_batch",
+    "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
+    "aw_ksw_plan_stats", "aw_ksw_plan_dp_ms", "aw_ksw_plan_free",
+    "aw_set_traceback_budget", "aw_set_tuning", "aw_last_error", "aw_device_count",
+    "aw_int32_peak_ops",
+]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m anchorwave_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    vp, i8, i32, i64 = C.c_void_p, C.c_int8, C.c_int, C.c_int64
+    ksw_args = [vp, i32, vp, i32, vp, i8, vp, i8, i8, i8, i8, i32, i32, i32, i32, C.POINTER(KswExtz)]
+    lib.ksw_extd2_gpu.argtypes = ksw_args
+    lib.ksw_extd2_gpu.restype = None
+    lib.ksw_extd2_singletrack_gpu.argtypes = ksw_args
+    lib.ksw_extd2_singletrack_gpu.restype = None
+    lib.aw_ksw_extd2_batch.argtypes = [i32, vp, vp, vp, vp, vp, i8, vp, i8, i8, i8, i8, i32, i32, i32, vp]
+    lib.aw_ksw_extd2_batch.restype = i32
+    lib.aw_ksw_plan_new.argtypes = [i32, vp, vp, vp, i8, vp, i8, i8, i8, i8, i32, i32, i32]
+    lib.aw_ksw_plan_new.restype = vp
+    lib.aw_ksw_plan_upload.argtypes = [vp, vp, vp]
+    lib.aw_ksw_plan_upload.restype = i32
+    lib.aw_ksw_plan_execute.argtypes = [vp, C.POINTER(C.c_float)]
+    lib.aw_ksw_plan_execute.restype = i32
+    lib.aw_ksw_plan_download.argtypes = [vp, vp]
+    lib.aw_ksw_plan_download.restype = i32
+    lib.aw_ksw_plan_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]
+    lib.aw_ksw_plan_stats.restype = i32
+    lib.aw_ksw_plan_dp_ms.argtypes = [vp]
+    lib.aw_ksw_plan_dp_ms.restype = C.c_float
+    lib.aw_ksw_plan_free.argtypes = [vp]
+    lib.aw_ksw_plan_free.restype = None
+    lib.aw_set_traceback_budget.argtypes = [i64]
+    lib.aw_set_traceback_budget.restype = None
+    lib.aw_set_tuning.argtypes = [i32, i32]
+    lib.aw_set_tuning.restype = None
+    lib.aw_last_error.argtypes = []
+    lib.aw_last_error.restype = C.c_char_p
+    lib.aw_device_count.argtypes = []
+    lib.aw_device_count.restype = i32
+    lib.aw_int32_peak_ops.argtypes = []
+    lib.aw_int32_peak_ops.restype = C.c_double
+    for name in EXPORTS:
+        getattr(lib, name)  # raises AttributeError if a declared symbol is missing
+    return lib
+
+
+lib = _load()
+libc = C.CDLL(None)
+libc.free.argtypes = [C.c_void_p]
+libc.free.restype = None
+
+
+def last_error() -> str:
+    msg = lib.aw_last_error()
+    return msg.decode() if msg else ""
+
+
+class AwError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        raise AwError(f"{what} failed ({rc}): {last_error()}")

@@ -1,0 +1,113 @@
+// Internal types shared by the KSW2 / WFA kernels and the C-ABI host layer.
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#define AW_NEG_INF (-0x40000000)
+#define AW_E_CUDA_INTERNAL (-2)
+#define AW_E_NOMEM_INTERNAL (-3)
+
+// Flags of ksw_extd2 (minimap2/ksw2.h:20-34).
+#define AW_EZ_SCORE_ONLY     0x01
+#define AW_EZ_RIGHT          0x02
+#define AW_EZ_GENERIC_SC     0x04
+#define AW_EZ_APPROX_MAX     0x08
+#define AW_EZ_APPROX_DROP    0x10
+#define AW_EZ_EXTZ_ONLY      0x40
+#define AW_EZ_REV_CIGAR      0x80
+#define AW_EZ_SPLICE_MASK    0x700
+#define AW_EZ_SEMIGLOBAL_END 0x800
+#define AW_EZ_SINGLETRACK    0x1000
+
+namespace aw {
+
+// Per-launch scoring constants, after the q+e <= q2+e2 swap of
+// minimap2/ksw2_extd2_sse.c:83.
+struct KswScore {
+    int q, e, q2, e2;
+    int qe, qe2;
+    int qe_pre;               // q+e of the caller's argument order: seeds H (ksw2_extd2_sse.c:73, :367)
+    int mch;                  // mat[0], the clamp of ksw2_extd2_sse.c:252
+    int long_thres, long_diff;  // ksw2_extd2_sse.c:107-110
+    uint32_t tab_lo[8];       // score row per target code: bytes for query codes 0..3
+    uint32_t tab_hi[8];       //                             bytes for query codes 4..7
+};
+
+// One pair of the batch as the kernels see it.
+struct KswPair {
+    int64_t qoff, toff;   // byte offsets of the 0..m-1 codes in the sequence arenas
+    int64_t tb_off;       // byte offset of this pair's traceback (CIGAR modes)
+    int64_t bnd_off;      // word offset of this pair's strip-boundary columns
+    int64_t cig_off;      // word offset of this pair's CIGAR slot (capacity qlen+tlen)
+    int32_t qlen, tlen;
+};
+
+// Scalar ksw_extz_t fields produced on the device (minimap2/ksw2.h:40-50).
+struct KswOut {
+    int32_t score, max, max_q, max_t, mqe, mqe_t, mte, mte_q;
+    int32_t n_cigar, zdropped, reach_end, stopped;
+};
+
+struct KswFullArgs {
+    const uint8_t *qcodes, *tcodes;
+    const KswPair *pairs;
+    const int32_t *order;     // processing order (largest first)
+    int32_t n;
+    uint8_t *tb;              // traceback arena (CIGAR modes)
+    uint32_t *bnd;            // strip-boundary arena
+    KswOut *out;
+    int32_t *queue;           // work-queue head (device counter)
+    int32_t *error;           // set non-zero if a bounded wait gave up
+    KswScore sc;
+};
+
+// Traceback geometry of the strip kernel: 32 lanes x KSW_COLS target columns per
+// strip; one byte per cell at  ((strip * (qlen + 31) + step) * 32 + lane) * KSW_COLS + col
+// where step = row + lane (the lane skew).
+constexpr int KSW_COLS = 8;
+constexpr int KSW_STRIP = 32 * KSW_COLS;
+
+inline int64_t ksw_full_tb_bytes(int qlen, int tlen) {
+    const int64_t nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
+    return nstrip * (int64_t)(qlen + 31) * KSW_STRIP;
+}
+inline int64_t ksw_full_bnd_words(int qlen, int tlen) {
+    const int64_t nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
+    return nstrip * (int64_t)qlen;
+}
+
+// Grow-only device allocation (pooled per host thread or per plan).
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = n < 4096 ? 4096 : n;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr, cap = 0;
+    }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+void set_error(const char *msg);
+
+// Launchers (ksw2_full.cu).
+int ksw_full_occupancy(int flag, int warps_per_pair, int groups_per_cta);
+cudaError_t launch_ksw_full(const KswFullArgs &a, int flag, int warps_per_pair,
+                            int groups_per_cta, int ctas, cudaStream_t st);
+cudaError_t launch_ksw_backtrack_full(const KswPair *pairs, const int32_t *order, int n,
+                                      const uint8_t *tb, KswOut *out, uint32_t *cig,
+                                      int flag, cudaStream_t st);
+cudaError_t launch_ksw_pack_cigar(const KswPair *pairs, int n, const KswOut *out,
+                                  const uint32_t *cig, const int64_t *packed_off,
+                                  uint32_t *packed, cudaStream_t st);
+
+}  // namespace aw

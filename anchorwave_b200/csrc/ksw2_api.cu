@@ -1,0 +1,694 @@
+// C-ABI host layer for the KSW2 kernels (drop-in ksw_extd2 entries, batch and
+// plan APIs).  Host-side responsibilities:
+//   * the argument checks and early returns of ksw_extd2 (minimap2/ksw2_extd2_sse.c:80-105,
+//     ksw2_extd2_avx.c:129-133), done before any device work;
+//   * routing each pair to the full-matrix strip kernel or to the exact
+//     anti-diagonal kernel (banded / Singletrack / z-drop / other flags);
+//   * batch planning: pairs sorted largest first, traceback arenas packed into
+//     waves under an HBM budget (the -M admission envelope of
+//     AlignmentResourceScheduler.cpp:706 restated for device memory);
+//   * per-thread pooled device/pinned buffers (grow-only) and a private stream
+//     pair, so concurrent host threads never share state (the reference's
+//     one-call-per-worker threading contract, SURVEY boundary table);
+//   * CIGAR ownership exactly as ksw_push_cigar (minimap2/ksw2.h:144-154).
+#include "aw_internal.h"
+#include "ksw2_exact.h"
+#include "../../include/anchorwave_b200.h"
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <dlfcn.h>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace aw {
+
+// ---- diagnostics -----------------------------------------------------------
+static thread_local std::string tls_err;
+void set_error(const char *s) {
+    tls_err = s;
+    if (getenv("AW_VERBOSE")) fprintf(stderr, "[aw_b200] %s\n", s);
+}
+static void set_error(const std::string &s) { set_error(s.c_str()); }
+#define AW_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t _e = (call);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(_e));              \
+            return AW_E_CUDA;                                                           \
+        }                                                                               \
+    } while (0)
+
+// ---- tuning ----------------------------------------------------------------
+static int64_t g_tb_budget = 0;           // 0 = 60% of free memory
+static int g_large_warps = 8;
+static int g_large_tlen = 4096;
+static std::mutex g_cfg_mu;
+
+// ---- pooled buffers ----------------------------------------------------------
+struct PinBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max(n + n / 2, (size_t)4096);
+        cudaError_t e = cudaMallocHost(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr, cap = 0;
+    }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+struct Buffers {
+    DevBuf qcodes, tcodes, pairs, order, out, cig, packed, packed_off, tb, bnd, queue, error;
+    DevBuf exact_ws;
+    PinBuf h_codes, h_pairs, h_order, h_out, h_packed, h_packed_off, h_small;
+    cudaStream_t st = nullptr, st2 = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    std::vector<cudaEvent_t> ev_k;  // per-launch timing events
+    int device = -1;
+    int sms = 0;
+    ~Buffers() {
+        qcodes.release(); tcodes.release(); pairs.release(); order.release(); out.release();
+        cig.release(); packed.release(); packed_off.release(); tb.release(); bnd.release();
+        queue.release(); error.release(); exact_ws.release();
+        h_codes.release(); h_pairs.release(); h_order.release(); h_out.release();
+        h_packed.release(); h_packed_off.release(); h_small.release();
+        for (auto e : ev_k) cudaEventDestroy(e);
+        if (ev_a) cudaEventDestroy(ev_a);
+        if (ev_b) cudaEventDestroy(ev_b);
+        if (ev_t0) cudaEventDestroy(ev_t0);
+        if (ev_t1) cudaEventDestroy(ev_t1);
+        if (st) cudaStreamDestroy(st);
+        if (st2) cudaStreamDestroy(st2);
+    }
+    int init() {
+        if (st) return AW_OK;
+        AW_CUDA(cudaGetDevice(&device));
+        AW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        AW_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        AW_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        AW_CUDA(cudaEventCreateWithFlags(&ev_a, cudaEventDisableTiming));
+        AW_CUDA(cudaEventCreateWithFlags(&ev_b, cudaEventDisableTiming));
+        AW_CUDA(cudaEventCreate(&ev_t0));
+        AW_CUDA(cudaEventCreate(&ev_t1));
+        return AW_OK;
+    }
+};
+
+static thread_local Buffers *tls_buf = nullptr;
+static Buffers *thread_buffers() {
+    if (!tls_buf) {
+        tls_buf = new Buffers();
+        // released when the thread exits
+        static thread_local struct Reaper {
+            ~Reaper() { delete tls_buf; tls_buf = nullptr; }
+        } reaper;
+        (void)reaper;
+    }
+    return tls_buf;
+}
+
+// ---- per-pair routing ----------------------------------------------------------
+struct Params {
+    int8_t m;
+    int8_t mat[64];
+    int q, e, q2, e2;   // after the swap
+    int zdrop, end_bonus, flag;
+    int min_sc, max_sc;
+    int qe_pre;         // q+e before the swap
+    bool early_return;  // -min_sc > 2(q+e): ksw2_extd2_sse.c:105
+};
+
+static bool make_params(int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2,
+                        int zdrop, int end_bonus, int flag, Params &P) {
+    if (m < 2 || m > 8) return false;
+    P.m = m;
+    memset(P.mat, 0, sizeof(P.mat));
+    memcpy(P.mat, mat, (size_t)m * m);
+    int qq = q, ee = e, qq2 = q2, ee2 = e2;
+    P.qe_pre = q + e;
+    if (qq2 + ee2 < qq + ee) std::swap(qq, qq2), std::swap(ee, ee2);
+    P.q = qq, P.e = ee, P.q2 = qq2, P.e2 = ee2;
+    P.zdrop = zdrop, P.end_bonus = end_bonus, P.flag = flag;
+    P.max_sc = mat[0], P.min_sc = mat[1];
+    for (int t = 1; t < m * m; ++t) P.max_sc = std::max<int>(P.max_sc, mat[t]), P.min_sc = std::min<int>(P.min_sc, mat[t]);
+    P.early_return = -P.min_sc > 2 * (P.q + P.e);
+    return true;
+}
+
+static KswScore make_score(const Params &P) {
+    KswScore S;
+    S.q = P.q, S.e = P.e, S.q2 = P.q2, S.e2 = P.e2;
+    S.qe = P.q + P.e, S.qe2 = P.q2 + P.e2;
+    S.qe_pre = P.qe_pre;
+    S.mch = P.mat[0];
+    int lt = P.e != P.e2 ? (P.q2 - P.q) / (P.e - P.e2) - 1 : 0;
+    if (P.q2 + P.e2 + lt * P.e2 > P.q + P.e + lt * P.e) ++lt;
+    S.long_thres = lt;
+    S.long_diff = lt * (P.e - P.e2) - (P.q2 - P.q) - P.e2;
+    const int m = P.m;
+    const int8_t scN = P.mat[m * m - 1] == 0 ? (int8_t)(-P.e2) : P.mat[m * m - 1];
+    for (int tc = 0; tc < 8; ++tc) {
+        uint8_t row[8];
+        for (int qc = 0; qc < 8; ++qc) {
+            int8_t v;
+            if (P.flag & AW_EZ_GENERIC_SC)
+                v = (tc < m && qc < m) ? P.mat[tc * m + qc] : 0;
+            else {
+                v = tc == qc ? P.mat[0] : P.mat[1];
+                if (tc == m - 1 || qc == m - 1) v = scN;
+            }
+            row[qc] = (uint8_t)v;
+        }
+        memcpy(&S.tab_lo[tc], row, 4);
+        memcpy(&S.tab_hi[tc], row + 4, 4);
+    }
+    return S;
+}
+
+// The strip kernel computes in 32-bit registers.  It is exact when the int8
+// intermediates of the reference never wrap and when none of the features it
+// omits (band, z-drop, max tracking, Singletrack, approximate max, extension
+// end) is requested.  The magnitude bound below keeps every intermediate of
+// the recurrence (a, b, a2, b2 before and after the z adjustment, u, v, x,
+// y, x2, y2) inside int8 for the invariant ranges x,y in [-(q+e),-e],
+// x2,y2 in [-(q2+e2),-e2], u,v in [-(q+e), mch+(q+e)].
+static bool full_path_ok(const Params &P, int qlen, int tlen, int w) {
+    if (exact_stop_enabled()) return false;
+    const int allowed = AW_EZ_SCORE_ONLY | AW_EZ_RIGHT | AW_EZ_GENERIC_SC | AW_EZ_REV_CIGAR |
+                        AW_EZ_SEMIGLOBAL_END;
+    if (P.flag & ~allowed) return false;
+    if (!(w < 0 || w >= std::max(qlen, tlen))) return false;
+    if (P.zdrop >= 0) return false;
+    if (P.max_sc > 0 || P.mat[0] < P.max_sc) return false;
+    if (P.q < 0 || P.e < 0 || P.q2 < 0 || P.e2 < 0) return false;
+    if (P.e2 > P.e || P.q2 < P.q) return false;
+    const int mag = (P.q2 + P.e2) + (P.q + P.e) + std::abs(P.min_sc) + std::abs((int)P.mat[0]);
+    if (mag > 100) return false;
+    const int64_t nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
+    if (nstrip * (int64_t)(qlen + 1) + qlen > INT_MAX / 2) return false;
+    return true;
+}
+
+static void reset_extz(ksw_extz_t *ez) {  // minimap2/ksw2.h:194-199
+    ez->max_q = ez->max_t = ez->mqe_t = ez->mte_q = -1;
+    ez->max = 0, ez->score = ez->mqe = ez->mte = AW_NEG_INF;
+    ez->n_cigar = 0, ez->zdropped = 0, ez->reach_end = 0, ez->stopped = 0;
+}
+
+// ---- CIGAR ownership ------------------------------------------------------------
+typedef void *(*krealloc_fn)(void *, void *, size_t);
+static krealloc_fn find_krealloc() {
+    static krealloc_fn fn = (krealloc_fn)dlsym(RTLD_DEFAULT, "krealloc");
+    return fn;
+}
+
+// Store n words into ez->cigar with the capacity growth ksw_push_cigar would have
+// produced (m_cigar doubles from its entry value, starting at 4).
+static bool store_cigar(void *km, ksw_extz_t *ez, const uint32_t *words, int n) {
+    ez->n_cigar = n;
+    if (n == 0) return true;
+    int m = ez->m_cigar;
+    if (n > m) {
+        int mm = m;
+        while (mm < n) mm = mm ? mm << 1 : 4;
+        void *p;
+        if (km) {
+            krealloc_fn kr = find_krealloc();
+            if (!kr) {
+                set_error("km != NULL but no krealloc symbol in the process");
+                ez->n_cigar = 0;
+                return false;
+            }
+            p = kr(km, ez->cigar, (size_t)mm << 2);
+        } else {
+            p = realloc(ez->cigar, (size_t)mm << 2);
+        }
+        if (!p) {
+            ez->n_cigar = 0;
+            return false;
+        }
+        ez->cigar = (uint32_t *)p;
+        ez->m_cigar = mm;
+    }
+    memcpy(ez->cigar, words, (size_t)n * 4);
+    return true;
+}
+
+}  // namespace aw
+
+using namespace aw;
+
+// ---- plan ----------------------------------------------------------------------------
+struct aw_ksw_plan {
+    Buffers own;              // used when the plan owns its buffers
+    Buffers *B = nullptr;     // buffers in use (own or the thread's pool)
+    Params P;
+    KswScore S;
+    int n = 0;
+    std::vector<int> qlen, tlen, w;
+    std::vector<int> route;   // 0 = no device work (early return), 1 = strip kernel, 2 = exact kernel
+    std::vector<int> early_zdrop;
+    std::vector<KswPair> pairs;
+    std::vector<int64_t> qoff, toff;
+    int64_t qbytes = 0, tbytes = 0, cig_words = 0;
+    // waves of strip-kernel pairs: order array segments
+    struct Wave {
+        int begin_small, n_small, begin_large, n_large;  // ranges in order[]
+        int64_t tb_bytes, bnd_words;
+    };
+    std::vector<Wave> waves;
+    std::vector<int32_t> order;      // strip-kernel processing order, wave by wave
+    std::vector<int32_t> exact_ids;  // pairs for the exact kernel
+    int64_t tb_cap = 0, bnd_cap = 0;
+    int64_t cells = 0, tb_total = 0;
+    int launches = 0;
+    bool uploaded = false, executed = false;
+    float dp_ms_mean = 0.f;
+    int dp_launches = 0;
+};
+
+static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen, const int *w) {
+    pl->n = n;
+    pl->qlen.assign(qlen, qlen + n);
+    pl->tlen.assign(tlen, tlen + n);
+    pl->w.assign(n, -1);
+    if (w) pl->w.assign(w, w + n);
+    pl->route.assign(n, 0);
+    pl->early_zdrop.assign(n, 0);
+    pl->pairs.resize(n);
+    pl->qoff.resize(n);
+    pl->toff.resize(n);
+    const Params &P = pl->P;
+    int64_t qb = 0, tbt = 0, cw = 0;
+    for (int i = 0; i < n; ++i) {
+        const int ql = pl->qlen[i], tl = pl->tlen[i];
+        pl->qoff[i] = qb, pl->toff[i] = tbt;
+        if (ql > 0) qb += ql;
+        if (tl > 0) tbt += tl;
+        // ksw2_extd2_sse.c:81 / ksw2_extd2_avx.c:129-133 / :105
+        if (P.m <= 1 || ql <= 0 || tl <= 0) continue;
+        if (ql > INT_MAX - tl + 1) { pl->early_zdrop[i] = 1; continue; }
+        if (P.early_return) continue;
+        pl->route[i] = full_path_ok(P, ql, tl, pl->w[i]) ? 1 : 2;
+        KswPair &kp = pl->pairs[i];
+        kp.qoff = pl->qoff[i], kp.toff = pl->toff[i];
+        kp.qlen = ql, kp.tlen = tl;
+        kp.cig_off = cw;
+        kp.tb_off = 0, kp.bnd_off = 0;
+        cw += (int64_t)ql + tl + 2;
+        pl->cells += (int64_t)ql * tl;
+    }
+    pl->qbytes = qb, pl->tbytes = tbt, pl->cig_words = cw;
+    // strip-kernel pairs: largest first, packed into traceback waves
+    std::vector<int32_t> strip;
+    for (int i = 0; i < n; ++i)
+        if (pl->route[i] == 1) strip.push_back(i);
+        else if (pl->route[i] == 2) pl->exact_ids.push_back(i);
+    std::sort(strip.begin(), strip.end(), [&](int a, int b) {
+        const int64_t ca = (int64_t)pl->qlen[a] * pl->tlen[a], cb = (int64_t)pl->qlen[b] * pl->tlen[b];
+        return ca != cb ? ca > cb : a < b;
+    });
+    const bool cigar = !(P.flag & AW_EZ_SCORE_ONLY);
+    int64_t budget;
+    {
+        std::lock_guard<std::mutex> lk(g_cfg_mu);
+        budget = g_tb_budget;
+    }
+    if (budget <= 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = (size_t)16 << 30;
+        budget = (int64_t)(fr * 0.6);
+    }
+    // LPT multiway partition of traceback bytes into the fewest waves that fit
+    std::vector<std::vector<int32_t>> wv;
+    std::vector<int64_t> wload, wbnd;
+    for (int32_t i : strip) {
+        const int64_t tbb = cigar ? ksw_full_tb_bytes(pl->qlen[i], pl->tlen[i]) : 0;
+        const int64_t bw = ksw_full_bnd_words(pl->qlen[i], pl->tlen[i]);
+        pl->tb_total += tbb;
+        if (tbb > budget) {
+            set_error("pair traceback exceeds the HBM traceback budget");
+            return AW_E_NOMEM;
+        }
+        int best = -1;
+        for (size_t k = 0; k < wv.size(); ++k)
+            if (wload[k] + tbb <= budget && (best < 0 || wload[k] < wload[best])) best = (int)k;
+        if (best < 0) {
+            wv.emplace_back();
+            wload.push_back(0);
+            wbnd.push_back(0);
+            best = (int)wv.size() - 1;
+        }
+        KswPair &kp = pl->pairs[i];
+        kp.tb_off = wload[best];
+        kp.bnd_off = wbnd[best];
+        wload[best] += (tbb + 255) / 256 * 256;
+        wbnd[best] += (bw + 63) / 64 * 64;
+        wv[best].push_back(i);
+    }
+    int large_tlen, large_warps;
+    {
+        std::lock_guard<std::mutex> lk(g_cfg_mu);
+        large_tlen = g_large_tlen, large_warps = g_large_warps;
+    }
+    for (size_t k = 0; k < wv.size(); ++k) {
+        aw_ksw_plan::Wave W;
+        std::vector<int32_t> lg, sm;
+        for (int32_t i : wv[k]) (pl->tlen[i] >= large_tlen && large_warps > 1 ? lg : sm).push_back(i);
+        W.begin_large = (int)pl->order.size();
+        W.n_large = (int)lg.size();
+        pl->order.insert(pl->order.end(), lg.begin(), lg.end());
+        W.begin_small = (int)pl->order.size();
+        W.n_small = (int)sm.size();
+        pl->order.insert(pl->order.end(), sm.begin(), sm.end());
+        W.tb_bytes = wload[k];
+        W.bnd_words = wbnd[k];
+        pl->tb_cap = std::max(pl->tb_cap, W.tb_bytes);
+        pl->bnd_cap = std::max(pl->bnd_cap, W.bnd_words);
+        pl->waves.push_back(W);
+    }
+    pl->S = make_score(P);
+    return AW_OK;
+}
+
+static int plan_alloc(aw_ksw_plan_t *pl) {
+    Buffers *B = pl->B;
+    int rc = B->init();
+    if (rc) return rc;
+    const int n = pl->n;
+    AW_CUDA(B->qcodes.ensure(pl->qbytes + 16));
+    AW_CUDA(B->tcodes.ensure(pl->tbytes + 16));
+    AW_CUDA(B->pairs.ensure(sizeof(KswPair) * (size_t)std::max(n, 1)));
+    AW_CUDA(B->order.ensure(sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size() + 1)));
+    AW_CUDA(B->out.ensure(sizeof(KswOut) * (size_t)std::max(n, 1)));
+    AW_CUDA(B->cig.ensure(4 * (size_t)(pl->cig_words + 1)));
+    AW_CUDA(B->packed.ensure(4 * (size_t)(pl->cig_words + 1)));
+    AW_CUDA(B->packed_off.ensure(8 * (size_t)std::max(n, 1)));
+    AW_CUDA(B->tb.ensure((size_t)pl->tb_cap + 256));
+    AW_CUDA(B->bnd.ensure(4 * (size_t)pl->bnd_cap + 256));
+    AW_CUDA(B->queue.ensure(sizeof(int32_t) * 64 * (pl->waves.size() + 2)));
+    AW_CUDA(B->error.ensure(sizeof(int32_t) * 4));
+    AW_CUDA(B->h_pairs.ensure(sizeof(KswPair) * (size_t)std::max(n, 1)));
+    AW_CUDA(B->h_order.ensure(sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size() + 1)));
+    AW_CUDA(B->h_out.ensure(sizeof(KswOut) * (size_t)std::max(n, 1)));
+    AW_CUDA(B->h_packed_off.ensure(8 * (size_t)std::max(n, 1)));
+    return AW_OK;
+}
+
+static int plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uint8_t *const *target) {
+    Buffers *B = pl->B;
+    const int n = pl->n;
+    AW_CUDA(B->h_codes.ensure((size_t)(pl->qbytes + pl->tbytes) + 32));
+    uint8_t *hq = B->h_codes.as<uint8_t>(), *ht = hq + pl->qbytes + 16;
+    for (int i = 0; i < n; ++i) {
+        if (pl->qlen[i] > 0) memcpy(hq + pl->qoff[i], query[i], (size_t)pl->qlen[i]);
+        if (pl->tlen[i] > 0) memcpy(ht + pl->toff[i], target[i], (size_t)pl->tlen[i]);
+    }
+    memcpy(B->h_pairs.p, pl->pairs.data(), sizeof(KswPair) * (size_t)n);
+    int32_t *ho = B->h_order.as<int32_t>();
+    std::copy(pl->order.begin(), pl->order.end(), ho);
+    std::copy(pl->exact_ids.begin(), pl->exact_ids.end(), ho + pl->order.size());
+    AW_CUDA(cudaMemcpyAsync(B->qcodes.p, hq, (size_t)pl->qbytes, cudaMemcpyHostToDevice, B->st));
+    AW_CUDA(cudaMemcpyAsync(B->tcodes.p, ht, (size_t)pl->tbytes, cudaMemcpyHostToDevice, B->st));
+    AW_CUDA(cudaMemcpyAsync(B->pairs.p, B->h_pairs.p, sizeof(KswPair) * (size_t)n, cudaMemcpyHostToDevice, B->st));
+    AW_CUDA(cudaMemcpyAsync(B->order.p, ho, sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size()),
+                            cudaMemcpyHostToDevice, B->st));
+    pl->uploaded = true;
+    return AW_OK;
+}
+
+static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
+    Buffers *B = pl->B;
+    const Params &P = pl->P;
+    if (!pl->uploaded) { set_error("plan not uploaded"); return AW_E_INVAL; }
+    const size_t nq = 64 * (pl->waves.size() + 2);
+    int launches = 0;
+    AW_CUDA(cudaMemsetAsync(B->queue.p, 0, sizeof(int32_t) * nq, B->st));
+    AW_CUDA(cudaMemsetAsync(B->error.p, 0, sizeof(int32_t) * 4, B->st));
+    AW_CUDA(cudaMemsetAsync(B->out.p, 0, sizeof(KswOut) * (size_t)std::max(pl->n, 1), B->st));
+    AW_CUDA(cudaEventRecord(B->ev_t0, B->st));
+    int large_warps;
+    {
+        std::lock_guard<std::mutex> lk(g_cfg_mu);
+        large_warps = g_large_warps;
+    }
+    // per-launch timing events for the DP kernels
+    const size_t need_ev = 2 * (pl->waves.size() * 2 + 2);
+    while (B->ev_k.size() < need_ev) {
+        cudaEvent_t e;
+        AW_CUDA(cudaEventCreate(&e));
+        B->ev_k.push_back(e);
+    }
+    int dp_count = 0;
+    for (size_t k = 0; k < pl->waves.size(); ++k) {
+        const auto &W = pl->waves[k];
+        KswFullArgs a;
+        a.qcodes = B->qcodes.as<uint8_t>(), a.tcodes = B->tcodes.as<uint8_t>();
+        a.pairs = B->pairs.as<KswPair>(), a.out = B->out.as<KswOut>();
+        a.tb = B->tb.as<uint8_t>(), a.bnd = B->bnd.as<uint32_t>();
+        a.error = B->error.as<int32_t>();
+        a.sc = pl->S;
+        // fork: large pairs on st2 (groups of large_warps warps), small on st (single warps)
+        AW_CUDA(cudaEventRecord(B->ev_a, B->st));
+        AW_CUDA(cudaStreamWaitEvent(B->st2, B->ev_a, 0));
+        if (W.n_large > 0) {
+            a.order = B->order.as<int32_t>() + W.begin_large;
+            a.n = W.n_large;
+            a.queue = B->queue.as<int32_t>() + 64 * (2 * k);
+            const int groups = 8 / large_warps;
+            const int occ = std::max(1, ksw_full_occupancy(P.flag, large_warps, groups));
+            const int ctas = std::min(W.n_large / groups + 1, occ * B->sms);
+            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count], B->st2));
+            AW_CUDA(launch_ksw_full(a, P.flag, large_warps, groups, ctas, B->st2));
+            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count + 1], B->st2));
+            ++dp_count;
+            ++launches;
+        }
+        if (W.n_small > 0) {
+            a.order = B->order.as<int32_t>() + W.begin_small;
+            a.n = W.n_small;
+            a.queue = B->queue.as<int32_t>() + 64 * (2 * k + 1);
+            const int occ = std::max(1, ksw_full_occupancy(P.flag, 1, 8));
+            const int ctas = std::min((W.n_small + 7) / 8, occ * B->sms);
+            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count], B->st));
+            AW_CUDA(launch_ksw_full(a, P.flag, 1, 8, ctas, B->st));
+            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count + 1], B->st));
+            ++dp_count;
+            ++launches;
+        }
+        AW_CUDA(cudaEventRecord(B->ev_b, B->st2));
+        AW_CUDA(cudaStreamWaitEvent(B->st, B->ev_b, 0));
+        if (!(P.flag & AW_EZ_SCORE_ONLY) && W.n_large + W.n_small > 0) {
+            AW_CUDA(launch_ksw_backtrack_full(B->pairs.as<KswPair>(), B->order.as<int32_t>() + W.begin_large,
+                                              W.n_large + W.n_small, B->tb.as<uint8_t>(), B->out.as<KswOut>(),
+                                              B->cig.as<uint32_t>(), P.flag, B->st));
+            ++launches;
+        }
+    }
+    if (!pl->exact_ids.empty()) {
+        int rc = run_exact_ksw(pl->exact_ids.size(), B->order.as<int32_t>() + pl->order.size(),
+                               B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), B->pairs.as<KswPair>(),
+                               pl->pairs, pl->exact_ids, pl->w, P.m, P.mat, pl->S, P.zdrop, P.end_bonus,
+                               P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), B->exact_ws,
+                               B->st, &launches);
+        if (rc) return rc;
+    }
+    AW_CUDA(cudaEventRecord(B->ev_t1, B->st));
+    AW_CUDA(cudaStreamSynchronize(B->st));
+    int32_t err = 0;
+    AW_CUDA(cudaMemcpy(&err, B->error.p, 4, cudaMemcpyDeviceToHost));
+    if (err) { set_error("a bounded device wait gave up (pipeline stall)"); return AW_E_TIMEOUT; }
+    if (ms) AW_CUDA(cudaEventElapsedTime(ms, B->ev_t0, B->ev_t1));
+    float tot = 0.f;
+    for (int d = 0; d < dp_count; ++d) {
+        float t = 0.f;
+        AW_CUDA(cudaEventElapsedTime(&t, B->ev_k[2 * d], B->ev_k[2 * d + 1]));
+        tot += t;
+    }
+    pl->dp_ms_mean = dp_count ? tot / dp_count : 0.f;
+    pl->dp_launches = dp_count;
+    pl->launches = launches;
+    pl->executed = true;
+    return AW_OK;
+}
+
+static int plan_download(aw_ksw_plan_t *pl, ksw_extz_t *ez, void *km) {
+    Buffers *B = pl->B;
+    const int n = pl->n;
+    if (!pl->executed) { set_error("plan not executed"); return AW_E_INVAL; }
+    AW_CUDA(cudaMemcpyAsync(B->h_out.p, B->out.p, sizeof(KswOut) * (size_t)n, cudaMemcpyDeviceToHost, B->st));
+    AW_CUDA(cudaStreamSynchronize(B->st));
+    const KswOut *ho = B->h_out.as<KswOut>();
+    const bool cigar = !(pl->P.flag & AW_EZ_SCORE_ONLY);
+    int64_t total = 0;
+    int64_t *poff = B->h_packed_off.as<int64_t>();
+    for (int i = 0; i < n; ++i) {
+        poff[i] = total;
+        if (pl->route[i] && cigar) total += ho[i].n_cigar;
+    }
+    if (cigar && total > 0) {
+        AW_CUDA(cudaMemcpyAsync(B->packed_off.p, poff, 8 * (size_t)n, cudaMemcpyHostToDevice, B->st));
+        AW_CUDA(launch_ksw_pack_cigar(B->pairs.as<KswPair>(), n, B->out.as<KswOut>(), B->cig.as<uint32_t>(),
+                                      B->packed_off.as<int64_t>(), B->packed.as<uint32_t>(), B->st));
+        AW_CUDA(B->h_packed.ensure(4 * (size_t)total));
+        AW_CUDA(cudaMemcpyAsync(B->h_packed.p, B->packed.p, 4 * (size_t)total, cudaMemcpyDeviceToHost, B->st));
+        AW_CUDA(cudaStreamSynchronize(B->st));
+    }
+    const uint32_t *hp = B->h_packed.as<uint32_t>();
+    int rc = AW_OK;
+    for (int i = 0; i < n; ++i) {
+        ksw_extz_t *z = &ez[i];
+        reset_extz(z);
+        if (pl->early_zdrop[i]) { z->zdropped = 1; continue; }
+        if (!pl->route[i]) continue;
+        const KswOut &o = ho[i];
+        z->max = (uint32_t)o.max & 0x7fffffffu;
+        z->max_q = o.max_q, z->max_t = o.max_t, z->mqe = o.mqe, z->mqe_t = o.mqe_t;
+        z->mte = o.mte, z->mte_q = o.mte_q, z->score = o.score;
+        z->zdropped = o.zdropped ? 1 : 0, z->reach_end = o.reach_end, z->stopped = o.stopped;
+        if (cigar && o.n_cigar > 0) {
+            if (!store_cigar(km, z, hp + poff[i], o.n_cigar)) { z->zdropped = 1; rc = AW_E_NOMEM; }
+        }
+    }
+    return rc;
+}
+
+// ---- exported entry points --------------------------------------------------------------
+extern "C" {
+
+const char *aw_last_error(void) { return tls_err.c_str(); }
+
+int aw_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+void aw_set_traceback_budget(int64_t bytes) {
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    g_tb_budget = bytes;
+}
+
+void aw_set_tuning(int large_warps, int large_tlen_threshold) {
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    if (large_warps == 1 || large_warps == 2 || large_warps == 4 || large_warps == 8) g_large_warps = large_warps;
+    if (large_tlen_threshold > 0) g_large_tlen = large_tlen_threshold;
+}
+
+aw_ksw_plan_t *aw_ksw_plan_new(int n, const int *qlen, const int *tlen, const int *w, int8_t m,
+                               const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int zdrop,
+                               int end_bonus, int flag) {
+    if (n < 0 || (n > 0 && (!qlen || !tlen || !mat))) { set_error("invalid arguments"); return nullptr; }
+    aw_ksw_plan_t *pl = new aw_ksw_plan_t();
+    pl->B = &pl->own;
+    if (!make_params(m, mat, q, e, q2, e2, zdrop, end_bonus, flag, pl->P)) {
+        set_error("alphabet size m must be 2..8");
+        delete pl;
+        return nullptr;
+    }
+    if (plan_build(pl, n, qlen, tlen, w) || plan_alloc(pl)) { delete pl; return nullptr; }
+    return pl;
+}
+
+int aw_ksw_plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uint8_t *const *target) {
+    if (!pl) return AW_E_INVAL;
+    return plan_upload(pl, query, target);
+}
+
+int aw_ksw_plan_execute(aw_ksw_plan_t *pl, float *ms) {
+    if (!pl) return AW_E_INVAL;
+    return plan_execute(pl, ms);
+}
+
+int aw_ksw_plan_download(aw_ksw_plan_t *pl, ksw_extz_t *ez) {
+    if (!pl || !ez) return AW_E_INVAL;
+    return plan_download(pl, ez, nullptr);
+}
+
+int aw_ksw_plan_stats(const aw_ksw_plan_t *pl, int64_t *cells, int64_t *tb_bytes, int *waves, int *launches) {
+    if (!pl) return AW_E_INVAL;
+    if (cells) *cells = pl->cells;
+    if (tb_bytes) *tb_bytes = pl->tb_total;
+    if (waves) *waves = (int)pl->waves.size();
+    if (launches) *launches = pl->launches;
+    return AW_OK;
+}
+
+float aw_ksw_plan_dp_ms(const aw_ksw_plan_t *pl) { return pl ? pl->dp_ms_mean : 0.f; }
+
+void aw_ksw_plan_free(aw_ksw_plan_t *pl) { delete pl; }
+
+int aw_ksw_extd2_batch(int n, const int *qlen, const uint8_t *const *query, const int *tlen,
+                       const uint8_t *const *target, const int *w, int8_t m, const int8_t *mat, int8_t q,
+                       int8_t e, int8_t q2, int8_t e2, int zdrop, int end_bonus, int flag, ksw_extz_t *ez) {
+    if (n < 0 || (n > 0 && (!qlen || !tlen || !query || !target || !mat || !ez))) return AW_E_INVAL;
+    if (n == 0) return AW_OK;
+    aw_ksw_plan_t pl;
+    pl.B = thread_buffers();
+    if (!make_params(m, mat, q, e, q2, e2, zdrop, end_bonus, flag, pl.P)) {
+        set_error("alphabet size m must be 2..8");
+        for (int i = 0; i < n; ++i) reset_extz(&ez[i]), ez[i].zdropped = 1;
+        return AW_E_UNSUPPORTED;
+    }
+    int rc = plan_build(&pl, n, qlen, tlen, w);
+    if (!rc) rc = plan_alloc(&pl);
+    if (!rc) rc = plan_upload(&pl, query, target);
+    if (!rc) rc = plan_execute(&pl, nullptr);
+    if (!rc) rc = plan_download(&pl, ez, nullptr);
+    if (rc)
+        for (int i = 0; i < n; ++i)
+            if (!pl.executed) reset_extz(&ez[i]), ez[i].zdropped = 1;
+    pl.B = nullptr;
+    return rc;
+}
+
+static void single_call(void *km, int qlen, const uint8_t *query, int tlen, const uint8_t *target, int8_t m,
+                        const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int w, int zdrop,
+                        int end_bonus, int flag, ksw_extz_t *ez) {
+    reset_extz(ez);
+    if (m <= 1 || qlen <= 0 || tlen <= 0) return;
+    aw_ksw_plan_t pl;
+    pl.B = thread_buffers();
+    if (!make_params(m, mat, q, e, q2, e2, zdrop, end_bonus, flag, pl.P)) {
+        set_error("alphabet size m must be 2..8");
+        ez->zdropped = 1;
+        return;
+    }
+    int rc = plan_build(&pl, 1, &qlen, &tlen, &w);
+    if (!rc) rc = plan_alloc(&pl);
+    if (!rc) rc = plan_upload(&pl, &query, &target);
+    if (!rc) rc = plan_execute(&pl, nullptr);
+    if (!rc) rc = plan_download(&pl, ez, km);
+    if (rc && !pl.executed) reset_extz(ez), ez->zdropped = 1;
+    pl.B = nullptr;
+}
+
+void ksw_extd2_gpu(void *km, int qlen, const uint8_t *query, int tlen, const uint8_t *target, int8_t m,
+                   const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int w, int zdrop,
+                   int end_bonus, int flag, ksw_extz_t *ez) {
+    single_call(km, qlen, query, tlen, target, m, mat, q, e, q2, e2, w, zdrop, end_bonus,
+                flag & ~AW_EZ_SINGLETRACK, ez);
+}
+
+void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                               int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int w,
+                               int zdrop, int end_bonus, int flag, ksw_extz_t *ez) {
+    single_call(km, qlen, query, tlen, target, m, mat, q, e, q2, e2, w, zdrop, end_bonus,
+                flag | AW_EZ_SINGLETRACK, ez);
+}
+
+}  // extern "C"

@@ -1,0 +1,337 @@
+"""Host-side mirror of AnchorWave's KSW2 interface, running on the B200 kernels.
+
+Two layers, both reached through libaw_b200.so's C ABI:
+
+* the minimap2 entry points (minimap2/ksw2.h:91-107, ksw2_singletrack.hpp:17-46):
+  :func:`ksw_extd2`, :func:`ksw_extd2_singletrack`, plus the batched form
+  :func:`ksw_extd2_batch` and :class:`KswPlan` (device-resident batch);
+* the AnchorWave callers that sit on that boundary
+  (src/myImportandFunction/alignSlidingWindow.cpp): :func:`minimap2_alignment`
+  (:241-332), :func:`alignment_minimap2` (semiglobal end, :334-431),
+  :func:`align_sliding_window_minimap2` (banded, :800-890), :func:`ksw2_score_only`
+  (:723-796), :func:`align_ksw2_singletrack` / ``_banded`` (:892-1013) and
+  :func:`score_gapped_two_piece_affine` (:677-721) -- same names, argument meaning
+  (AnchorWave's negative penalties) and error behaviour.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from ._lib import AwError, KswExtz, check, last_error, lib, libc
+
+KSW_NEG_INF = -0x40000000
+KSW_EZ_SCORE_ONLY = 0x01
+KSW_EZ_RIGHT = 0x02
+KSW_EZ_GENERIC_SC = 0x04
+KSW_EZ_APPROX_MAX = 0x08
+KSW_EZ_APPROX_DROP = 0x10
+KSW_EZ_EXTZ_ONLY = 0x40
+KSW_EZ_REV_CIGAR = 0x80
+KSW_EZ_SEMIGLOBAL_END = 0x800
+KSW_EZ_SINGLETRACK = 0x1000
+
+_ENC = np.full(256, 4, dtype=np.uint8)
+for _i, _c in enumerate(b"ACGT"):
+    _ENC[_c] = _i
+    _ENC[_c + 32] = _i
+
+
+@dataclass
+class KswResult:
+    """The comparable ksw_extz_t fields plus the CIGAR (BAM-packed words)."""
+    max: int
+    zdropped: int
+    max_q: int
+    max_t: int
+    mqe: int
+    mqe_t: int
+    mte: int
+    mte_q: int
+    score: int
+    n_cigar: int
+    reach_end: int
+    stopped: int
+    cigar: List[int] = field(default_factory=list)
+
+    def key(self):
+        return (self.max, self.zdropped, self.max_q, self.max_t, self.mqe, self.mqe_t, self.mte,
+                self.mte_q, self.score, self.n_cigar, self.reach_end, self.stopped, tuple(self.cigar))
+
+
+def _take(ez: KswExtz) -> KswResult:
+    cig = list(np.ctypeslib.as_array(ez.cigar, shape=(ez.n_cigar,))) if ez.n_cigar > 0 and ez.cigar else []
+    res = KswResult(ez.max, ez.zdropped, ez.max_q, ez.max_t, ez.mqe, ez.mqe_t, ez.mte, ez.mte_q,
+                    ez.score, ez.n_cigar, ez.reach_end, ez.stopped, [int(c) for c in cig])
+    if ez.cigar:
+        libc.free(C.cast(ez.cigar, C.c_void_p))
+        ez.cigar = None
+        ez.m_cigar = 0
+    return res
+
+
+def _codes(seq) -> np.ndarray:
+    if isinstance(seq, np.ndarray):
+        return np.ascontiguousarray(seq, dtype=np.uint8)
+    if isinstance(seq, str):
+        seq = seq.encode()
+    return np.frombuffer(bytes(seq), dtype=np.uint8)
+
+
+def _mat(mat) -> C.Array:
+    vals = list(mat)
+    return (C.c_int8 * len(vals))(*vals)
+
+
+def ksw_extd2(query, target, mat, q, e, q2, e2, w=-1, zdrop=-1, end_bonus=0, flag=0, m=5) -> KswResult:
+    """One ksw_extd2 call on the GPU (sequences as 0..m-1 codes)."""
+    qa, ta = _codes(query), _codes(target)
+    ez = KswExtz()
+    lib.ksw_extd2_gpu(None, len(qa), qa.ctypes.data, len(ta), ta.ctypes.data, m, _mat(mat), q, e, q2, e2,
+                      w, zdrop, end_bonus, flag, C.byref(ez))
+    return _take(ez)
+
+
+def ksw_extd2_singletrack(query, target, mat, q, e, q2, e2, w=-1, zdrop=-1, end_bonus=0, flag=0,
+                          m=5) -> KswResult:
+    qa, ta = _codes(query), _codes(target)
+    ez = KswExtz()
+    lib.ksw_extd2_singletrack_gpu(None, len(qa), qa.ctypes.data, len(ta), ta.ctypes.data, m, _mat(mat), q, e,
+                                  q2, e2, w, zdrop, end_bonus, flag, C.byref(ez))
+    return _take(ez)
+
+
+def _ptr_array(arrs: Sequence[np.ndarray]):
+    ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    return ptrs
+
+
+def ksw_extd2_batch(queries, targets, mat, q, e, q2, e2, w=None, zdrop=-1, end_bonus=0, flag=0,
+                    m=5) -> List[KswResult]:
+    """n independent ksw_extd2 calls in one submission (aw_ksw_extd2_batch)."""
+    qs = [_codes(x) for x in queries]
+    ts = [_codes(x) for x in targets]
+    n = len(qs)
+    if n == 0:
+        return []
+    ql = np.array([len(x) for x in qs], dtype=np.int32)
+    tl = np.array([len(x) for x in ts], dtype=np.int32)
+    wa = None if w is None else np.ascontiguousarray(np.broadcast_to(np.asarray(w, dtype=np.int32), (n,)))
+    ez = (KswExtz * n)()
+    rc = lib.aw_ksw_extd2_batch(n, ql.ctypes.data, _ptr_array(qs), tl.ctypes.data, _ptr_array(ts),
+                                None if wa is None else wa.ctypes.data, m, _mat(mat), q, e, q2, e2, zdrop,
+                                end_bonus, flag, ez)
+    out = [_take(ez[i]) for i in range(n)]
+    check(rc, "aw_ksw_extd2_batch")
+    return out
+
+
+class KswPlan:
+    """A batch kept resident on the device (aw_ksw_plan_*): upload once, execute many times."""
+
+    def __init__(self, queries, targets, mat, q, e, q2, e2, w=None, zdrop=-1, end_bonus=0, flag=0, m=5):
+        self.qs = [_codes(x) for x in queries]
+        self.ts = [_codes(x) for x in targets]
+        self.n = len(self.qs)
+        self.ql = np.array([len(x) for x in self.qs], dtype=np.int32)
+        self.tl = np.array([len(x) for x in self.ts], dtype=np.int32)
+        self.w = None if w is None else np.ascontiguousarray(
+            np.broadcast_to(np.asarray(w, dtype=np.int32), (self.n,)))
+        self._mat = _mat(mat)
+        self.h = lib.aw_ksw_plan_new(self.n, self.ql.ctypes.data, self.tl.ctypes.data,
+                                     None if self.w is None else self.w.ctypes.data, m, self._mat, q, e, q2, e2,
+                                     zdrop, end_bonus, flag)
+        if not self.h:
+            raise AwError(f"aw_ksw_plan_new failed: {last_error()}")
+
+    def upload(self):
+        check(lib.aw_ksw_plan_upload(self.h, _ptr_array(self.qs), _ptr_array(self.ts)), "aw_ksw_plan_upload")
+
+    def execute(self) -> float:
+        ms = C.c_float(0.0)
+        check(lib.aw_ksw_plan_execute(self.h, C.byref(ms)), "aw_ksw_plan_execute")
+        return ms.value
+
+    def dp_ms(self) -> float:
+        return float(lib.aw_ksw_plan_dp_ms(self.h))
+
+    def download(self) -> List[KswResult]:
+        ez = (KswExtz * self.n)()
+        rc = lib.aw_ksw_plan_download(self.h, ez)
+        out = [_take(ez[i]) for i in range(self.n)]
+        check(rc, "aw_ksw_plan_download")
+        return out
+
+    def stats(self):
+        cells, tb = C.c_int64(0), C.c_int64(0)
+        waves, launches = C.c_int(0), C.c_int(0)
+        check(lib.aw_ksw_plan_stats(self.h, C.byref(cells), C.byref(tb), C.byref(waves), C.byref(launches)),
+              "aw_ksw_plan_stats")
+        return {"cells": cells.value, "tb_bytes": tb.value, "waves": waves.value, "launches": launches.value}
+
+    def close(self):
+        if self.h:
+            lib.aw_ksw_plan_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def set_traceback_budget(nbytes: int):
+    lib.aw_set_traceback_budget(int(nbytes))
+
+
+def set_tuning(large_warps: int = 0, large_tlen_threshold: int = 0):
+    lib.aw_set_tuning(int(large_warps), int(large_tlen_threshold))
+
+
+# ---- AnchorWave callers on the KSW2 boundary -------------------------------------
+
+def anchorwave_matrix(mismatching_penalty: int) -> List[int]:
+    """5x5 matrix: match 0, every unequal pair (N included) -|mismatch| (alignSlidingWindow.cpp:245-255)."""
+    b = mismatching_penalty if mismatching_penalty < 0 else -mismatching_penalty
+    return [0 if i == j else b for i in range(5) for j in range(5)]
+
+
+def encode(seq: str) -> Tuple[np.ndarray, int]:
+    """encodeKswSequence (alignSlidingWindow.cpp:645-660): ACGT -> 0..3, other -> 4 + GENERIC_SC."""
+    codes = _ENC[np.frombuffer(seq.encode() if isinstance(seq, str) else bytes(seq), dtype=np.uint8)]
+    return codes, (KSW_EZ_GENERIC_SC if (codes == 4).any() else 0)
+
+
+def decode_cigar(cigar: Sequence[int], dna_q: str, dna_d: str) -> Tuple[str, str, int, int]:
+    """CIGAR -> gapped rows (alignSlidingWindow.cpp:307-324): M/=/X copy both, I query only, D target only."""
+    aq, ad = [], []
+    qp = tp = 0
+    for c in cigar:
+        ln, op = c >> 4, c & 0xF
+        if op in (0, 7, 8):
+            aq.append(dna_q[qp:qp + ln]); ad.append(dna_d[tp:tp + ln]); qp += ln; tp += ln
+        elif op == 1:
+            aq.append(dna_q[qp:qp + ln]); ad.append("-" * ln); qp += ln
+        elif op == 2:
+            aq.append("-" * ln); ad.append(dna_d[tp:tp + ln]); tp += ln
+        else:
+            raise ValueError(f"unexpected CIGAR op {op}")
+    return "".join(aq), "".join(ad), qp, tp
+
+
+def score_gapped_two_piece_affine(aln_q: str, aln_d: str, mismatching_penalty: int, open1: int, extend1: int,
+                                  open2: int, extend2: int) -> int:
+    """scoreGappedTwoPieceAffineAlignment (alignSlidingWindow.cpp:677-721); penalties are negative."""
+    if len(aln_q) != len(aln_d):
+        raise RuntimeError("KSW2 returned alignment rows with different lengths")
+    score = 0
+    col = 0
+    n = len(aln_q)
+    while col < n:
+        qg, dg = aln_q[col] == "-", aln_d[col] == "-"
+        if qg and dg:
+            raise RuntimeError("KSW2 returned an alignment column with two gaps")
+        if qg or dg:
+            end = col + 1
+            while end < n and (aln_q[end] == "-") == qg and (aln_d[end] == "-") != qg:
+                end += 1
+            ln = end - col
+            score += max(open1 + extend1 * ln, open2 + extend2 * ln)
+            col = end
+            continue
+        if aln_q[col] != aln_d[col]:
+            score += mismatching_penalty
+        col += 1
+    return score
+
+
+def minimap2_alignment(dna_q: str, dna_d: str, matching_score: int, mismatching_penalty: int, open1: int,
+                       extend1: int, open2: int, extend2: int) -> Tuple[int, str, str]:
+    """minimap2AlignmentWithArena (alignSlidingWindow.cpp:241-332): global KSW2 with CIGAR.
+    Returns (ez.score, aligned query, aligned reference)."""
+    qs, f1 = encode(dna_q)
+    ts, f2 = encode(dna_d)
+    res = ksw_extd2(qs, ts, anchorwave_matrix(mismatching_penalty), -open1, -extend1, -open2, -extend2,
+                    -1, -1, 0, f1 | f2)
+    aq, ad, qp, tp = decode_cigar(res.cigar, dna_q, dna_d)
+    assert qp == len(dna_q) and tp == len(dna_d)
+    return res.score, aq, ad
+
+
+def alignment_minimap2(dna_q: str, dna_d: str, matching_score: int, mismatching_penalty: int, open1: int,
+                       extend1: int, open2: int, extend2: int) -> Tuple[int, str, str, int, int]:
+    """alignmentMinimap2WithArena (alignSlidingWindow.cpp:334-431): traceback from the better end
+    (KSW_EZ_SEMIGLOBAL_END).  Returns (score, aln_q, aln_d, endPositionq, endPositiont)."""
+    qs, f1 = encode(dna_q)
+    ts, f2 = encode(dna_d)
+    res = ksw_extd2(qs, ts, anchorwave_matrix(mismatching_penalty), -open1, -extend1, -open2, -extend2,
+                    -1, -1, 0, KSW_EZ_SEMIGLOBAL_END | f1 | f2)
+    if res.mqe > res.mte:
+        end_t, end_q = res.mqe_t + 1, len(dna_q)
+    else:
+        end_t, end_q = len(dna_d), res.mte_q + 1
+    aq, ad, qp, tp = decode_cigar(res.cigar, dna_q, dna_d)
+    assert qp == end_q and tp == end_t
+    return res.score, aq, ad, end_q, end_t
+
+
+def align_sliding_window_minimap2(dna_q: str, dna_d: str, sliding_window_size: int, mismatching_penalty: int,
+                                  open1: int, extend1: int, open2: int, extend2: int) -> Tuple[int, str, str]:
+    """alignSlidingWindow_minimap2 (alignSlidingWindow.cpp:800-890): full (-1) or banded KSW2,
+    re-scored with the two-piece objective."""
+    qs, f1 = encode(dna_q)
+    ts, f2 = encode(dna_d)
+    res = ksw_extd2(qs, ts, anchorwave_matrix(mismatching_penalty), -open1, -extend1, -open2, -extend2,
+                    int(sliding_window_size), -1, 0, f1 | f2)
+    aq, ad, qp, tp = decode_cigar(res.cigar, dna_q, dna_d)
+    assert qp == len(dna_q) and tp == len(dna_d)
+    return score_gapped_two_piece_affine(aq, ad, mismatching_penalty, open1, extend1, open2, extend2), aq, ad
+
+
+def ksw2_score_only(dna_q: str, dna_d: str, mismatching_penalty: int, open1: int, extend1: int, open2: int,
+                    extend2: int) -> Tuple[int, bool]:
+    """ksw2ScoreOnly (alignSlidingWindow.cpp:723-796): (score, stopped)."""
+    if not dna_q or not dna_d:
+        ln = max(len(dna_q), len(dna_d))
+        return max(open1 + extend1 * ln, open2 + extend2 * ln), False
+    qs, f1 = encode(dna_q)
+    ts, f2 = encode(dna_d)
+    res = ksw_extd2(qs, ts, anchorwave_matrix(mismatching_penalty), -open1, -extend1, -open2, -extend2,
+                    -1, -1, 0, KSW_EZ_SCORE_ONLY | f1 | f2)
+    return res.score, bool(res.stopped)
+
+
+def align_ksw2_singletrack_banded(dna_q: str, dna_d: str, band_width: int, mismatching_penalty: int,
+                                  open1: int, extend1: int, open2: int, extend2: int) -> Tuple[int, str, str, bool]:
+    """alignKsw2SingletrackImpl (alignSlidingWindow.cpp:892-990): (score, aln_q, aln_d, stopped).
+    Score is KSW_NEG_INF with empty rows when the traceback fails."""
+    if not dna_q or not dna_d:
+        ln = max(len(dna_q), len(dna_d))
+        aq = dna_q if dna_q else "-" * ln
+        ad = dna_d if dna_d else "-" * ln
+        return max(open1 + extend1 * ln, open2 + extend2 * ln), aq, ad, False
+    if band_width < -1:
+        raise ValueError("KSW2-Singletrack band width must be -1..INT_MAX")
+    qs, f1 = encode(dna_q)
+    ts, f2 = encode(dna_d)
+    res = ksw_extd2_singletrack(qs, ts, anchorwave_matrix(mismatching_penalty), -open1, -extend1, -open2,
+                                -extend2, int(band_width), -1, 0, f1 | f2)
+    if res.stopped or res.zdropped:
+        return KSW_NEG_INF, "", "", bool(res.stopped)
+    try:
+        aq, ad, qp, tp = decode_cigar(res.cigar, dna_q, dna_d)
+    except ValueError:
+        return KSW_NEG_INF, "", "", False
+    if qp != len(dna_q) or tp != len(dna_d):
+        return KSW_NEG_INF, "", "", False
+    return score_gapped_two_piece_affine(aq, ad, mismatching_penalty, open1, extend1, open2, extend2), aq, ad, False
+
+
+def align_ksw2_singletrack(dna_q: str, dna_d: str, mismatching_penalty: int, open1: int, extend1: int,
+                           open2: int, extend2: int):
+    """alignKsw2Singletrack (alignSlidingWindow.cpp:992-1003): unbanded Singletrack."""
+    return align_ksw2_singletrack_banded(dna_q, dna_d, -1, mismatching_penalty, open1, extend1, open2, extend2)

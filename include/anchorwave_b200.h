@@ -1,0 +1,121 @@
+/*
+ * anchorwave_b200.h -- C ABI of libaw_b200.so, the B200 (sm_100a) implementation
+ * of AnchorWave's per-interval alignment kernels.
+ *
+ * Plain C types only (pointers, sizes, ints); no CUDA or torch types.  Every
+ * entry point is reentrant: each host thread gets its own CUDA stream and its
+ * own pooled device buffers.  Errors never cross the ABI as exceptions; the
+ * drop-in KSW2 entries report them as ez->zdropped = 1 (the reference's own
+ * failure convention, minimap2/ksw2_extd2_avx.c:138-141) and record a message
+ * readable with aw_last_error().
+ */
+#ifndef ANCHORWAVE_B200_H
+#define ANCHORWAVE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef KSW2_H_
+/* Result record, layout-identical to ksw_extz_t of minimap2/ksw2.h:40-50. */
+typedef struct {
+    uint32_t max:31, zdropped:1;
+    int max_q, max_t;      /* max extension coordinate */
+    int mqe, mqe_t;        /* max score when reaching the end of query */
+    int mte, mte_q;        /* max score when reaching the end of target */
+    int score;             /* max score reaching both ends; may be KSW_NEG_INF */
+    int m_cigar, n_cigar;
+    int reach_end;
+    int stopped;           /* cooperative stop requested */
+    uint32_t *cigar;       /* BAM ops: len<<4 | {0=M,1=I,2=D} */
+} ksw_extz_t;
+#endif
+
+/* ---- drop-in KSW2 entries -------------------------------------------------- */
+
+/*
+ * Replaces ksw_extd2_sse / ksw_extd2_avx2 / ksw_extd2_avx512
+ * (minimap2/ksw2.h:91-107; called from
+ * src/myImportandFunction/alignSlidingWindow.cpp:288-297, :380-389, :762-792,
+ * :840-846).  Same arguments, same ksw_extz_t results bit for bit (scores, end
+ * coordinates, CIGAR including tie-breaking) as the AVX-512 kernel.
+ * CIGAR ownership as in the reference: the buffer is (re)allocated with
+ * krealloc(km, ...) when km != NULL (kalloc arena of the calling process,
+ * looked up at run time) and with realloc() when km == NULL; the caller frees
+ * it with kfree(km, ez->cigar) / free().  ez->m_cigar/ez->cigar on entry are
+ * reused like ksw_push_cigar does.
+ */
+void ksw_extd2_gpu(void *km, int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                   int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2,
+                   int w, int zdrop, int end_bonus, int flag, ksw_extz_t *ez);
+
+/*
+ * Replaces ksw_extd2_singletrack_avx512 / _avx2 (minimap2/ksw2_singletrack.hpp:32-46):
+ * KSW2 score recurrence with the Singletrack two-track traceback.
+ */
+void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tlen,
+                               const uint8_t *target, int8_t m, const int8_t *mat, int8_t q,
+                               int8_t e, int8_t q2, int8_t e2, int w, int zdrop, int end_bonus,
+                               int flag, ksw_extz_t *ez);
+
+/* ---- batched KSW2 ------------------------------------------------------------ */
+
+/*
+ * n independent ksw_extd2 calls in one submission (the batched form of the
+ * AnchorTaskExecutor loop, src/service/AnchorTaskExecutor.h:54-160).  Pair i
+ * is (query[i], qlen[i]) x (target[i], tlen[i]) with band w[i] (w == NULL:
+ * all -1).  Results land in ez[i] exactly as n calls of ksw_extd2_gpu would
+ * leave them; ez[i].cigar is malloc'd (km semantics: NULL arena).
+ * Returns 0 on success, a negative AW_E* code otherwise.
+ */
+int aw_ksw_extd2_batch(int n, const int *qlen, const uint8_t *const *query, const int *tlen,
+                       const uint8_t *const *target, const int *w, int8_t m, const int8_t *mat,
+                       int8_t q, int8_t e, int8_t q2, int8_t e2, int zdrop, int end_bonus,
+                       int flag, ksw_extz_t *ez);
+
+/* Plan API: keep a batch resident on the device to run it repeatedly. */
+typedef struct aw_ksw_plan aw_ksw_plan_t;
+aw_ksw_plan_t *aw_ksw_plan_new(int n, const int *qlen, const int *tlen, const int *w, int8_t m,
+                               const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2,
+                               int zdrop, int end_bonus, int flag);
+int aw_ksw_plan_upload(aw_ksw_plan_t *plan, const uint8_t *const *query,
+                       const uint8_t *const *target);
+/* Runs every wave of the plan on its stream; ms (optional) receives the CUDA-event
+ * time of the device work between the first and the last launch. */
+int aw_ksw_plan_execute(aw_ksw_plan_t *plan, float *ms);
+int aw_ksw_plan_download(aw_ksw_plan_t *plan, ksw_extz_t *ez);
+/* Device-side statistics of the plan: cells, traceback bytes, waves, launches. */
+int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_bytes, int *waves,
+                      int *launches_per_execute);
+/* Mean CUDA-event time (ms) of the plan's DP kernel launches in the last execute. */
+float aw_ksw_plan_dp_ms(const aw_ksw_plan_t *plan);
+void aw_ksw_plan_free(aw_ksw_plan_t *plan);
+
+/* ---- configuration and diagnostics ------------------------------------------ */
+
+/* HBM budget (bytes) for traceback arenas per host thread; mirrors the -M
+ * admission envelope (src/myImportandFunction/AlignmentResourceScheduler.cpp:706).
+ * 0 = default (60% of free device memory). */
+void aw_set_traceback_budget(int64_t bytes);
+/* Warps that cooperate on one pair for pairs with tlen >= threshold, and the
+ * threshold (autotuner knobs; 0 keeps the current value). */
+void aw_set_tuning(int large_warps, int large_tlen_threshold);
+const char *aw_last_error(void);
+int aw_device_count(void);
+/* Integer-ALU peak probe: IADD3/IMNMX-class 32-bit ops per second measured on
+ * the current device (used as the roofline denominator for the DP kernels). */
+double aw_int32_peak_ops(void);
+
+#define AW_OK            0
+#define AW_E_INVAL     (-1)
+#define AW_E_CUDA      (-2)
+#define AW_E_NOMEM     (-3)
+#define AW_E_TIMEOUT   (-4)
+#define AW_E_UNSUPPORTED (-5)
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANCHORWAVE_B200_H */

@@ -1,0 +1,63 @@
+"""CPU: the C-ABI library loads and exports every function include/anchorwave_b200.h declares;
+host-side helpers (workload generators, CIGAR decoding, two-piece rescoring) behave like the
+reference's; without a GPU the entry points fail loudly instead of falling back to the CPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+import oracle
+from anchorwave_b200 import _lib, ksw2, workloads as W
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "anchorwave_b200.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\(", text, flags=re.M)
+    return sorted(set(n for n in names if n not in ("defined",)))
+
+
+def test_header_declares_expected_entry_points():
+    names = header_functions()
+    for required in ("ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "aw_ksw_extd2_batch"):
+        assert required in names
+
+
+def test_library_exports_every_header_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in header_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.EXPORTS) <= set(header_functions())
+
+
+def test_no_cpu_fallback_without_gpu():
+    if _lib.lib.aw_device_count() > 0:
+        return  # GPU present: covered by the gpu tests
+    r = ksw2.ksw_extd2(b"\x00\x01\x02", b"\x00\x01\x03", ksw2.anchorwave_matrix(-4), 4, 2, 24, 1)
+    assert r.zdropped == 1 and r.n_cigar == 0
+    assert _lib.last_error()
+
+
+def test_workloads_deterministic_and_shaped():
+    a = W.batched_full_set(32, seed=1)
+    b = W.batched_full_set(32, seed=1)
+    assert all((x == y).all() for x, y in zip(a.queries, b.queries))
+    assert all(200 <= len(t) <= 20000 for t in a.targets)
+    q, t = W.plain_pair(0)
+    assert len(t) == 5000 and 4000 < len(q) < 5000
+    assert W.band_cells(100, 100, -1) == 100 * 100
+
+
+def test_decode_and_rescore_match_reference_semantics(restatement):
+    rng = np.random.default_rng(9)
+    for _ in range(20):
+        qc, tc = W.divergent_pair(rng, int(rng.integers(30, 400)), 0.02, 0.2, 4.0)
+        r = restatement.ksw_extd2(qc.tobytes(), tc.tobytes(), oracle.anchorwave_matrix(-4), 4, 2, 24, 1)
+        qs, ts = W.to_ascii(qc).decode(), W.to_ascii(tc).decode()
+        aq, ad, qp, tp = ksw2.decode_cigar(r.cigar, qs, ts)
+        assert qp == len(qs) and tp == len(ts) and len(aq) == len(ad)
+        # in full mode the emitted CIGAR's two-piece score is the DP optimum
+        assert ksw2.score_gapped_two_piece_affine(aq, ad, -4, -4, -2, -24, -1) == r.score

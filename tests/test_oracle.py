@@ -1,0 +1,113 @@
+"""CPU: the oracle itself is pinned -- the plain-C restatement against the golden vectors
+generated from the compiled reference, and (where oracle/_ref is present) against the
+compiled reference live on fresh seeded corpora, for all three SIMD variants."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from anchorwave_b200 import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ksw2_golden.json")
+
+
+def _golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def _mat(c):
+    return c.get("mat") or oracle.anchorwave_matrix(c["mismatch"])
+
+
+def _codes(s):
+    return W.to_codes(s.encode()).tobytes()
+
+
+def test_restatement_matches_golden(restatement):
+    g = _golden()
+    bad = []
+    for c in g["cases"]:
+        flag = c["flag"] | (oracle.KSW_EZ_SINGLETRACK if c["variant"] == 2 else 0)
+        r = restatement.ksw_extd2(_codes(c["query"]), _codes(c["target"]), _mat(c), c["q"], c["e"], c["q2"],
+                                  c["e2"], w=c["w"], zdrop=c["zdrop"], end_bonus=c["end_bonus"], flag=flag,
+                                  block=g["block"])
+        exp = c["result"]
+        got = {k: getattr(r, k) for k in exp}
+        if got != exp:
+            bad.append(c["name"])
+    assert not bad, f"restatement differs from golden on {bad}"
+
+
+def test_reference_matches_golden(reference):
+    g = _golden()
+    if reference.block != g["block"]:
+        pytest.skip("host ISA differs from the golden generator's")
+    for c in g["cases"][:40]:
+        r = reference.ksw_extd2(_codes(c["query"]), _codes(c["target"]), _mat(c), c["q"], c["e"], c["q2"],
+                                c["e2"], w=c["w"], zdrop=c["zdrop"], end_bonus=c["end_bonus"], flag=c["flag"],
+                                variant=c["variant"])
+        assert {k: getattr(r, k) for k in c["result"]} == c["result"], c["name"]
+
+
+FLAGS = [0, oracle.KSW_EZ_SCORE_ONLY, oracle.KSW_EZ_RIGHT, oracle.KSW_EZ_SEMIGLOBAL_END, oracle.KSW_EZ_EXTZ_ONLY,
+         oracle.KSW_EZ_APPROX_MAX, oracle.KSW_EZ_REV_CIGAR, oracle.KSW_EZ_APPROX_MAX | oracle.KSW_EZ_APPROX_DROP]
+PEN = [(4, 2, 24, 1), (8, 2, 75, 1), (6, 1, 20, 0), (2, 3, 30, 1), (24, 1, 4, 2)]
+
+
+@pytest.mark.parametrize("isa", ["avx512", "avx2", "sse"])
+def test_restatement_matches_reference_random(restatement, isa):
+    try:
+        ref = oracle.Reference(isa)
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    if isa != "sse" and oracle.ISA_BLOCK[oracle.cpu_isa()] < oracle.ISA_BLOCK[isa]:
+        pytest.skip(f"host cannot run {isa}")
+    rng = np.random.default_rng(11 + len(isa))
+    n = 0
+    for it in range(160):
+        L = int(rng.integers(1, 500))
+        qc, tc = W.divergent_pair(rng, L, 0.01, 0.3, 4.0)
+        if rng.random() < 0.2:
+            qc = qc.copy()
+            qc[rng.integers(0, len(qc), 3)] = 4
+        gen = oracle.KSW_EZ_GENERIC_SC if (4 in qc or 4 in tc) else 0
+        pen = PEN[it % len(PEN)]
+        w = -1 if it % 3 == 0 else int(rng.integers(0, max(2, L // 3)))
+        flag = FLAGS[it % len(FLAGS)] | gen
+        zdrop = -1 if it % 5 else 60
+        mat = oracle.anchorwave_matrix(-4) if it % 7 else [2 if a == b else -4 for a in range(5) for b in range(5)]
+        a = restatement.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop, flag=flag,
+                                  block=ref.block)
+        b = ref.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop, flag=flag)
+        assert a.key() == b.key(), (it, L, w, hex(flag), pen)
+        if isa != "sse" and not (flag & (oracle.KSW_EZ_SCORE_ONLY | oracle.KSW_EZ_SEMIGLOBAL_END | oracle.KSW_EZ_EXTZ_ONLY)):
+            a = restatement.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop,
+                                      flag=flag | oracle.KSW_EZ_SINGLETRACK, block=ref.block)
+            b = ref.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop, flag=flag, variant=2)
+            assert a.key() == b.key(), ("singletrack", it, L, w, hex(flag), pen)
+        n += 1
+    assert n == 160
+
+
+def test_restatement_stop_hook_matches_reference(restatement, reference):
+    rng = np.random.default_rng(5)
+    q, t = W.divergent_pair(rng, 900, 0.05, 0.05, 3.0)
+    mat = oracle.anchorwave_matrix(-4)
+    for stop_at in (0, 256, 512, 1024, 5000):
+        a = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, stop_interval=256, stop_at=stop_at,
+                                  block=reference.block)
+        b = reference.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, stop_interval=256, stop_at=stop_at)
+        assert a.key() == b.key(), stop_at
+
+
+def test_simd_variants_agree_in_full_mode(reference):
+    """Full-mode results are independent of the SIMD width (padding lanes are never read)."""
+    rng = np.random.default_rng(3)
+    for _ in range(30):
+        q, t = W.divergent_pair(rng, int(rng.integers(50, 800)), 0.01, 0.15, 4.0)
+        a = reference.ksw_extd2(q.tobytes(), t.tobytes(), oracle.anchorwave_matrix(-4), 4, 2, 24, 1, variant=0)
+        b = reference.ksw_extd2(q.tobytes(), t.tobytes(), oracle.anchorwave_matrix(-4), 4, 2, 24, 1, variant=1)
+        assert a.key() == b.key()
