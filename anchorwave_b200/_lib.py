@@ -25,7 +25,7 @@ class KswExtz(C.Structure):
 EXPORTS = [
     "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "aw_ksw_extd2_batch",
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
-    "aw_ksw_plan_stats", "aw_ksw_plan_dp_ms", "aw_ksw_plan_free",
+    "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops",
 ]
@@ -53,8 +53,8 @@ def _load():
     lib.aw_ksw_plan_download.restype = i32
     lib.aw_ksw_plan_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]
     lib.aw_ksw_plan_stats.restype = i32
-    lib.aw_ksw_plan_dp_ms.argtypes = [vp]
-    lib.aw_ksw_plan_dp_ms.restype = C.c_float
+    lib.aw_ksw_plan_timing.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    lib.aw_ksw_plan_timing.restype = i32
     lib.aw_ksw_plan_free.argtypes = [vp]
     lib.aw_ksw_plan_free.restype = None
     lib.aw_set_traceback_budget.argtypes = [i64]

@@ -277,8 +277,7 @@ struct aw_ksw_plan {
     int64_t cells = 0, tb_total = 0;
     int launches = 0;
     bool uploaded = false, executed = false;
-    float dp_ms_mean = 0.f;
-    int dp_launches = 0;
+    float dp_ms = 0.f, bt_ms = 0.f;
 };
 
 static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen, const int *w) {
@@ -446,15 +445,15 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
         std::lock_guard<std::mutex> lk(g_cfg_mu);
         large_warps = g_large_warps;
     }
-    // per-launch timing events for the DP kernels
-    const size_t need_ev = 2 * (pl->waves.size() * 2 + 2);
+    // per-wave timing events: DP phase start, DP phase end (after the join), backtrack end
+    const size_t need_ev = 3 * pl->waves.size() + 3;
     while (B->ev_k.size() < need_ev) {
         cudaEvent_t e;
         AW_CUDA(cudaEventCreate(&e));
         B->ev_k.push_back(e);
     }
-    int dp_count = 0;
-    for (size_t k = 0; k < pl->waves.size(); ++k) {
+    const int nw = (int)pl->waves.size();
+    for (int k = 0; k < nw; ++k) {
         const auto &W = pl->waves[k];
         KswFullArgs a;
         a.qcodes = B->qcodes.as<uint8_t>(), a.tcodes = B->tcodes.as<uint8_t>();
@@ -462,6 +461,7 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
         a.tb = B->tb.as<uint8_t>(), a.bnd = B->bnd.as<uint32_t>();
         a.error = B->error.as<int32_t>();
         a.sc = pl->S;
+        AW_CUDA(cudaEventRecord(B->ev_k[3 * k], B->st));
         // fork: large pairs on st2 (groups of large_warps warps), small on st (single warps)
         AW_CUDA(cudaEventRecord(B->ev_a, B->st));
         AW_CUDA(cudaStreamWaitEvent(B->st2, B->ev_a, 0));
@@ -472,10 +472,7 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
             const int groups = 8 / large_warps;
             const int occ = std::max(1, ksw_full_occupancy(P.flag, large_warps, groups));
             const int ctas = std::min(W.n_large / groups + 1, occ * B->sms);
-            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count], B->st2));
             AW_CUDA(launch_ksw_full(a, P.flag, large_warps, groups, ctas, B->st2));
-            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count + 1], B->st2));
-            ++dp_count;
             ++launches;
         }
         if (W.n_small > 0) {
@@ -484,20 +481,19 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
             a.queue = B->queue.as<int32_t>() + 64 * (2 * k + 1);
             const int occ = std::max(1, ksw_full_occupancy(P.flag, 1, 8));
             const int ctas = std::min((W.n_small + 7) / 8, occ * B->sms);
-            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count], B->st));
             AW_CUDA(launch_ksw_full(a, P.flag, 1, 8, ctas, B->st));
-            AW_CUDA(cudaEventRecord(B->ev_k[2 * dp_count + 1], B->st));
-            ++dp_count;
             ++launches;
         }
         AW_CUDA(cudaEventRecord(B->ev_b, B->st2));
         AW_CUDA(cudaStreamWaitEvent(B->st, B->ev_b, 0));
+        AW_CUDA(cudaEventRecord(B->ev_k[3 * k + 1], B->st));
         if (!(P.flag & AW_EZ_SCORE_ONLY) && W.n_large + W.n_small > 0) {
             AW_CUDA(launch_ksw_backtrack_full(B->pairs.as<KswPair>(), B->order.as<int32_t>() + W.begin_large,
                                               W.n_large + W.n_small, B->tb.as<uint8_t>(), B->out.as<KswOut>(),
                                               B->cig.as<uint32_t>(), P.flag, B->st));
             ++launches;
         }
+        AW_CUDA(cudaEventRecord(B->ev_k[3 * k + 2], B->st));
     }
     if (!pl->exact_ids.empty()) {
         int rc = run_exact_ksw(pl->exact_ids.size(), B->order.as<int32_t>() + pl->order.size(),
@@ -513,14 +509,15 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
     AW_CUDA(cudaMemcpy(&err, B->error.p, 4, cudaMemcpyDeviceToHost));
     if (err) { set_error("a bounded device wait gave up (pipeline stall)"); return AW_E_TIMEOUT; }
     if (ms) AW_CUDA(cudaEventElapsedTime(ms, B->ev_t0, B->ev_t1));
-    float tot = 0.f;
-    for (int d = 0; d < dp_count; ++d) {
-        float t = 0.f;
-        AW_CUDA(cudaEventElapsedTime(&t, B->ev_k[2 * d], B->ev_k[2 * d + 1]));
-        tot += t;
+    float dp = 0.f, bt = 0.f;
+    for (int k = 0; k < nw; ++k) {
+        float t0 = 0.f, t1 = 0.f;
+        AW_CUDA(cudaEventElapsedTime(&t0, B->ev_k[3 * k], B->ev_k[3 * k + 1]));
+        AW_CUDA(cudaEventElapsedTime(&t1, B->ev_k[3 * k + 1], B->ev_k[3 * k + 2]));
+        dp += t0, bt += t1;
     }
-    pl->dp_ms_mean = dp_count ? tot / dp_count : 0.f;
-    pl->dp_launches = dp_count;
+    pl->dp_ms = dp;
+    pl->bt_ms = bt;
     pl->launches = launches;
     pl->executed = true;
     return AW_OK;
@@ -628,7 +625,12 @@ int aw_ksw_plan_stats(const aw_ksw_plan_t *pl, int64_t *cells, int64_t *tb_bytes
     return AW_OK;
 }
 
-float aw_ksw_plan_dp_ms(const aw_ksw_plan_t *pl) { return pl ? pl->dp_ms_mean : 0.f; }
+int aw_ksw_plan_timing(const aw_ksw_plan_t *pl, float *dp_ms, float *bt_ms) {
+    if (!pl) return AW_E_INVAL;
+    if (dp_ms) *dp_ms = pl->dp_ms;
+    if (bt_ms) *bt_ms = pl->bt_ms;
+    return AW_OK;
+}
 
 void aw_ksw_plan_free(aw_ksw_plan_t *pl) { delete pl; }
 

@@ -335,9 +335,10 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
             const bool act = pos <= en16;
             if (act) {
                 const int blk = pos / B, l = pos % B, bfirst = stB / B;
-                const int blane = blk == bfirst ? st16 - blk * B : 0;
+                // only the first block takes the band-edge value, at lane st16-stB;
+                // lane 0 of every later block takes the previous block's last lane
                 int8_t xs, vs, x2s;
-                if (l == blane) xs = x1, vs = v1, x2s = x21;
+                if (blk == bfirst && l == st16 - stB) xs = x1, vs = v1, x2s = x21;
                 else if (l == 0 && blk == bfirst) {
                     const int src = blk * B + 15;
                     xs = W.x[src], vs = W.v[src], x2s = W.x2[src];

@@ -155,8 +155,11 @@ class KswPlan:
         check(lib.aw_ksw_plan_execute(self.h, C.byref(ms)), "aw_ksw_plan_execute")
         return ms.value
 
-    def dp_ms(self) -> float:
-        return float(lib.aw_ksw_plan_dp_ms(self.h))
+    def timing(self):
+        """(dp_ms, backtrack_ms) of the last execute, CUDA events on the plan's stream."""
+        dp, bt = C.c_float(0.0), C.c_float(0.0)
+        check(lib.aw_ksw_plan_timing(self.h, C.byref(dp), C.byref(bt)), "aw_ksw_plan_timing")
+        return dp.value, bt.value
 
     def download(self) -> List[KswResult]:
         ez = (KswExtz * self.n)()

@@ -1,0 +1,348 @@
+"""Benchmark of the batched KSW2 alignment stage on B200 (one JSON line on rank 0).
+
+Workload (default): 4,096 interval pairs, target length log-uniform 200 bp-20 kb, divergence
+U(1%,15%) (80% substitutions, 20% indels of geometric length mean 4), AnchorWave scoring
+(match 0, mismatch -4, gap 4+2l / 24+l), global ksw_extd2 with CIGAR.  Seeded synthetic
+sequences stand in for the reference's B73/Mo17 intervals.
+
+A step = one pass of the hot path over the whole batch: the DP of every pair, the traceback
+and the CIGARs.
+  * value: inputs already resident in HBM (plan API), CUDA events around K steps on the
+    plan's stream; GCUPS = total DP cells / time.
+  * e2e: the same batch through the public C-ABI call aw_ksw_extd2_batch with host buffers
+    (pinned staging, H2D of the sequences, D2H of results and CIGARs) per step.
+  * plain_per_call: the plain per-call GPU form (one ksw_extd2_gpu call per pair) on a sample.
+  * cpu_baseline: AnchorWave's own AVX KSW2 compiled from the reference tree (oracle/_ref),
+    all host threads, bounded sample.
+  * roofline: the DP kernels are bound by the 32-bit integer ALU; achieved integer op rate =
+    DP cells x 47 ops/cell / DP-phase CUDA-event time, against the integer peak measured live
+    by aw_int32_peak_ops(); the traceback store stream is reported against HBM bandwidth.
+
+`--impl reference` times the reference CPU implementation (oracle/_ref) on the same workload,
+metric and unit.  With torchrun (N>1) every rank aligns its own batch (weak scaling, no
+collective on the data path); rank 0 prints the line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+OPS_PER_CELL_CIGAR = 47
+OPS_PER_CELL_SCORE = 31
+METRIC = "batched GCUPS & pairs/s vs plain per-call on 1 B200, bit-exact; p50/p99 latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--pairs", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-sample", type=int, default=64)
+    return ap.parse_args()
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        import torch
+        pg.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload(args, rank):
+    from anchorwave_b200 import workloads as W
+    return W.batched_full_set(args.pairs, seed=args.seed + rank)
+
+
+def run_reference_arm(args):
+    rank, world, local, pg = dist_init(args.gpus)
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    try:
+        ref = oracle.Reference()
+    except FileNotFoundError as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"compiled reference missing: {e}"}))
+        return 0
+    ps = workload(args, 0)
+    mat = oracle.anchorwave_matrix(-4)
+    import numpy as np
+    rng = np.random.default_rng(12345)
+    order = rng.permutation(len(ps))
+    qs = [ps.queries[i].tobytes() for i in order]
+    ts = [ps.targets[i].tobytes() for i in order]
+    cells_of = [len(ps.queries[i]) * len(ps.targets[i]) for i in order]
+    nthreads = os.cpu_count() or 1
+    budget = max(2.0, min(30.0, 60.0 / max(1, args.steps + args.warmup)))
+
+    def step():
+        r = ref.ksw_batch(qs, ts, mat, 4, 2, 24, 1, nthreads=nthreads, time_budget_s=budget)
+        # pairs handed out before the deadline are all finished by the time the call returns
+        done = r["done"]
+        hs = r["hash"]
+        finished = [i for i in range(len(qs)) if hs[i] != 0][:done]
+        cells = sum(cells_of[i] for i in finished)
+        return cells, len(finished), r["seconds"]
+
+    for _ in range(args.warmup):
+        step()
+    tot_c = tot_p = tot_s = 0.0
+    for _ in range(args.steps):
+        c, p, s = step()
+        tot_c += c
+        tot_p += p
+        tot_s += s
+    gcups = tot_c / tot_s / 1e9
+    line = {"metric": METRIC, "impl": "reference", "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+            "data": "synthetic (seeded; stands in for B73/Mo17 intervals)",
+            "pairs_per_s": tot_p / tot_s,
+            "config": {"workload": ps.name, "pairs": len(ps), "scoring": "match 0, mismatch -4, gap 4+2l/24+l",
+                       "form": "ksw_extd2 global with CIGAR"},
+            "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": nthreads, "kind": "reference",
+                             "sample": f"pairs of the workload in seeded random order, {budget:.1f} s per step, "
+                                       f"ksw_extd2_{ref.isa} from the reference sources"},
+            "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline(ps, budget):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle
+    ref = oracle.Reference()
+    rng = np.random.default_rng(54321)
+    order = rng.permutation(len(ps))
+    qs = [ps.queries[i].tobytes() for i in order]
+    ts = [ps.targets[i].tobytes() for i in order]
+    nthreads = os.cpu_count() or 1
+    r = ref.ksw_batch(qs, ts, oracle.anchorwave_matrix(-4), 4, 2, 24, 1, nthreads=nthreads,
+                      time_budget_s=budget)
+    done_idx = [i for i in range(len(qs)) if r["hash"][i] != 0]
+    cells = sum(len(qs[i]) * len(ts[i]) for i in done_idx)
+    return {"value": cells / r["seconds"] / 1e9, "unit": "GCUPS", "cores": nthreads, "kind": "reference",
+            "pairs_per_s": len(done_idx) / r["seconds"],
+            "sample": f"{len(done_idx)} pairs of the workload in seeded random order within {budget:.0f} s, "
+                      f"ksw_extd2_{ref.isa} compiled from the reference sources, {nthreads} threads"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    rank, world, local, pg = dist_init(args.gpus)
+    import numpy as np
+
+    from anchorwave_b200 import _lib, ksw2
+    ps = workload(args, rank)
+    mat = ksw2.anchorwave_matrix(-4)
+    cells = ps.cells()
+    n = len(ps)
+
+    plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1)
+    plan.upload()
+    st = plan.stats()
+    for _ in range(args.warmup):
+        plan.execute()
+    int_peak = _lib.lib.aw_int32_peak_ops()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(pg)
+    step_ms, dp_ms, bt_ms = [], [], []
+    for _ in range(args.steps):
+        step_ms.append(plan.execute())
+        d, b = plan.timing()
+        dp_ms.append(d)
+        bt_ms.append(b)
+    barrier(pg)
+    clocks = sampler.stop()
+    res_dev = plan.download()
+    total_ms = max_over_ranks(pg, float(sum(step_ms)))
+    ms_per_step = total_ms / args.steps
+    value = world * cells / (ms_per_step * 1e-3) / 1e9
+    pairs_per_s = world * n / (ms_per_step * 1e-3)
+    launches = plan.stats()["launches"]
+    plan.close()
+
+    # e2e through the public C-ABI call with host buffers
+    for _ in range(1):
+        ksw2.ksw_extd2_batch(ps.queries, ps.targets, mat, 4, 2, 24, 1)
+    barrier(pg)
+    e2e_s = []
+    res_e2e = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res_e2e = ksw2.ksw_extd2_batch(ps.queries, ps.targets, mat, 4, 2, 24, 1)
+        e2e_s.append(time.perf_counter() - t0)
+    barrier(pg)
+    e2e_step = max_over_ranks(pg, float(np.mean(e2e_s)))
+    identical = all(a.key() == b.key() for a, b in zip(res_dev, res_e2e))
+    h2d = int(sum(len(q) for q in ps.queries) + sum(len(t) for t in ps.targets) + n * 48 + n * 4)
+    d2h = int(n * 48 + sum(r.n_cigar for r in res_e2e) * 4)
+
+    # plain per-call GPU form on a sample of the same workload
+    rng = np.random.default_rng(777)
+    sample = rng.choice(n, size=min(args.plain_sample, n), replace=False)
+    ksw2.ksw_extd2(ps.queries[sample[0]], ps.targets[sample[0]], mat, 4, 2, 24, 1)
+    lat, pc_cells = [], 0
+    for i in sample:
+        t0 = time.perf_counter()
+        ksw2.ksw_extd2(ps.queries[i], ps.targets[i], mat, 4, 2, 24, 1)
+        lat.append(time.perf_counter() - t0)
+        pc_cells += len(ps.queries[i]) * len(ps.targets[i])
+    plain = {"gcups": pc_cells / sum(lat) / 1e9, "pairs_per_s": len(lat) / sum(lat),
+             "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
+             "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)), "sample_pairs": len(lat)}
+
+    if rank != 0:
+        barrier(pg)
+        return 0
+
+    hbm_peak, hbm_kind = load_peaks()
+    dp_mean = float(np.mean(dp_ms))
+    achieved_ops = cells * OPS_PER_CELL_CIGAR / (dp_mean * 1e-3)
+    tb_gbs = st["tb_bytes"] / (dp_mean * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8",
+        "data": "synthetic (seeded; stands in for B73/Mo17 intervals)",
+        "pairs_per_s": pairs_per_s,
+        "config": {"workload": ps.name, "pairs": n, "cells": cells, "scoring": "match 0, mismatch -4, gap 4+2l/24+l",
+                   "form": "ksw_extd2 global with CIGAR", "parallelism": f"replicas x{world}",
+                   "l2": f"each step writes {st['tb_bytes'] / 1e9:.0f} GB of traceback, far above the 126 MB L2",
+                   "waves": st["waves"]},
+        "latency_ms": {"batch_step_p50": float(np.percentile(step_ms, 50)),
+                       "batch_step_p99": float(np.percentile(step_ms, 99)),
+                       "plain_per_call_p50": plain["latency_ms_p50"], "plain_per_call_p99": plain["latency_ms_p99"]},
+        "plain_per_call": plain,
+        "batched_vs_plain_pairs_per_s": pairs_per_s / world / plain["pairs_per_s"],
+        "phase_ms": {"dp": dp_mean, "traceback": float(np.mean(bt_ms))},
+        "roofline": {"bound": "int32", "achieved": achieved_ops / 1e12, "peak": int_peak / 1e12, "unit": "TOPS",
+                     "frac": achieved_ops / int_peak if int_peak else None, "traffic": None,
+                     "peak_source": "aw_int32_peak_ops() live microbenchmark (add/max/min/xor chains)",
+                     "ops_per_cell": OPS_PER_CELL_CIGAR,
+                     "hbm_store": {"achieved": tb_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": tb_gbs / hbm_peak,
+                                   "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_kind})"}},
+        "e2e": {"value": world * cells / e2e_step / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "pairs_per_s": world * n / e2e_step,
+                "results_identical_to_device_path": identical},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(ps, args.cpu_budget)
+        except FileNotFoundError as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line))
+    barrier(pg)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

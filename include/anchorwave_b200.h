@@ -89,8 +89,9 @@ int aw_ksw_plan_download(aw_ksw_plan_t *plan, ksw_extz_t *ez);
 /* Device-side statistics of the plan: cells, traceback bytes, waves, launches. */
 int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_bytes, int *waves,
                       int *launches_per_execute);
-/* Mean CUDA-event time (ms) of the plan's DP kernel launches in the last execute. */
-float aw_ksw_plan_dp_ms(const aw_ksw_plan_t *plan);
+/* CUDA-event times (ms) of the last execute, summed over waves: the DP phase (the
+ * concurrent strip-kernel launches) and the traceback phase (backtrack kernel). */
+int aw_ksw_plan_timing(const aw_ksw_plan_t *plan, float *dp_ms, float *bt_ms);
 void aw_ksw_plan_free(aw_ksw_plan_t *plan);
 
 /* ---- configuration and diagnostics ------------------------------------------ */
