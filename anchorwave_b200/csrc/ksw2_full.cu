@@ -247,7 +247,9 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
                 if (lane == 31 && s + 1 < nstrip) {
                     const int jj = k - 31;
                     if (jj >= 0 && ((jj & 31) == 31 || jj == qlen - 1)) {
-                        __threadfence_block();
+                        // the consumer reads these rows from L2 (ld.cg), so they must be
+                        // visible at device scope before the row count is published
+                        __threadfence();
                         cuda::atomic_ref<int, cuda::thread_scope_block> pw(prog[wg]);
                         pw.store(s * (qlen + 1) + jj + 1, cuda::memory_order_release);
                     }
