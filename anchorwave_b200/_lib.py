@@ -27,7 +27,7 @@ EXPORTS = [
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_last_error", "aw_device_count",
-    "aw_int32_peak_ops",
+    "aw_int32_peak_ops", "aw_ksw_extd2_device_noalloc",
 ]
 
 
@@ -67,6 +67,8 @@ def _load():
     lib.aw_device_count.restype = i32
     lib.aw_int32_peak_ops.argtypes = []
     lib.aw_int32_peak_ops.restype = C.c_double
+    lib.aw_ksw_extd2_device_noalloc.argtypes = [i32, vp, i32, vp, i8, vp, i8, i8, i8, i8, i32, vp, vp, i32, vp]
+    lib.aw_ksw_extd2_device_noalloc.restype = i32
     for name in EXPORTS:
         getattr(lib, name)  # raises AttributeError if a declared symbol is missing
     return lib

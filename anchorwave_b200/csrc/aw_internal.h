@@ -99,6 +99,10 @@ struct DevBuf {
 
 void set_error(const char *msg);
 
+// Strip-path parameter check + score table (ksw2_api.cu).
+int full_path_params(int qlen, int tlen, int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2,
+                     int8_t e2, int flag, KswScore *S);
+
 // Launchers (ksw2_full.cu).
 int ksw_full_occupancy(int flag, int warps_per_pair, int groups_per_cta);
 cudaError_t launch_ksw_full(const KswFullArgs &a, int flag, int warps_per_pair,

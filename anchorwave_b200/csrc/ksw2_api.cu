@@ -694,3 +694,20 @@ void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tle
 }
 
 }  // extern "C"
+
+namespace aw {
+// Parameter checks and score table of the full-matrix strip path, for callers
+// outside this file.  Returns AW_OK when (qlen, tlen, parameters, flag) can run
+// on the strip kernel, 1 when ksw_extd2 would return at once without any DP
+// (the ksw2_extd2_sse.c:81/:105 early exits), AW_E_UNSUPPORTED otherwise.
+int full_path_params(int qlen, int tlen, int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2,
+                     int8_t e2, int flag, KswScore *S) {
+    if (m <= 1 || qlen <= 0 || tlen <= 0) return 1;
+    Params P;
+    if (!make_params(m, mat, q, e, q2, e2, -1, 0, flag, P)) return AW_E_UNSUPPORTED;
+    if (P.early_return) return 1;
+    if (!full_path_ok(P, qlen, tlen, -1)) return AW_E_UNSUPPORTED;
+    *S = make_score(P);
+    return AW_OK;
+}
+}  // namespace aw

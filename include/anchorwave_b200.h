@@ -94,6 +94,43 @@ int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_byt
 int aw_ksw_plan_timing(const aw_ksw_plan_t *plan, float *dp_ms, float *bt_ms);
 void aw_ksw_plan_free(aw_ksw_plan_t *plan);
 
+/* ---- allocation-free entry (no counterpart in the reference) ----------------------- */
+
+/* Scalar ksw_extz_t fields as written to device memory by the entry below. */
+typedef struct {
+    int32_t score, max, max_q, max_t, mqe, mqe_t, mte, mte_q;
+    int32_t n_cigar, zdropped, reach_end, stopped;
+} aw_ksw_result_t;
+
+/* Size of the fixed device scratch array behind aw_ksw_extd2_device_noalloc. */
+#define AW_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/*
+ * Full-matrix global ksw_extd2 (w = -1, no z-drop) of one pair, for callers that
+ * must not allocate device memory at call time: a process whose device memory is
+ * entirely reserved by its own caching allocator, or a latency-critical loop that
+ * cannot take the implicit synchronisation of cudaMalloc/cudaFree.  This entry
+ * point has no counterpart in the reference.  All buffers are the caller's device
+ * memory: d_query/d_target hold 0..m-1 codes, *d_result receives the scalar
+ * fields and d_cigar (cigar_capacity >= qlen + tlen words; may be NULL with
+ * KSW_EZ_SCORE_ONLY) the CIGAR, both exactly as ksw_extd2_gpu would produce.
+ * mat stays in host memory.  Work is enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream); the call returns without waiting.
+ * Scratch comes from one fixed __device__ array of AW_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until exit; pairs whose traceback and
+ * strip-boundary columns do not fit it (about 5,600 x 5,600 cells) are rejected
+ * with AW_E_NOMEM.  Calls share that array: calls whose GPU work overlaps race
+ * and must be serialised by the caller.  The first call on a device resolves the
+ * array's address (cudaGetSymbolAddress), so make it before any stream capture.
+ * Flags beyond SCORE_ONLY / RIGHT / GENERIC_SC / REV_CIGAR / SEMIGLOBAL_END, and
+ * parameters outside the strip kernel's exact int8 envelope, return
+ * AW_E_UNSUPPORTED.  Returns AW_OK or a negative AW_E* code (aw_last_error()).
+ */
+int aw_ksw_extd2_device_noalloc(int qlen, const uint8_t *d_query, int tlen, const uint8_t *d_target,
+                                int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2,
+                                int flag, aw_ksw_result_t *d_result, uint32_t *d_cigar,
+                                int cigar_capacity, void *stream);
+
 /* ---- configuration and diagnostics ------------------------------------------ */
 
 /* HBM budget (bytes) for traceback arenas per host thread; mirrors the -M
