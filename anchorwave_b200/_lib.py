@@ -28,13 +28,22 @@ EXPORTS = [
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops", "aw_ksw_extd2_device_noalloc",
+    "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
+    "wavefront_align_batch_gpu",
 ]
 
 
-def _load():
-    if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing; build it with `python -m anchorwave_b200.build`")
-    lib = C.CDLL(LIB_PATH)
+class WfaAttr(C.Structure):
+    """wavefront_gpu_attr_t (include/anchorwave_b200.h)."""
+    _fields_ = [("mismatch", C.c_int), ("gap_opening1", C.c_int), ("gap_extension1", C.c_int),
+                ("gap_opening2", C.c_int), ("gap_extension2", C.c_int), ("singletrack", C.c_int),
+                ("max_memory_abort", C.c_int64)]
+
+
+def _load(path: str = LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing; build it with `python -m anchorwave_b200.build`")
+    lib = C.CDLL(path)
     vp, i8, i32, i64 = C.c_void_p, C.c_int8, C.c_int, C.c_int64
     ksw_args = [vp, i32, vp, i32, vp, i8, vp, i8, i8, i8, i8, i32, i32, i32, i32, C.POINTER(KswExtz)]
     lib.ksw_extd2_gpu.argtypes = ksw_args
@@ -69,6 +78,16 @@ def _load():
     lib.aw_int32_peak_ops.restype = C.c_double
     lib.aw_ksw_extd2_device_noalloc.argtypes = [i32, vp, i32, vp, i8, vp, i8, i8, i8, i8, i32, vp, vp, i32, vp]
     lib.aw_ksw_extd2_device_noalloc.restype = i32
+    lib.wavefront_aligner_new_gpu.argtypes = [C.POINTER(WfaAttr)]
+    lib.wavefront_aligner_new_gpu.restype = vp
+    lib.wavefront_aligner_delete_gpu.argtypes = [vp]
+    lib.wavefront_aligner_delete_gpu.restype = None
+    lib.wavefront_align_gpu.argtypes = [vp, C.c_char_p, i32, C.c_char_p, i32]
+    lib.wavefront_align_gpu.restype = i32
+    lib.wavefront_gpu_cigar.argtypes = [vp, C.POINTER(C.c_char_p), C.POINTER(i32), C.POINTER(i32)]
+    lib.wavefront_gpu_cigar.restype = i32
+    lib.wavefront_align_batch_gpu.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, C.POINTER(C.c_float)]
+    lib.wavefront_align_batch_gpu.restype = i32
     for name in EXPORTS:
         getattr(lib, name)  # raises AttributeError if a declared symbol is missing
     return lib

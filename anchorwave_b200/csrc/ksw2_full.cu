@@ -66,11 +66,43 @@ __device__ __forceinline__ void group_sync(int g, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(nthreads) : "memory");
 }
 
+#ifndef AW_CELL_DPX
+#define AW_CELL_DPX 1
+#endif
+
 template <bool CIGAR, bool RIGHT>
 __device__ __forceinline__ void cell(int s, int &xs, int &vs, int &x2s, int &ut, int &yt, int &y2t,
                                      int &d, const KswScore &S) {
     int a = xs + vs, b = yt + ut, a2 = x2s + vs, b2 = y2t + ut;
     int z = s;
+#if AW_CELL_DPX
+    // Arg-max chain with the reference's tie rules, one DPX max+predicate per step:
+    // left-aligned takes a candidate only if strictly greater (ksw2_extd2_sse.c:244-251),
+    // right-aligned also on equality (:291-298).
+    bool p;
+    if (!CIGAR) {
+        z = __vimax3_s32(z, a, b);
+        z = __vimax3_s32(z, a2, b2);
+    } else if (!RIGHT) {
+        z = __vibmax_s32(z, a, &p);  // p = z >= a
+        d = p ? 0 : 1;
+        z = __vibmax_s32(z, b, &p);
+        d = p ? d : 2;
+        z = __vibmax_s32(z, a2, &p);
+        d = p ? d : 3;
+        z = __vibmax_s32(z, b2, &p);
+        d = p ? d : 4;
+    } else {
+        z = __vibmax_s32(a, z, &p);  // p = a >= z
+        d = p ? 1 : 0;
+        z = __vibmax_s32(b, z, &p);
+        d = p ? 2 : d;
+        z = __vibmax_s32(a2, z, &p);
+        d = p ? 3 : d;
+        z = __vibmax_s32(b2, z, &p);
+        d = p ? 4 : d;
+    }
+#else
     if (!CIGAR) {
         z = max(max(max(z, a), max(b, a2)), b2);
     } else if (!RIGHT) {
@@ -92,8 +124,29 @@ __device__ __forceinline__ void cell(int s, int &xs, int &vs, int &x2s, int &ut,
         d = z > b2 ? d : 4;
         z = max(z, b2);
     }
+#endif
     z = min(z, S.mch);
     const int un = z - vs, vn = z - ut;
+#if AW_CELL_DPX >= 2
+    if (!(CIGAR && RIGHT)) {
+        // x' = max(a - z + q, 0) - (q + e) = max(a + (-e - z), -(q + e)): one add+max each
+        const int nez = -S.e - z, nez2 = -S.e2 - z;
+        xs = __viaddmax_s32(a, nez, -S.qe);
+        yt = __viaddmax_s32(b, nez, -S.qe);
+        x2s = __viaddmax_s32(a2, nez2, -S.qe2);
+        y2t = __viaddmax_s32(b2, nez2, -S.qe2);
+        if (CIGAR) {
+            // continuation bit (a - z + q > 0) == (x' + q + e > 0) == min(x' + q + e, 1)
+            d += 0x08 * __viaddmin_s32(xs, S.qe, 1);
+            d += 0x10 * __viaddmin_s32(yt, S.qe, 1);
+            d += 0x20 * __viaddmin_s32(x2s, S.qe2, 1);
+            d += 0x40 * __viaddmin_s32(y2t, S.qe2, 1);
+        }
+        ut = un;
+        vs = vn;
+        return;
+    }
+#endif
     a = a - z + S.q;
     b = b - z + S.q;
     a2 = a2 - z + S.q2;

@@ -1,0 +1,482 @@
+// Gap-affine-2p end-to-end WFA (WFA2-lib as AnchorWave configures it:
+// src/myImportandFunction/WfaAlignment.cpp:143-170) on sm_100a.
+//
+// One warp per pair; the lanes cover the diagonals of a wavefront.  Per score s:
+//   * extend M[s] (wavefront/wavefront_extend.c:86-121): each lane advances its
+//     diagonal by comparing 8 bytes of pattern and text at a time (one XOR and
+//     __ffsll per 8 bases); sentinels after each sequence ('!' pattern, '?' text,
+//     wavefront/wavefront_sequences.c:37-39) stop the run;
+//   * end-to-end check on diagonal tlen-plen (wavefront/wavefront_termination.c:37-60);
+//   * compute s+1 from M[s-x], M[s-o1-e1], I1/D1[s-e1], M[s-o2-e2], I2/D2[s-e2]
+//     (wavefront/wavefront_compute_affine2p.c:45-106) over the limits of
+//     wavefront/wavefront_compute.c:56-105 (a missing input counts as the null
+//     wavefront lo=1, hi=-1), allocating I/D outputs only when one of their
+//     inputs exists (:459-572), then trimming out-of-matrix ends (:654-690).
+// Values outside a wavefront's trimmed [lo, hi] read as NULL, which is what the
+// reference's NULL end padding gives.  Standard mode retains every component of
+// every score for the piggyback backtrace (wavefront/wavefront_backtrace.c:321-530);
+// Singletrack keeps only M and recycles I/D through a ring of max(e1,e2)+1 slots,
+// then reconstructs the path from M (:587-762).
+//
+// Memory: per-score headers and wavefront arrays come from one device pool by a
+// bump allocator (atomicAdd, 256 KiB chunks).  A pair that finds the pool empty
+// stops with WFA_RETRY and the host re-runs it in a later round with a fresh pool.
+#include "aw_internal.h"
+#include "wfa_internal.h"
+
+namespace aw {
+namespace {
+
+constexpr int32_t WF_NULL = INT32_MIN / 2;
+constexpr int HDR_CHUNK = 256;               // scores per header chunk
+constexpr int64_t DATA_CHUNK = 256 << 10;    // bytes per data chunk
+
+struct CompHdr {
+    int32_t lo, hi, base, pad;
+    int64_t off;  // byte offset of offsets[base] in the pool
+};
+struct ScoreHdr {
+    CompHdr c[5];  // M, I1, D1, I2, D2
+};
+enum { CM = 0, CI1 = 1, CD1 = 2, CI2 = 3, CD2 = 4 };
+
+struct Alloc {
+    int64_t cur, end;
+    bool ok;
+};
+
+__device__ __forceinline__ int64_t pool_grab(const WfaArgs &A, int64_t bytes) {
+    const unsigned long long b = atomicAdd(A.pool_head, (unsigned long long)bytes);
+    if ((int64_t)(b + bytes) > A.pool_bytes) return -1;
+    return (int64_t)b;
+}
+
+// Lane-0 bump allocation inside the warp's current chunk; broadcast to the warp.
+__device__ int64_t warp_alloc(const WfaArgs &A, Alloc &al, int64_t bytes, int lane) {
+    bytes = (bytes + 15) & ~(int64_t)15;
+    int64_t r = -1;
+    if (lane == 0) {
+        if (al.ok) {
+            if (al.cur + bytes > al.end) {
+                const int64_t sz = bytes > DATA_CHUNK ? bytes : DATA_CHUNK;
+                const int64_t b = pool_grab(A, sz);
+                if (b < 0) al.ok = false;
+                else al.cur = b, al.end = b + sz;
+            }
+            if (al.ok) {
+                r = al.cur;
+                al.cur += bytes;
+            }
+        }
+    }
+    r = __shfl_sync(0xffffffffu, r, 0);
+    al.ok = __shfl_sync(0xffffffffu, al.ok ? 1 : 0, 0);
+    al.cur = __shfl_sync(0xffffffffu, al.cur, 0);
+    al.end = __shfl_sync(0xffffffffu, al.end, 0);
+    return r;
+}
+
+__device__ __forceinline__ ScoreHdr *hdr_ptr(const WfaArgs &A, const int64_t *ctab, int s) {
+    return (ScoreHdr *)(A.pool + ctab[s / HDR_CHUNK]) + (s % HDR_CHUNK);
+}
+
+__device__ __forceinline__ int32_t getv(const WfaArgs &A, const CompHdr &h, int k) {
+    if (k < h.lo || k > h.hi) return WF_NULL;
+    return ((const int32_t *)(A.pool + h.off))[k - h.base];
+}
+
+__device__ __forceinline__ uint64_t load8(const uint8_t *base, int64_t pos) {
+    const uintptr_t a = (uintptr_t)(base + pos);
+    const uint64_t *p = (const uint64_t *)(a & ~(uintptr_t)7);
+    const int sh = (int)(a & 7) * 8;
+    const uint64_t lo = p[0];
+    if (!sh) return lo;
+    return (lo >> sh) | (p[1] << (64 - sh));
+}
+
+__device__ __forceinline__ bool in_matrix(int32_t o, int k, int plen, int tlen) {
+    return (uint32_t)o <= (uint32_t)tlen && (uint32_t)(o - k) <= (uint32_t)plen;
+}
+
+// Trim [lo, hi] of one component (wavefront/wavefront_compute.c:654-690), warp-parallel.
+__device__ void warp_trim(const int32_t *d, int base, int &lo, int &hi, int plen, int tlen, int lane) {
+    int nh = lo - 1;
+    for (int top = hi; top >= lo; top -= 32) {
+        const int k = top - lane;
+        const bool ok = k >= lo && in_matrix(d[k - base], k, plen, tlen);
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (b) {
+            nh = top - (__ffs(b) - 1);
+            break;
+        }
+    }
+    int nl = nh + 1;
+    for (int bot = lo; bot <= nh; bot += 32) {
+        const int k = bot + lane;
+        const bool ok = k <= nh && in_matrix(d[k - base], k, plen, tlen);
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (b) {
+            nl = bot + (__ffs(b) - 1);
+            break;
+        }
+    }
+    lo = nl, hi = nh;
+}
+
+__device__ __forceinline__ int64_t pb(int32_t o, int t) {
+    return (int64_t)((((uint64_t)(int64_t)o) << 4) | (uint64_t)t);
+}
+
+struct OpsWriter {
+    char *buf;
+    int n, cap;
+    bool ok;
+    __device__ void put(char c, int times) {
+        for (int i = 0; i < times; ++i) {
+            if (n >= cap) { ok = false; return; }
+            buf[n++] = c;
+        }
+    }
+};
+
+__global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
+    const int lane = threadIdx.x & 31;
+    const WfaPen P = A.pen;
+    for (;;) {
+        int pi = 0;
+        if (lane == 0) pi = atomicAdd(A.queue, 1);
+        pi = __shfl_sync(0xffffffffu, pi, 0);
+        if (pi >= A.n) break;
+        const int idx = A.order[pi];
+        const WfaPairDev PR = A.pairs[idx];
+        const int plen = PR.plen, tlen = PR.tlen;
+        const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
+        int64_t *ctab = A.ctab + PR.ctab_off;
+        Alloc al{0, 0, true};
+        const int64_t pool_start = -1;
+        (void)pool_start;
+        int status = 0, end_score = -1;
+        // Singletrack ring for I/D: R slots x 4 components x cap offsets
+        const int R = (P.e1 > P.e2 ? P.e1 : P.e2) + 1;
+        const int ring_cap = plen + tlen + 8;
+        int64_t ring = -1;
+        if (A.singletrack) {
+            ring = warp_alloc(A, al, (int64_t)R * 4 * ring_cap * 4, lane);
+            if (ring < 0) status = WFA_RETRY;
+        }
+        // score 0
+        int64_t h0 = -1;
+        if (status == 0) {
+            h0 = warp_alloc(A, al, (int64_t)sizeof(ScoreHdr) * HDR_CHUNK, lane);
+            if (h0 < 0) status = WFA_RETRY;
+        }
+        int64_t d0 = -1;
+        if (status == 0) {
+            d0 = warp_alloc(A, al, 16, lane);
+            if (d0 < 0) status = WFA_RETRY;
+        }
+        if (status == 0 && lane == 0) {
+            ctab[0] = h0;
+            ScoreHdr *H = (ScoreHdr *)(A.pool + h0);
+            for (int c = 0; c < 5; ++c) H->c[c] = CompHdr{1, -1, 0, 0, 0};
+            H->c[CM] = CompHdr{0, 0, 0, 0, d0};
+            *(int32_t *)(A.pool + d0) = 0;
+        }
+        __syncwarp();
+        const int k_end = tlen - plen;
+        int s = 0, num_null = 0;
+        const int smax = PR.ctab_cap * HDR_CHUNK - 1;
+        while (status == 0) {
+            // ---- extend M[s] and check the end
+            {
+                const ScoreHdr *H = hdr_ptr(A, ctab, s);
+                const CompHdr m = H->c[CM];
+                if (m.lo <= m.hi) {
+                    int32_t *d = (int32_t *)(A.pool + m.off);
+                    for (int k = m.lo + lane; k <= m.hi; k += 32) {
+                        const int32_t o = d[k - m.base];
+                        if (o == WF_NULL) continue;
+                        int64_t v = (int64_t)o - k, h = o;
+                        for (;;) {
+                            const uint64_t x = load8(pat, v) ^ load8(txt, h);
+                            if (x) {
+                                const int nb = (__ffsll((long long)x) - 1) >> 3;
+                                v += nb, h += nb;
+                                break;
+                            }
+                            v += 8, h += 8;
+                        }
+                        d[k - m.base] = (int32_t)h;
+                    }
+                    __syncwarp();
+                    if (m.lo <= k_end && k_end <= m.hi && d[k_end - m.base] >= tlen) {
+                        end_score = s;
+                        break;
+                    }
+                } else if (num_null > A.max_score_scope) {
+                    status = -3;  // end unreachable (cannot happen end-to-end without heuristics)
+                    break;
+                }
+            }
+            // ---- compute s+1
+            ++s;
+            if (s > smax) {
+                status = WFA_OVERFLOW;
+                break;
+            }
+            if (s % HDR_CHUNK == 0) {
+                const int64_t hb = warp_alloc(A, al, (int64_t)sizeof(ScoreHdr) * HDR_CHUNK, lane);
+                if (hb < 0) {
+                    status = WFA_RETRY;
+                    break;
+                }
+                if (lane == 0) ctab[s / HDR_CHUNK] = hb;
+                __syncwarp();
+            }
+            ScoreHdr *OH = hdr_ptr(A, ctab, s);
+            const CompHdr NUL{1, -1, 0, 0, 0};
+            const int sm = s - P.x, so1 = s - P.o1 - P.e1, se1 = s - P.e1, so2 = s - P.o2 - P.e2, se2 = s - P.e2;
+            const CompHdr m_misms = sm >= 0 ? hdr_ptr(A, ctab, sm)->c[CM] : NUL;
+            const CompHdr m_open1 = so1 >= 0 ? hdr_ptr(A, ctab, so1)->c[CM] : NUL;
+            const CompHdr i1 = se1 >= 0 ? hdr_ptr(A, ctab, se1)->c[CI1] : NUL;
+            const CompHdr d1 = se1 >= 0 ? hdr_ptr(A, ctab, se1)->c[CD1] : NUL;
+            const CompHdr m_open2 = so2 >= 0 ? hdr_ptr(A, ctab, so2)->c[CM] : NUL;
+            const CompHdr i2 = se2 >= 0 ? hdr_ptr(A, ctab, se2)->c[CI2] : NUL;
+            const CompHdr d2 = se2 >= 0 ? hdr_ptr(A, ctab, se2)->c[CD2] : NUL;
+            const bool n_mm = m_misms.lo > m_misms.hi, n_o1 = m_open1.lo > m_open1.hi, n_i1 = i1.lo > i1.hi,
+                       n_d1 = d1.lo > d1.hi, n_o2 = m_open2.lo > m_open2.hi, n_i2 = i2.lo > i2.hi,
+                       n_d2 = d2.lo > d2.hi;
+            if (n_mm && n_o1 && n_i1 && n_d1 && n_o2 && n_i2 && n_d2) {
+                if (lane == 0)
+                    for (int c = 0; c < 5; ++c) OH->c[c] = NUL;
+                __syncwarp();
+                ++num_null;
+                continue;
+            }
+            num_null = 0;
+            // limits (null inputs contribute lo=1, hi=-1)
+            int lo = m_misms.lo, hi = m_misms.hi;
+            lo = min(lo, m_open1.lo - 1), hi = max(hi, m_open1.hi + 1);
+            lo = min(lo, i1.lo + 1), hi = max(hi, i1.hi + 1);
+            lo = min(lo, d1.lo - 1), hi = max(hi, d1.hi - 1);
+            lo = min(lo, m_open2.lo - 1), hi = max(hi, m_open2.hi + 1);
+            lo = min(lo, i2.lo + 1), hi = max(hi, i2.hi + 1);
+            lo = min(lo, d2.lo - 1), hi = max(hi, d2.hi - 1);
+            const bool a_i1 = !n_o1 || !n_i1, a_d1 = !n_o1 || !n_d1, a_i2 = !n_o2 || !n_i2, a_d2 = !n_o2 || !n_d2;
+            const int width = hi - lo + 1;
+            CompHdr out[5];
+            for (int c = 0; c < 5; ++c) out[c] = NUL;
+            const bool alloc_c[5] = {true, a_i1, a_d1, a_i2, a_d2};
+            const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
+            int nstore = 1;
+            if (!A.singletrack) nstore += (int)a_i1 + (int)a_d1 + (int)a_i2 + (int)a_d2;
+            if (A.singletrack && width > ring_cap) {
+                status = WFA_OVERFLOW;
+                break;
+            }
+            const int64_t blk = warp_alloc(A, al, wb * nstore, lane);
+            if (blk < 0) {
+                status = WFA_RETRY;
+                break;
+            }
+            {
+                int64_t o = blk;
+                for (int c = 0; c < 5; ++c) {
+                    if (!alloc_c[c]) continue;
+                    int64_t place;
+                    if (c == CM || !A.singletrack) place = o, o += wb;
+                    else place = ring + ((int64_t)((s % R) * 4 + (c - 1)) * ring_cap) * 4;
+                    out[c] = CompHdr{lo, hi, lo, 0, place};
+                }
+            }
+            int32_t *oM = (int32_t *)(A.pool + out[CM].off);
+            int32_t *oI1 = a_i1 ? (int32_t *)(A.pool + out[CI1].off) : nullptr;
+            int32_t *oD1 = a_d1 ? (int32_t *)(A.pool + out[CD1].off) : nullptr;
+            int32_t *oI2 = a_i2 ? (int32_t *)(A.pool + out[CI2].off) : nullptr;
+            int32_t *oD2 = a_d2 ? (int32_t *)(A.pool + out[CD2].off) : nullptr;
+            for (int k = lo + lane; k <= hi; k += 32) {
+                const int32_t ins1 = max(getv(A, m_open1, k - 1), getv(A, i1, k - 1)) + 1;
+                const int32_t ins2 = max(getv(A, m_open2, k - 1), getv(A, i2, k - 1)) + 1;
+                const int32_t del1 = max(getv(A, m_open1, k + 1), getv(A, d1, k + 1));
+                const int32_t del2 = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
+                const int32_t misms = getv(A, m_misms, k) + 1;
+                int32_t best = max(max(del1, del2), max(misms, max(ins1, ins2)));
+                if (!in_matrix(best, k, plen, tlen)) best = WF_NULL;
+                oM[k - lo] = best;
+                if (oI1) oI1[k - lo] = ins1;
+                if (oD1) oD1[k - lo] = del1;
+                if (oI2) oI2[k - lo] = ins2;
+                if (oD2) oD2[k - lo] = del2;
+            }
+            __syncwarp();
+            for (int c = 0; c < 5; ++c) {
+                if (!alloc_c[c]) continue;
+                int tl = out[c].lo, th = out[c].hi;
+                warp_trim((const int32_t *)(A.pool + out[c].off), out[c].base, tl, th, plen, tlen, lane);
+                out[c].lo = tl, out[c].hi = th;
+            }
+            if (lane == 0)
+                for (int c = 0; c < 5; ++c) OH->c[c] = out[c];
+            __syncwarp();
+        }
+        // ---- backtrace (lane 0)
+        if (lane == 0) {
+            WfaOutDev o;
+            o.status = status, o.score = 0, o.n_ops = 0, o.final_s = s;
+            o.mem_bytes = 0;
+            if (status == 0) {
+                OpsWriter w{A.ops + PR.ops_off, 0, plen + tlen + 8, true};
+                if (!A.singletrack) {
+                    enum { BM = 9, BD2E = 8, BD2O = 7, BD1E = 6, BD1O = 5, BI2E = 4, BI2O = 3, BI1E = 2, BI1O = 1 };
+                    int mt = CM, sc = end_score, k = k_end;
+                    int32_t off = tlen;
+                    int v = off - k, h = off;
+                    const int64_t NEG = pb(WF_NULL, 0);
+                    while (v > 0 && h > 0 && sc > 0) {
+                        const int smm = sc - P.x, sg1 = sc - P.o1 - P.e1, sg2 = sc - P.o2 - P.e2, sx1 = sc - P.e1,
+                                  sx2 = sc - P.e2;
+                        auto G = [&](int scr, int comp, int kk, int add, int t) -> int64_t {
+                            if (scr < 0) return NEG;
+                            const CompHdr hh = hdr_ptr(A, ctab, scr)->c[comp];
+                            return pb(getv(A, hh, kk) + add, t);
+                        };
+                        int64_t mall;
+                        const int64_t i1o = (mt == CM || mt == CI1) ? G(sg1, CM, k - 1, 1, BI1O) : NEG;
+                        const int64_t i1e = (mt == CM || mt == CI1) ? G(sx1, CI1, k - 1, 1, BI1E) : NEG;
+                        const int64_t d1o = (mt == CM || mt == CD1) ? G(sg1, CM, k + 1, 0, BD1O) : NEG;
+                        const int64_t d1e = (mt == CM || mt == CD1) ? G(sx1, CD1, k + 1, 0, BD1E) : NEG;
+                        const int64_t i2o = (mt == CM || mt == CI2) ? G(sg2, CM, k - 1, 1, BI2O) : NEG;
+                        const int64_t i2e = (mt == CM || mt == CI2) ? G(sx2, CI2, k - 1, 1, BI2E) : NEG;
+                        const int64_t d2o = (mt == CM || mt == CD2) ? G(sg2, CM, k + 1, 0, BD2O) : NEG;
+                        const int64_t d2e = (mt == CM || mt == CD2) ? G(sx2, CD2, k + 1, 0, BD2E) : NEG;
+                        if (mt == CM) {
+                            const int64_t misms = G(smm, CM, k, 1, BM);
+                            mall = max(misms, max(max(max(i1o, i1e), max(i2o, i2e)), max(max(d1o, d1e), max(d2o, d2e))));
+                        } else if (mt == CI1) mall = max(i1o, i1e);
+                        else if (mt == CI2) mall = max(i2o, i2e);
+                        else if (mt == CD1) mall = max(d1o, d1e);
+                        else mall = max(d2o, d2e);
+                        if (mall < 0) break;
+                        if (mt == CM) {
+                            const int mo = (int)(mall >> 4);
+                            w.put('M', off - mo);
+                            off = mo;
+                            v = off - k, h = off;
+                            if (v <= 0 || h <= 0) break;
+                        }
+                        const int bt = (int)(mall & 0xf);
+                        switch (bt) {
+                        case BM: sc = smm; mt = CM; break;
+                        case BI1O: sc = sg1; mt = CM; break;
+                        case BI1E: sc = sx1; mt = CI1; break;
+                        case BI2O: sc = sg2; mt = CM; break;
+                        case BI2E: sc = sx2; mt = CI2; break;
+                        case BD1O: sc = sg1; mt = CM; break;
+                        case BD1E: sc = sx1; mt = CD1; break;
+                        case BD2O: sc = sg2; mt = CM; break;
+                        default: sc = sx2; mt = CD2; break;
+                        }
+                        if (bt == BM) w.put('X', 1), --off;
+                        else if (bt <= BI2E) w.put('I', 1), --k, --off;
+                        else w.put('D', 1), ++k;
+                        v = off - k, h = off;
+                    }
+                    if (mt == CM) {
+                        if (v > 0 && h > 0) {
+                            const int nm = v < h ? v : h;
+                            w.put('M', nm);
+                            v -= nm, h -= nm;
+                        }
+                        w.put('D', v > 0 ? v : 0);
+                        w.put('I', h > 0 ? h : 0);
+                    }
+                } else {
+                    int sc = end_score, k = k_end, gl = 0;
+                    bool in_m = true, ok = true;
+                    int32_t off = tlen, off_be = off;
+                    const int64_t maxgap = (int64_t)plen + tlen;
+                    while (sc != 0) {
+                        if (sc < 0 || off < 0) { ok = false; break; }
+                        if (in_m) {
+                            const int v = off - k, h = off;
+                            if (v < 0 || h < 0 || v > plen || h > tlen) { ok = false; break; }
+                            int nm = 0;
+                            while (nm < v && nm < h && pat[v - nm - 1] == txt[h - nm - 1]) ++nm;
+                            off_be = off - nm;
+                            const int ms = sc - P.x;
+                            bool took = false;
+                            if (ms >= 0) {
+                                const CompHdr mh = hdr_ptr(A, ctab, ms)->c[CM];
+                                if (mh.lo <= k && k <= mh.hi &&
+                                    ((const int32_t *)(A.pool + mh.off))[k - mh.base] + 1 == off_be) {
+                                    w.put('M', nm);
+                                    w.put('X', 1);
+                                    off = off_be - 1;
+                                    sc = ms;
+                                    took = true;
+                                }
+                            }
+                            if (!took) in_m = false, gl = 0;
+                            continue;
+                        }
+                        ++gl;
+                        if ((int64_t)gl > maxgap) { ok = false; break; }
+                        const int ki = k - gl, kd = k + gl;
+                        for (int piece = 0; piece < 2; ++piece) {
+                            const int64_t isc = piece == 0 ? (int64_t)sc - P.o1 - (int64_t)gl * P.e1
+                                                           : (int64_t)sc - P.o2 - (int64_t)gl * P.e2;
+                            if (isc < 0 || isc > s) continue;
+                            const CompHdr ih = hdr_ptr(A, ctab, (int)isc)->c[CM];
+                            const int32_t *id = (const int32_t *)(A.pool + ih.off);
+                            if (ih.lo <= ki && ki <= ih.hi && id[ki - ih.base] + gl >= off_be &&
+                                id[ki - ih.base] + gl <= off) {
+                                w.put('M', off - (id[ki - ih.base] + gl));
+                                w.put('I', gl);
+                                k = ki, off = id[ki - ih.base], sc = (int)isc, in_m = true;
+                                break;
+                            }
+                            if (ih.lo <= kd && kd <= ih.hi && id[kd - ih.base] >= off_be && id[kd - ih.base] <= off) {
+                                w.put('M', off - id[kd - ih.base]);
+                                w.put('D', gl);
+                                k = kd, off = id[kd - ih.base], sc = (int)isc, in_m = true;
+                                break;
+                            }
+                        }
+                    }
+                    if (ok && (!in_m || k != 0 || off < 0 || off > plen || off > tlen)) ok = false;
+                    if (ok)
+                        for (int i = 0; i < off; ++i)
+                            if (pat[i] != txt[i]) { ok = false; break; }
+                    if (ok) w.put('M', off);
+                    if (!ok) o.status = WFA_UNATTAINABLE;
+                }
+                if (!w.ok) o.status = WFA_OVERFLOW;
+                if (o.status == 0) {
+                    for (int a = 0, b = w.n - 1; a < b; ++a, --b) {
+                        const char t = w.buf[a];
+                        w.buf[a] = w.buf[b], w.buf[b] = t;
+                    }
+                    o.score = -end_score;
+                    o.n_ops = w.n;
+                }
+            }
+            A.out[idx] = o;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st) {
+    wfa_kernel<<<ctas, 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+int wfa_occupancy() {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_kernel, 128, 0) != cudaSuccess) return 1;
+    return nb;
+}
+
+}  // namespace aw

@@ -1,0 +1,298 @@
+// C-ABI host layer of the WFA kernel: a GPU aligner handle that mirrors
+// wavefront_aligner_new / wavefront_align / wavefront_aligner_delete
+// (WFA2-lib wavefront/wfa.h:129-134, :210-215) with the attributes AnchorWave sets
+// (src/myImportandFunction/WfaAlignment.cpp:143-170), plus a batched entry.
+// One handle per host thread (AnchorWave keeps a thread-local aligner per memory
+// mode, WfaAlignment.cpp:217-221); each handle owns a stream and pooled buffers.
+#include "aw_internal.h"
+#include "wfa_internal.h"
+#include "../../include/anchorwave_b200.h"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace aw;
+
+namespace {
+
+constexpr int HDR_CHUNK = 256;
+constexpr int PAD = 16;  // sentinel bytes after every sequence
+
+struct PinBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr, cap = 0;
+        const size_t want = std::max(n + n / 2, (size_t)4096);
+        const cudaError_t e = cudaMallocHost(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    ~PinBuf() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+int64_t al8(int64_t v) { return (v + 7) & ~(int64_t)7; }
+
+}  // namespace
+
+struct wavefront_aligner_gpu {
+    wavefront_gpu_attr_t attr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DevBuf d_pat, d_txt, d_pairs, d_order, d_pool, d_head, d_ctab, d_ops, d_out, d_queue;
+    PinBuf h_pat, h_txt, h_ops;
+    std::vector<WfaPairDev> pairs;
+    std::vector<WfaOutDev> outs;
+    // single-call result
+    std::string ops;
+    int score = 0;
+    uint64_t mem_used = 0;
+    int sms = 0;
+    float last_ms = 0.f;
+    int last_launches = 0;
+    ~wavefront_aligner_gpu() {
+        d_pat.release(), d_txt.release(), d_pairs.release(), d_order.release(), d_pool.release();
+        d_head.release(), d_ctab.release(), d_ops.release(), d_out.release(), d_queue.release();
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+#define WCUDA(call)                                                         \
+    do {                                                                    \
+        cudaError_t _e = (call);                                            \
+        if (_e != cudaSuccess) {                                            \
+            set_error((std::string(#call) + ": " + cudaGetErrorString(_e)).c_str()); \
+            return AW_E_CUDA;                                               \
+        }                                                                   \
+    } while (0)
+
+static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *pattern, const int *plen,
+                     const char *const *text, const int *tlen) {
+    const wavefront_gpu_attr_t &A = al->attr;
+    al->pairs.assign(n, WfaPairDev{});
+    al->outs.assign(n, WfaOutDev{});
+    int64_t pb = 0, tb = 0, ob = 0, cb = 0;
+    for (int i = 0; i < n; ++i) {
+        WfaPairDev &P = al->pairs[i];
+        const int p = plen[i], t = tlen[i];
+        P.plen = p, P.tlen = t;
+        P.poff = pb, P.toff = tb;
+        pb += al8(p + PAD) + 8, tb += al8(t + PAD) + 8;
+        P.ops_off = ob;
+        ob += (int64_t)p + t + 8;
+        // score bound: all mismatches plus one gap for the length difference
+        // (wavefront/wavefront_components.c:118-124)
+        const int64_t d = std::abs(p - t);
+        const int64_t bound = (int64_t)std::min(p, t) * A.mismatch +
+                              std::max(A.gap_opening1 + d * A.gap_extension1, A.gap_opening2 + d * A.gap_extension2) + 2;
+        P.ctab_cap = (int32_t)((bound + HDR_CHUNK) / HDR_CHUNK + 1);
+        P.ctab_off = cb;
+        cb += P.ctab_cap;
+    }
+    WCUDA(al->h_pat.ensure((size_t)pb + 64));
+    WCUDA(al->h_txt.ensure((size_t)tb + 64));
+    uint8_t *hp = (uint8_t *)al->h_pat.p, *ht = (uint8_t *)al->h_txt.p;
+    for (int i = 0; i < n; ++i) {
+        const WfaPairDev &P = al->pairs[i];
+        if (P.plen > 0) memcpy(hp + P.poff, pattern[i], (size_t)P.plen);
+        memset(hp + P.poff + P.plen, '!', (size_t)(al8(P.plen + PAD) + 8 - P.plen));
+        if (P.tlen > 0) memcpy(ht + P.toff, text[i], (size_t)P.tlen);
+        memset(ht + P.toff + P.tlen, '?', (size_t)(al8(P.tlen + PAD) + 8 - P.tlen));
+    }
+    std::vector<int32_t> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        const int64_t la = (int64_t)plen[a] + tlen[a], lb = (int64_t)plen[b] + tlen[b];
+        return la != lb ? la > lb : a < b;
+    });
+    WCUDA(al->d_pat.ensure((size_t)pb + 64));
+    WCUDA(al->d_txt.ensure((size_t)tb + 64));
+    WCUDA(al->d_pairs.ensure(sizeof(WfaPairDev) * (size_t)n));
+    WCUDA(al->d_order.ensure(sizeof(int32_t) * (size_t)n));
+    WCUDA(al->d_ctab.ensure(8 * (size_t)cb + 64));
+    WCUDA(al->d_ops.ensure((size_t)ob + 64));
+    WCUDA(al->d_out.ensure(sizeof(WfaOutDev) * (size_t)n));
+    WCUDA(al->d_queue.ensure(64));
+    WCUDA(al->d_head.ensure(64));
+    // device pool: half of free memory (capped by max_memory_abort when set)
+    if (al->d_pool.cap == 0) {
+        size_t fr = 0, tot = 0;
+        WCUDA(cudaMemGetInfo(&fr, &tot));
+        int64_t want = (int64_t)(fr * 0.5);
+        if (A.max_memory_abort > 0) want = std::min<int64_t>(want, A.max_memory_abort);
+        want = std::max<int64_t>(want, (int64_t)64 << 20);
+        WCUDA(al->d_pool.ensure((size_t)want));
+    }
+    WCUDA(cudaMemcpyAsync(al->d_pat.p, hp, (size_t)pb, cudaMemcpyHostToDevice, al->st));
+    WCUDA(cudaMemcpyAsync(al->d_txt.p, ht, (size_t)tb, cudaMemcpyHostToDevice, al->st));
+    WCUDA(cudaMemcpyAsync(al->d_pairs.p, al->pairs.data(), sizeof(WfaPairDev) * (size_t)n, cudaMemcpyHostToDevice,
+                          al->st));
+    WfaArgs W;
+    W.pat = al->d_pat.as<uint8_t>(), W.txt = al->d_txt.as<uint8_t>();
+    W.pairs = al->d_pairs.as<WfaPairDev>();
+    W.pool = al->d_pool.as<uint8_t>(), W.pool_bytes = (int64_t)al->d_pool.cap;
+    W.pool_head = al->d_head.as<unsigned long long>();
+    W.ctab = al->d_ctab.as<int64_t>();
+    W.ops = al->d_ops.as<char>();
+    W.out = al->d_out.as<WfaOutDev>();
+    W.queue = al->d_queue.as<int32_t>();
+    W.pen = WfaPen{A.mismatch, A.gap_opening1, A.gap_extension1, A.gap_opening2, A.gap_extension2};
+    W.singletrack = A.singletrack ? 1 : 0;
+    const int scope = std::max(A.gap_opening1 + A.gap_extension1, A.gap_opening2 + A.gap_extension2);
+    W.max_score_scope = std::max(scope, A.mismatch) + 1;
+    const int occ = std::max(1, wfa_occupancy());
+    // Rounds: every round restarts the pool; pairs that found it exhausted run again.
+    // If a round completes nothing, the remaining pairs run one at a time, and a pair
+    // that cannot finish with the whole pool to itself reports WF_STATUS_OOM (the
+    // reference's max-memory abort).
+    std::vector<int32_t> pending = order;
+    float total_ms = 0.f;
+    int launches = 0;
+    bool serial = false;
+    while (!pending.empty()) {
+        std::vector<int32_t> batch = serial ? std::vector<int32_t>{pending[0]} : pending;
+        WCUDA(cudaMemcpyAsync(al->d_order.p, batch.data(), sizeof(int32_t) * batch.size(), cudaMemcpyHostToDevice,
+                              al->st));
+        WCUDA(cudaMemsetAsync(al->d_queue.p, 0, 4, al->st));
+        WCUDA(cudaMemsetAsync(al->d_head.p, 0, 8, al->st));
+        W.order = al->d_order.as<int32_t>();
+        W.n = (int32_t)batch.size();
+        const int ctas = std::min((W.n + 3) / 4, occ * al->sms);
+        WCUDA(cudaEventRecord(al->e0, al->st));
+        WCUDA(launch_wfa(W, ctas, al->st));
+        WCUDA(cudaEventRecord(al->e1, al->st));
+        ++launches;
+        WCUDA(cudaMemcpyAsync(al->outs.data(), al->d_out.p, sizeof(WfaOutDev) * (size_t)n, cudaMemcpyDeviceToHost,
+                              al->st));
+        WCUDA(cudaStreamSynchronize(al->st));
+        float ms = 0.f;
+        WCUDA(cudaEventElapsedTime(&ms, al->e0, al->e1));
+        total_ms += ms;
+        std::vector<int32_t> again;
+        for (int32_t i : batch)
+            if (al->outs[i].status == WFA_RETRY) again.push_back(i);
+        if (serial) {
+            if (!again.empty()) al->outs[pending[0]].status = WFA_OOM;
+            pending.erase(pending.begin());
+        } else if (again.size() == batch.size()) {
+            serial = true;
+        } else {
+            pending.swap(again);
+        }
+    }
+    al->last_ms = total_ms;
+    al->last_launches = launches;
+    return AW_OK;
+}
+
+static int fetch_ops(wavefront_aligner_gpu *al, int n) {
+    int64_t ob = 0;
+    for (int i = 0; i < n; ++i) ob = std::max<int64_t>(ob, al->pairs[i].ops_off + al->pairs[i].plen + al->pairs[i].tlen + 8);
+    WCUDA(al->h_ops.ensure((size_t)ob + 64));
+    WCUDA(cudaMemcpyAsync(al->h_ops.p, al->d_ops.p, (size_t)ob, cudaMemcpyDeviceToHost, al->st));
+    WCUDA(cudaStreamSynchronize(al->st));
+    return AW_OK;
+}
+
+static int public_status(int st) {
+    if (st == WFA_RETRY || st == WFA_OVERFLOW) return WFA_OOM;
+    return st;
+}
+
+extern "C" {
+
+wavefront_aligner_gpu_t *wavefront_aligner_new_gpu(const wavefront_gpu_attr_t *attr) {
+    if (!attr) {
+        set_error("wavefront_aligner_new_gpu: attributes required");
+        return nullptr;
+    }
+    // wavefront/wavefront_penalties.c:141-150
+    if (attr->mismatch <= 0 || attr->gap_opening1 < 0 || attr->gap_extension1 <= 0 || attr->gap_opening2 < 0 ||
+        attr->gap_extension2 <= 0) {
+        set_error("wavefront_aligner_new_gpu: penalties must be X>0, O1>=0, E1>0, O2>=0, E2>0");
+        return nullptr;
+    }
+    wavefront_aligner_gpu *al = new wavefront_aligner_gpu();
+    al->attr = *attr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&al->sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&al->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&al->e0) != cudaSuccess || cudaEventCreate(&al->e1) != cudaSuccess) {
+        set_error("wavefront_aligner_new_gpu: CUDA initialisation failed");
+        delete al;
+        return nullptr;
+    }
+    return al;
+}
+
+void wavefront_aligner_delete_gpu(wavefront_aligner_gpu_t *al) { delete al; }
+
+int wavefront_align_gpu(wavefront_aligner_gpu_t *al, const char *pattern, int pattern_length, const char *text,
+                        int text_length) {
+    if (!al || pattern_length < 0 || text_length < 0 || (pattern_length > 0 && !pattern) ||
+        (text_length > 0 && !text))
+        return AW_E_INVAL;
+    al->ops.clear();
+    al->score = 0;
+    const int rc = run_batch(al, 1, &pattern, &pattern_length, &text, &text_length);
+    if (rc) return rc;
+    const WfaOutDev &o = al->outs[0];
+    if (o.status == WFA_COMPLETED) {
+        if (fetch_ops(al, 1)) return AW_E_CUDA;
+        al->ops.assign((const char *)al->h_ops.p + al->pairs[0].ops_off, (size_t)o.n_ops);
+        al->score = o.score;
+    }
+    return public_status(o.status);
+}
+
+int wavefront_gpu_cigar(const wavefront_aligner_gpu_t *al, const char **operations, int *num_operations,
+                        int *score) {
+    if (!al) return AW_E_INVAL;
+    if (operations) *operations = al->ops.c_str();
+    if (num_operations) *num_operations = (int)al->ops.size();
+    if (score) *score = al->score;
+    return AW_OK;
+}
+
+int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *al, int n, const char *const *pattern,
+                              const int *pattern_length, const char *const *text, const int *text_length,
+                              int *status, int *score, int64_t *ops_offset, int *n_ops, char *ops,
+                              int64_t ops_capacity, float *device_ms) {
+    if (!al || n < 0 || (n > 0 && (!pattern || !pattern_length || !text || !text_length || !status || !score)))
+        return AW_E_INVAL;
+    if (n == 0) return AW_OK;
+    int64_t need = 0;
+    for (int i = 0; i < n; ++i) need += (int64_t)pattern_length[i] + text_length[i];
+    if (ops && ops_capacity < need) {
+        set_error("wavefront_align_batch_gpu: ops buffer needs sum(plen + tlen) bytes");
+        return AW_E_INVAL;
+    }
+    const int rc = run_batch(al, n, pattern, pattern_length, text, text_length);
+    if (rc) return rc;
+    if (device_ms) *device_ms = al->last_ms;
+    if (ops && fetch_ops(al, n)) return AW_E_CUDA;
+    int64_t pos = 0;
+    for (int i = 0; i < n; ++i) {
+        const WfaOutDev &o = al->outs[i];
+        status[i] = public_status(o.status);
+        score[i] = o.status == WFA_COMPLETED ? o.score : 0;
+        const int nops = o.status == WFA_COMPLETED ? o.n_ops : 0;
+        if (n_ops) n_ops[i] = nops;
+        if (ops_offset) ops_offset[i] = pos;
+        if (ops && nops) memcpy(ops + pos, (const char *)al->h_ops.p + al->pairs[i].ops_off, (size_t)nops);
+        pos += nops;
+    }
+    return AW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,52 @@
+// Internal types of the WFA kernel (wfa.cu) and its host layer (wfa_api.cu).
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace aw {
+
+// WF status codes (WFA2-lib wavefront/wfa.h:46-55) plus internal retry/overflow.
+constexpr int WFA_COMPLETED = 0;
+constexpr int WFA_OOM = -200;
+constexpr int WFA_UNATTAINABLE = -300;
+constexpr int WFA_RETRY = -1000;     // device pool exhausted: re-run in a later round
+constexpr int WFA_OVERFLOW = -1001;  // a per-pair bound was exceeded
+
+struct WfaPen {
+    int x, o1, e1, o2, e2;
+};
+
+struct WfaPairDev {
+    int64_t poff, toff;    // padded pattern / text in the sequence arenas (8-byte aligned)
+    int32_t plen, tlen;
+    int64_t ops_off;       // CIGAR operation slot (plen + tlen + 8 chars)
+    int64_t ctab_off;      // header-chunk table (int64 pool offsets), ctab_cap entries
+    int32_t ctab_cap, pad;
+};
+
+struct WfaOutDev {
+    int32_t status, score, n_ops, final_s;
+    int64_t mem_bytes;
+};
+
+struct WfaArgs {
+    const uint8_t *pat, *txt;
+    const WfaPairDev *pairs;
+    const int32_t *order;
+    int32_t n;
+    uint8_t *pool;
+    int64_t pool_bytes;
+    unsigned long long *pool_head;
+    int64_t *ctab;
+    char *ops;
+    WfaOutDev *out;
+    int32_t *queue;
+    WfaPen pen;
+    int singletrack;
+    int max_score_scope;
+};
+
+cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st);
+int wfa_occupancy();
+
+}  // namespace aw

@@ -1,0 +1,127 @@
+"""Host-side mirror of AnchorWave's WFA interface on the B200 WFA kernel.
+
+* :class:`WfaAligner` mirrors the WFA2-lib aligner object AnchorWave caches per thread
+  (wavefront_aligner_new / wavefront_align / wavefront_aligner_delete, WFA2-lib
+  wavefront/wfa.h:129-134, :210-215) with the attributes of
+  src/myImportandFunction/WfaAlignment.cpp:143-170 (match 0, positive penalties, high
+  memory, no heuristic, end to end, full CIGAR, optional Singletrack).
+* :func:`align_with_wfa` mirrors alignWithWfaMode + decodeCigar
+  (WfaAlignment.cpp:223-391): reference is the pattern, query the text; 'M'/'X' consume
+  both, 'I' the query, 'D' the reference; score is the negated penalty.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from ._lib import AwError, WfaAttr, last_error, lib
+
+WF_STATUS_ALG_COMPLETED = 0
+WF_STATUS_OOM = -200
+WF_STATUS_UNATTAINABLE = -300
+
+
+def positive_penalty(p: int) -> int:
+    """AnchorWave passes negative penalties; WFA takes their magnitude (WfaAlignment.cpp:298-302)."""
+    return -p if p < 0 else p
+
+
+class WfaAligner:
+    def __init__(self, mismatch: int, gap_opening1: int, gap_extension1: int, gap_opening2: int,
+                 gap_extension2: int, singletrack: bool = False, max_memory_abort: int = 0):
+        self.attr = WfaAttr(mismatch, gap_opening1, gap_extension1, gap_opening2, gap_extension2,
+                            int(bool(singletrack)), int(max_memory_abort))
+        self.h = lib.wavefront_aligner_new_gpu(C.byref(self.attr))
+        if not self.h:
+            raise AwError(f"wavefront_aligner_new_gpu failed: {last_error()}")
+
+    def align(self, pattern: bytes, text: bytes) -> int:
+        """wavefront_align(aligner, pattern, |pattern|, text, |text|): returns the WF status."""
+        return lib.wavefront_align_gpu(self.h, pattern, len(pattern), text, len(text))
+
+    def cigar(self) -> Tuple[str, int]:
+        ops = C.c_char_p()
+        n = C.c_int(0)
+        score = C.c_int(0)
+        lib.wavefront_gpu_cigar(self.h, C.byref(ops), C.byref(n), C.byref(score))
+        return (C.string_at(ops, n.value).decode() if n.value else ""), score.value
+
+    def align_batch(self, patterns: Sequence[bytes], texts: Sequence[bytes]):
+        """n alignments in one submission: list of (status, score, ops) plus device ms."""
+        n = len(patterns)
+        if n == 0:
+            return [], 0.0
+        pbufs = [C.create_string_buffer(p, len(p) + 1) for p in patterns]
+        tbufs = [C.create_string_buffer(t, len(t) + 1) for t in texts]
+        pp = (C.c_void_p * n)(*[C.addressof(b) for b in pbufs])
+        tp = (C.c_void_p * n)(*[C.addressof(b) for b in tbufs])
+        pl = np.array([len(p) for p in patterns], dtype=np.int32)
+        tl = np.array([len(t) for t in texts], dtype=np.int32)
+        status = np.zeros(n, dtype=np.int32)
+        score = np.zeros(n, dtype=np.int32)
+        offs = np.zeros(n, dtype=np.int64)
+        nops = np.zeros(n, dtype=np.int32)
+        cap = int(pl.sum() + tl.sum()) + 1
+        ops = C.create_string_buffer(cap)
+        ms = C.c_float(0.0)
+        rc = lib.wavefront_align_batch_gpu(self.h, n, pp, pl.ctypes.data, tp, tl.ctypes.data, status.ctypes.data,
+                                           score.ctypes.data, offs.ctypes.data, nops.ctypes.data, ops, cap,
+                                           C.byref(ms))
+        if rc != 0:
+            raise AwError(f"wavefront_align_batch_gpu failed ({rc}): {last_error()}")
+        raw = ops.raw
+        out = [(int(status[i]), int(score[i]), raw[offs[i]:offs[i] + nops[i]].decode()) for i in range(n)]
+        return out, ms.value
+
+    def close(self):
+        if self.h:
+            lib.wavefront_aligner_delete_gpu(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def decode_cigar(query: str, reference: str, ops: str):
+    """decodeCigar (WfaAlignment.cpp:223-268): gapped rows, or None when the CIGAR does not fit."""
+    aq, ar = [], []
+    qp = rp = 0
+    for c in ops:
+        if c in "MX":
+            if qp >= len(query) or rp >= len(reference):
+                return None
+            aq.append(query[qp]); ar.append(reference[rp]); qp += 1; rp += 1
+        elif c == "I":
+            if qp >= len(query):
+                return None
+            aq.append(query[qp]); ar.append("-"); qp += 1
+        elif c == "D":
+            if rp >= len(reference):
+                return None
+            aq.append("-"); ar.append(reference[rp]); rp += 1
+        else:
+            return None
+    if qp != len(query) or rp != len(reference):
+        return None
+    return "".join(aq), "".join(ar)
+
+
+def align_with_wfa(query: str, reference: str, mismatching_penalty: int, open1: int, extend1: int, open2: int,
+                   extend2: int, singletrack: bool = False, aligner: WfaAligner = None):
+    """alignWithWfaMode (WfaAlignment.cpp:270-391) on the GPU: (status, score, aln_query, aln_reference)."""
+    al = aligner or WfaAligner(positive_penalty(mismatching_penalty), positive_penalty(open1),
+                               positive_penalty(extend1), positive_penalty(open2), positive_penalty(extend2),
+                               singletrack)
+    st = al.align(reference.encode(), query.encode())
+    if st != WF_STATUS_ALG_COMPLETED:
+        return st, 0, "", ""
+    ops, score = al.cigar()
+    dec = decode_cigar(query, reference, ops)
+    if dec is None:
+        return WF_STATUS_UNATTAINABLE, 0, "", ""
+    return st, score, dec[0], dec[1]

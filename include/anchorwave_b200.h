@@ -94,6 +94,38 @@ int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_byt
 int aw_ksw_plan_timing(const aw_ksw_plan_t *plan, float *dp_ms, float *bt_ms);
 void aw_ksw_plan_free(aw_ksw_plan_t *plan);
 
+/* ---- WFA (gap-affine-2p, end to end) ------------------------------------------ */
+
+/* Attributes of WfaAlignment.cpp:143-170: match 0, these penalties (positive), high
+ * memory, no heuristic, full CIGAR; singletrack selects the Singletrack traceback. */
+typedef struct {
+    int mismatch, gap_opening1, gap_extension1, gap_opening2, gap_extension2;
+    int singletrack;
+    int64_t max_memory_abort;   /* device pool cap in bytes (0 = half of free memory) */
+} wavefront_gpu_attr_t;
+
+typedef struct wavefront_aligner_gpu wavefront_aligner_gpu_t;
+
+/* Replaces wavefront_aligner_new (WFA2-lib wavefront/wfa.h:129-134). */
+wavefront_aligner_gpu_t *wavefront_aligner_new_gpu(const wavefront_gpu_attr_t *attr);
+/* Replaces wavefront_aligner_delete. */
+void wavefront_aligner_delete_gpu(wavefront_aligner_gpu_t *aligner);
+/* Replaces wavefront_align (wfa.h:210-215): pattern = reference, text = query.
+ * Returns the WF status (0 completed, -200 out of memory, -300 unattainable). */
+int wavefront_align_gpu(wavefront_aligner_gpu_t *aligner, const char *pattern, int pattern_length,
+                        const char *text, int text_length);
+/* The last alignment's CIGAR operations ('M','X','I','D'; the aligner->cigar
+ * operations[begin_offset..end_offset) of the reference) and its score (-penalty). */
+int wavefront_gpu_cigar(const wavefront_aligner_gpu_t *aligner, const char **operations,
+                        int *num_operations, int *score);
+/* n alignments in one submission.  ops (capacity >= sum(plen + tlen) bytes) receives
+ * the operations back to back, pair i at ops_offset[i] with n_ops[i] characters. */
+int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const char *const *pattern,
+                              const int *pattern_length, const char *const *text,
+                              const int *text_length, int *status, int *score,
+                              int64_t *ops_offset, int *n_ops, char *ops, int64_t ops_capacity,
+                              float *device_ms);
+
 /* ---- allocation-free entry (no counterpart in the reference) ----------------------- */
 
 /* Scalar ksw_extz_t fields as written to device memory by the entry below. */
