@@ -29,8 +29,30 @@ EXPORTS = [
     "aw_set_traceback_budget", "aw_set_tuning", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops", "aw_ksw_extd2_device_noalloc",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
-    "wavefront_align_batch_gpu",
+    "wavefront_align_batch_gpu", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
+    "aw_serve_result_free", "aw_serve_close",
 ]
+
+
+class ServeConfig(C.Structure):
+    """aw_serve_config_t (include/anchorwave_b200.h)."""
+    _fields_ = [("slots", C.c_int), ("max_batch", C.c_int), ("hbm_budget", C.c_int64), ("m", C.c_int8),
+                ("mat", C.c_int8 * 64), ("q", C.c_int8), ("e", C.c_int8), ("q2", C.c_int8), ("e2", C.c_int8),
+                ("wfa_x", C.c_int), ("wfa_o1", C.c_int), ("wfa_e1", C.c_int), ("wfa_o2", C.c_int),
+                ("wfa_e2", C.c_int)]
+
+
+class ServeResult(C.Structure):
+    """aw_serve_result_t."""
+    _fields_ = [("id", C.c_uint64), ("method", C.c_int), ("status", C.c_int), ("ez", KswExtz),
+                ("wfa_score", C.c_int), ("n_ops", C.c_int), ("ops", C.c_void_p), ("latency_s", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    """aw_serve_stats_t."""
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("micro_batches", C.c_uint64),
+                ("queued", C.c_uint64), ("inflight_bytes", C.c_int64), ("latency_p50_s", C.c_double),
+                ("latency_p99_s", C.c_double), ("elapsed_s", C.c_double)]
 
 
 class WfaAttr(C.Structure):
@@ -88,6 +110,18 @@ def _load(path: str = LIB_PATH):
     lib.wavefront_gpu_cigar.restype = i32
     lib.wavefront_align_batch_gpu.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, C.POINTER(C.c_float)]
     lib.wavefront_align_batch_gpu.restype = i32
+    lib.aw_serve_open.argtypes = [C.POINTER(ServeConfig)]
+    lib.aw_serve_open.restype = vp
+    lib.aw_serve_submit.argtypes = [vp, C.c_uint64, i32, i32, C.c_char_p, i32, C.c_char_p, i32]
+    lib.aw_serve_submit.restype = i32
+    lib.aw_serve_poll.argtypes = [vp, C.POINTER(ServeResult), i32, i32]
+    lib.aw_serve_poll.restype = i32
+    lib.aw_serve_stats.argtypes = [vp, C.POINTER(ServeStats)]
+    lib.aw_serve_stats.restype = i32
+    lib.aw_serve_result_free.argtypes = [C.POINTER(ServeResult)]
+    lib.aw_serve_result_free.restype = None
+    lib.aw_serve_close.argtypes = [vp]
+    lib.aw_serve_close.restype = None
     for name in EXPORTS:
         getattr(lib, name)  # raises AttributeError if a declared symbol is missing
     return lib

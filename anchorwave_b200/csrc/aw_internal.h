@@ -99,6 +99,9 @@ struct DevBuf {
 
 void set_error(const char *msg);
 
+// Traceback budget of the calling thread's batches, 0 = process-wide (ksw2_api.cu).
+void set_thread_tb_budget(int64_t bytes);
+
 // Strip-path parameter check + score table (ksw2_api.cu).
 int full_path_params(int qlen, int tlen, int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2,
                      int8_t e2, int flag, KswScore *S);

@@ -46,6 +46,7 @@ static void set_error(const std::string &s) { set_error(s.c_str()); }
 
 // ---- tuning ----------------------------------------------------------------
 static int64_t g_tb_budget = 0;           // 0 = 60% of free memory
+static thread_local int64_t tls_tb_budget = 0;  // per-thread override (serving workers)
 static int g_large_warps = 8;
 static int g_large_tlen = 4096;
 static std::mutex g_cfg_mu;
@@ -322,8 +323,8 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
         return ca != cb ? ca > cb : a < b;
     });
     const bool cigar = !(P.flag & AW_EZ_SCORE_ONLY);
-    int64_t budget;
-    {
+    int64_t budget = tls_tb_budget;
+    if (budget <= 0) {
         std::lock_guard<std::mutex> lk(g_cfg_mu);
         budget = g_tb_budget;
     }
@@ -399,7 +400,7 @@ static int plan_alloc(aw_ksw_plan_t *pl) {
     AW_CUDA(B->packed_off.ensure(8 * (size_t)std::max(n, 1)));
     AW_CUDA(B->tb.ensure((size_t)pl->tb_cap + 256));
     AW_CUDA(B->bnd.ensure(4 * (size_t)pl->bnd_cap + 256));
-    AW_CUDA(B->queue.ensure(sizeof(int32_t) * 64 * (pl->waves.size() + 2)));
+    AW_CUDA(B->queue.ensure(sizeof(int32_t) * 64 * (2 * pl->waves.size() + 2)));  // two counters per wave
     AW_CUDA(B->error.ensure(sizeof(int32_t) * 4));
     AW_CUDA(B->h_pairs.ensure(sizeof(KswPair) * (size_t)std::max(n, 1)));
     AW_CUDA(B->h_order.ensure(sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size() + 1)));
@@ -430,11 +431,12 @@ static int plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uin
     return AW_OK;
 }
 
-static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
+// Enqueues every wave of the plan on its stream (no host synchronisation).
+static int plan_launch(aw_ksw_plan_t *pl) {
     Buffers *B = pl->B;
     const Params &P = pl->P;
     if (!pl->uploaded) { set_error("plan not uploaded"); return AW_E_INVAL; }
-    const size_t nq = 64 * (pl->waves.size() + 2);
+    const size_t nq = 64 * (2 * pl->waves.size() + 2);  // large + small counter per wave, 256 B apart
     int launches = 0;
     AW_CUDA(cudaMemsetAsync(B->queue.p, 0, sizeof(int32_t) * nq, B->st));
     AW_CUDA(cudaMemsetAsync(B->error.p, 0, sizeof(int32_t) * 4, B->st));
@@ -504,6 +506,14 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
         if (rc) return rc;
     }
     AW_CUDA(cudaEventRecord(B->ev_t1, B->st));
+    pl->launches = launches;
+    return AW_OK;
+}
+
+// Waits for plan_launch's work, checks the device error flag, collects timings.
+static int plan_finish(aw_ksw_plan_t *pl, float *ms) {
+    Buffers *B = pl->B;
+    const int nw = (int)pl->waves.size();
     AW_CUDA(cudaStreamSynchronize(B->st));
     int32_t err = 0;
     AW_CUDA(cudaMemcpy(&err, B->error.p, 4, cudaMemcpyDeviceToHost));
@@ -518,9 +528,13 @@ static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
     }
     pl->dp_ms = dp;
     pl->bt_ms = bt;
-    pl->launches = launches;
     pl->executed = true;
     return AW_OK;
+}
+
+static int plan_execute(aw_ksw_plan_t *pl, float *ms) {
+    const int rc = plan_launch(pl);
+    return rc ? rc : plan_finish(pl, ms);
 }
 
 static int plan_download(aw_ksw_plan_t *pl, ksw_extz_t *ez, void *km) {
@@ -696,6 +710,9 @@ void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tle
 }  // extern "C"
 
 namespace aw {
+// Traceback budget of the calling thread's batches (0 = the process-wide setting).
+void set_thread_tb_budget(int64_t bytes) { tls_tb_budget = bytes; }
+
 // Parameter checks and score table of the full-matrix strip path, for callers
 // outside this file.  Returns AW_OK when (qlen, tlen, parameters, flag) can run
 // on the strip kernel, 1 when ksw_extd2 would return at once without any DP

@@ -67,7 +67,10 @@ __device__ __forceinline__ void group_sync(int g, int nthreads) {
 }
 
 #ifndef AW_CELL_DPX
-#define AW_CELL_DPX 1
+#define AW_CELL_DPX 2
+#endif
+#ifndef AW_ARGMAX_DPX
+#define AW_ARGMAX_DPX 1
 #endif
 
 template <bool CIGAR, bool RIGHT>
@@ -75,7 +78,7 @@ __device__ __forceinline__ void cell(int s, int &xs, int &vs, int &x2s, int &ut,
                                      int &d, const KswScore &S) {
     int a = xs + vs, b = yt + ut, a2 = x2s + vs, b2 = y2t + ut;
     int z = s;
-#if AW_CELL_DPX
+#if AW_CELL_DPX && AW_ARGMAX_DPX
     // Arg-max chain with the reference's tie rules, one DPX max+predicate per step:
     // left-aligned takes a candidate only if strictly greater (ksw2_extd2_sse.c:244-251),
     // right-aligned also on equality (:291-298).

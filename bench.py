@@ -280,7 +280,11 @@ def main():
         e2e_s.append(time.perf_counter() - t0)
     barrier(pg)
     e2e_step = max_over_ranks(pg, float(np.mean(e2e_s)))
-    identical = all(a.key() == b.key() for a, b in zip(res_dev, res_e2e))
+    diffs = [i for i, (a, b) in enumerate(zip(res_dev, res_e2e)) if a.key() != b.key()]
+    identical = not diffs
+    for i in diffs[:5]:
+        print(f"[bench] pair {i} (qlen {len(ps.queries[i])}, tlen {len(ps.targets[i])}) differs: device-resident "
+              f"{res_dev[i].key()[:12]} / e2e {res_e2e[i].key()[:12]}", file=sys.stderr)
     h2d = int(sum(len(q) for q in ps.queries) + sum(len(t) for t in ps.targets) + n * 48 + n * 4)
     d2h = int(n * 48 + sum(r.n_cigar for r in res_e2e) * 4)
 

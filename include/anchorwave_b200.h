@@ -126,6 +126,55 @@ int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const cha
                               int64_t *ops_offset, int *n_ops, char *ops, int64_t ops_capacity,
                               float *device_ms);
 
+/* ---- serving loop (continuous batching) --------------------------------------- */
+
+/* Engine of a request, as chosen by AnchorWave's exact-tier / fallback-tier selector
+ * (src/myImportandFunction/AlignmentAlgorithmSelector.cpp:1711). */
+#define AW_ROUTE_KSW2             0  /* ksw_extd2, full (band < 0) or banded */
+#define AW_ROUTE_KSW2_SINGLETRACK 1  /* ksw_extd2 with the Singletrack traceback */
+#define AW_ROUTE_WFA              2  /* gap-affine-2p WFA, high memory */
+#define AW_ROUTE_WFA_SINGLETRACK  3  /* gap-affine-2p WFA, Singletrack */
+
+typedef struct {
+    int slots;            /* concurrent micro-batches (workers with their own streams) */
+    int max_batch;        /* requests per micro-batch */
+    int64_t hbm_budget;   /* predicted device bytes admitted at once (0 = half of free) */
+    int8_t m;             /* KSW2 scoring: alphabet size, m*m matrix, q, e, q2, e2 */
+    int8_t mat[64];
+    int8_t q, e, q2, e2;
+    int wfa_x, wfa_o1, wfa_e1, wfa_o2, wfa_e2;  /* WFA penalties (positive) */
+} aw_serve_config_t;
+
+typedef struct {
+    uint64_t id;
+    int method;
+    int status;           /* 0 ok; WF status for WFA routes; AW_E* on failure */
+    ksw_extz_t ez;        /* KSW2 routes: ez.cigar malloc'd */
+    int wfa_score;        /* WFA routes: -penalty */
+    int n_ops;
+    char *ops;            /* WFA routes: 'M','X','I','D' operations, malloc'd */
+    double latency_s;     /* submit -> result ready */
+} aw_serve_result_t;
+
+typedef struct {
+    uint64_t submitted, completed, micro_batches, queued;
+    int64_t inflight_bytes;
+    double latency_p50_s, latency_p99_s, elapsed_s;
+} aw_serve_stats_t;
+
+typedef struct aw_server aw_server_t;
+
+/* Replaces the alignment-stage thread pool (src/service/AnchorTaskExecutor.h:54-160). */
+aw_server_t *aw_serve_open(const aw_serve_config_t *cfg);
+/* Enqueue one interval (ASCII sequences; ids consecutive from 0). Never blocks on the GPU. */
+int aw_serve_submit(aw_server_t *server, uint64_t id, int method, int band, const char *query,
+                    int qlen, const char *target, int tlen);
+/* Up to max finished results, strictly in id order (waits up to wait_ms for the next one). */
+int aw_serve_poll(aw_server_t *server, aw_serve_result_t *out, int max, int wait_ms);
+int aw_serve_stats(aw_server_t *server, aw_serve_stats_t *stats);
+void aw_serve_result_free(aw_serve_result_t *result);
+void aw_serve_close(aw_server_t *server);
+
 /* ---- allocation-free entry (no counterpart in the reference) ----------------------- */
 
 /* Scalar ksw_extz_t fields as written to device memory by the entry below. */

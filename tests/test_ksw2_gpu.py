@@ -139,6 +139,21 @@ def test_multiwarp_pipeline_and_waves(gpu, restatement, warps):
         assert r.key() == o.key()
 
 
+def test_repeated_batches_with_many_waves(gpu, restatement):
+    """Back-to-back batch calls on one thread whose plans need more and more traceback waves
+    (every wave has its own work-queue counters, all reset per call)."""
+    qs, ts, _ = _random_set(123, 40, 300, 3000)
+    mat = oracle.anchorwave_matrix(-4)
+    exp = [restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1).key() for q, t in zip(qs, ts)]
+    try:
+        for budget in (256 << 20, 64 << 20, 24 << 20, 12 << 20, 64 << 20):
+            gpu.set_traceback_budget(budget)
+            res = gpu.ksw_extd2_batch(qs, ts, mat, 4, 2, 24, 1)
+            assert [r.key() for r in res] == exp, budget
+    finally:
+        gpu.set_traceback_budget(0)
+
+
 def test_plan_repeatable(gpu):
     ps = W.batched_full_set(64, seed=9, lmax=3000)
     plan = gpu.KswPlan(ps.queries, ps.targets, oracle.anchorwave_matrix(-4), 4, 2, 24, 1)

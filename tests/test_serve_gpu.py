@@ -1,0 +1,106 @@
+"""GPU tests of the serving loop (continuous batching): every result equals the standalone
+call (alone vs in the mix), results are released strictly in id order, requests keep being
+admitted while earlier micro-batches run, and a small HBM budget still completes the trace."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from anchorwave_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+PEN = (4, 2, 24, 1)
+WPEN = (4, 4, 2, 24, 1)
+
+
+def _mix(seed, n):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        L = int(np.exp(rng.uniform(np.log(30), np.log(3000))))
+        q, t = W.divergent_pair(rng, L, 0.01, 0.12, 4.0)
+        if rng.random() < 0.1:
+            q = q.copy()
+            q[rng.integers(0, len(q), 2)] = 4
+        kind = i % 5
+        method = [0, 0, 1, 2, 3][kind]
+        band = int(0.3 * min(len(q), len(t))) if kind == 1 else -1
+        reqs.append((i, method, W.to_ascii(q), W.to_ascii(t), band))
+    return reqs
+
+
+def _standalone(gpu, wfa, method, q, t, band):
+    from anchorwave_b200 import ksw2
+    if method in (0, 1):
+        qc, f1 = ksw2.encode(q)
+        tc, f2 = ksw2.encode(t)
+        fn = gpu.ksw_extd2_singletrack if method == 1 else gpu.ksw_extd2
+        return fn(qc, tc, oracle.anchorwave_matrix(-4), *PEN, w=band, flag=f1 | f2).key()
+    al = wfa.WfaAligner(*WPEN, singletrack=(method == 3))
+    st = al.align(t, q)
+    ops, score = al.cigar() if st == 0 else ("", 0)
+    al.close()
+    return (st, score, ops)
+
+
+def _drain(srv, n, timeout=120):
+    out = []
+    t0 = time.time()
+    while len(out) < n and time.time() - t0 < timeout:
+        out += srv.poll(256, wait_ms=50)
+    return out
+
+
+def test_results_identical_alone_and_in_the_mix(gpu):
+    from anchorwave_b200 import serve, wfa
+    reqs = _mix(11, 60)
+    with serve.AlignmentServer(oracle.anchorwave_matrix(-4), *PEN, wfa_penalties=WPEN, slots=3,
+                               max_batch=8) as srv:
+        for rid, m, q, t, band in reqs:
+            srv.submit(rid, m, q, t, band)
+        got = _drain(srv, len(reqs))
+        st = srv.stats()
+    assert [g.id for g in got] == list(range(len(reqs)))
+    assert st["micro_batches"] >= 4
+    for g, (rid, m, q, t, band) in zip(got, reqs):
+        alone = _standalone(gpu, wfa, m, q, t, band)
+        assert (g.ksw if m in (0, 1) else g.wfa) == alone, (rid, m, len(q), len(t))
+
+
+def test_ordered_release_behind_a_slow_request(gpu):
+    from anchorwave_b200 import serve
+    rng = np.random.default_rng(3)
+    big_q, big_t = W.divergent_pair(rng, 12000, 0.05, 0.05, 4.0)
+    with serve.AlignmentServer(oracle.anchorwave_matrix(-4), *PEN, wfa_penalties=WPEN, slots=2,
+                               max_batch=1) as srv:
+        srv.submit(0, 0, W.to_ascii(big_q), W.to_ascii(big_t))
+        for i in range(1, 20):
+            q, t = W.divergent_pair(rng, 100, 0.05, 0.05, 4.0)
+            srv.submit(i, 0, W.to_ascii(q), W.to_ascii(t))
+        got = _drain(srv, 20)
+    assert [g.id for g in got] == list(range(20))
+
+
+def test_continuous_arrivals_and_small_budget(gpu):
+    """Requests arrive while earlier micro-batches run; a budget of a few traceback arenas
+    forces admission waits; the whole trace still completes, in order, unchanged."""
+    from anchorwave_b200 import serve, wfa
+    reqs = _mix(29, 80)
+    with serve.AlignmentServer(oracle.anchorwave_matrix(-4), *PEN, wfa_penalties=WPEN, slots=4, max_batch=4,
+                               hbm_budget=96 << 20) as srv:
+        def producer():
+            for rid, m, q, t, band in reqs:
+                srv.submit(rid, m, q, t, band)
+                time.sleep(0.002)
+        th = threading.Thread(target=producer)
+        th.start()
+        got = _drain(srv, len(reqs))
+        th.join()
+        st = srv.stats()
+    assert [g.id for g in got] == list(range(len(reqs)))
+    assert st["completed"] == len(reqs) and st["latency_p99_s"] >= st["latency_p50_s"] > 0
+    for g, (rid, m, q, t, band) in list(zip(got, reqs))[::7]:
+        assert (g.ksw if m in (0, 1) else g.wfa) == _standalone(gpu, wfa, m, q, t, band)
