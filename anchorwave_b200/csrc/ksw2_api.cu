@@ -47,6 +47,7 @@ static void set_error(const std::string &s) { set_error(s.c_str()); }
 // ---- tuning ----------------------------------------------------------------
 static int64_t g_tb_budget = 0;           // 0 = 60% of free memory
 static thread_local int64_t tls_tb_budget = 0;  // per-thread override (serving workers)
+static thread_local bool tls_all_large = false;  // single-pair calls: every pair gets a warp group
 static int g_large_warps = 8;
 static int g_large_tlen = 4096;
 static std::mutex g_cfg_mu;
@@ -368,7 +369,8 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
     for (size_t k = 0; k < wv.size(); ++k) {
         aw_ksw_plan::Wave W;
         std::vector<int32_t> lg, sm;
-        for (int32_t i : wv[k]) (pl->tlen[i] >= large_tlen && large_warps > 1 ? lg : sm).push_back(i);
+        for (int32_t i : wv[k])
+            ((pl->tlen[i] >= large_tlen || tls_all_large) && large_warps > 1 ? lg : sm).push_back(i);
         W.begin_large = (int)pl->order.size();
         W.n_large = (int)lg.size();
         pl->order.insert(pl->order.end(), lg.begin(), lg.end());
@@ -684,7 +686,10 @@ static void single_call(void *km, int qlen, const uint8_t *query, int tlen, cons
         ez->zdropped = 1;
         return;
     }
+    // one pair alone: let a whole warp group pipeline its strips whatever its length
+    tls_all_large = true;
     int rc = plan_build(&pl, 1, &qlen, &tlen, &w);
+    tls_all_large = false;
     if (!rc) rc = plan_alloc(&pl);
     if (!rc) rc = plan_upload(&pl, &query, &target);
     if (!rc) rc = plan_execute(&pl, nullptr);

@@ -9,6 +9,7 @@
 #include "../../include/anchorwave_b200.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -180,6 +181,9 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
         std::vector<int32_t> again;
         for (int32_t i : batch)
             if (al->outs[i].status == WFA_RETRY) again.push_back(i);
+        if (getenv("AW_VERBOSE"))
+            fprintf(stderr, "[aw_b200] WFA round %d: %zu pairs, %zu to retry, %.1f ms\n", launches, batch.size(),
+                    again.size(), ms);
         if (serial) {
             if (!again.empty()) al->outs[pending[0]].status = WFA_OOM;
             pending.erase(pending.begin());

@@ -129,6 +129,44 @@ def ksw_extd2_batch(queries, targets, mat, q, e, q2, e2, w=None, zdrop=-1, end_b
     return out
 
 
+class BatchCall:
+    """A prepared aw_ksw_extd2_batch call: argument arrays built once, so timing run() measures
+    the C-ABI call itself (host staging, H2D, kernels, D2H, CIGAR buffers in ksw_extz_t)."""
+
+    def __init__(self, queries, targets, mat, q, e, q2, e2, w=None, zdrop=-1, end_bonus=0, flag=0, m=5):
+        self.qs = [_codes(x) for x in queries]
+        self.ts = [_codes(x) for x in targets]
+        self.n = len(self.qs)
+        self.ql = np.array([len(x) for x in self.qs], dtype=np.int32)
+        self.tl = np.array([len(x) for x in self.ts], dtype=np.int32)
+        self.qp, self.tp = _ptr_array(self.qs), _ptr_array(self.ts)
+        self.w = None if w is None else np.ascontiguousarray(np.broadcast_to(np.asarray(w, dtype=np.int32), (self.n,)))
+        self.args = (m, _mat(mat), q, e, q2, e2, zdrop, end_bonus, flag)
+        self.ez = (KswExtz * self.n)()
+
+    def run(self) -> int:
+        m, mat, q, e, q2, e2, zdrop, end_bonus, flag = self.args
+        rc = lib.aw_ksw_extd2_batch(self.n, self.ql.ctypes.data, self.qp, self.tl.ctypes.data, self.tp,
+                                    None if self.w is None else self.w.ctypes.data, m, mat, q, e, q2, e2, zdrop,
+                                    end_bonus, flag, self.ez)
+        check(rc, "aw_ksw_extd2_batch")
+        return rc
+
+    def cigar_words(self) -> int:
+        return int(sum(self.ez[i].n_cigar for i in range(self.n)))
+
+    def results(self) -> List[KswResult]:
+        """Converts (and releases) the last run's ksw_extz_t array."""
+        return [_take(self.ez[i]) for i in range(self.n)]
+
+    def release(self):
+        for i in range(self.n):
+            if self.ez[i].cigar:
+                libc.free(C.cast(self.ez[i].cigar, C.c_void_p))
+                self.ez[i].cigar = None
+                self.ez[i].m_cigar = 0
+
+
 class KswPlan:
     """A batch kept resident on the device (aw_ksw_plan_*): upload once, execute many times."""
 
