@@ -109,7 +109,7 @@ struct aw_server {
 namespace {
 
 // Pops one micro-batch: the oldest request plus later ones of the same class
-// (engine, band, scoring flag) while they fit the batch size and the budget.
+// (engine, scoring flag) while they fit the batch size and the budget.
 bool take_batch(aw_server *S, std::vector<Req> &batch) {
     batch.clear();
     if (S->queue.empty()) return false;
@@ -117,9 +117,10 @@ bool take_batch(aw_server *S, std::vector<Req> &batch) {
     const int64_t budget = S->cfg.hbm_budget;
     if (S->inflight_bytes > 0 && S->inflight_bytes + head.pred > budget) return false;
     std::vector<uint8_t> tmp;
+    // requests of one class share a launch: same engine and KSW2 scoring flag (bands may differ)
     auto klass = [&](const Req &r) {
         const bool gen = r.method <= AW_ROUTE_KSW2_SINGLETRACK && (encode(r.q, tmp) | encode(r.t, tmp));
-        return std::make_tuple(r.method, r.band, gen);
+        return std::make_tuple(r.method, gen);
     };
     const auto k0 = klass(head);
     int64_t bytes = 0;

@@ -124,11 +124,11 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     WCUDA(al->d_out.ensure(sizeof(WfaOutDev) * (size_t)n));
     WCUDA(al->d_queue.ensure(64));
     WCUDA(al->d_head.ensure(64));
-    // device pool: half of free memory (capped by max_memory_abort when set)
+    // device pool: 85% of free memory (capped by max_memory_abort when set)
     if (al->d_pool.cap == 0) {
         size_t fr = 0, tot = 0;
         WCUDA(cudaMemGetInfo(&fr, &tot));
-        int64_t want = (int64_t)(fr * 0.5);
+        int64_t want = (int64_t)(fr * 0.85);
         if (A.max_memory_abort > 0) want = std::min<int64_t>(want, A.max_memory_abort);
         want = std::max<int64_t>(want, (int64_t)64 << 20);
         WCUDA(al->d_pool.ensure((size_t)want));

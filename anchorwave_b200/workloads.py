@@ -196,3 +196,39 @@ def band_cells(qlen: int, tlen: int, w: int) -> int:
             break
         total += en - st + 1
     return total
+
+
+@dataclass
+class Request:
+    id: int
+    method: int      # 0 KSW2 (full or banded), 1 KSW2 Singletrack, 2 WFA, 3 WFA Singletrack
+    band: int
+    query: bytes     # ASCII
+    target: bytes
+
+
+def serving_trace(n: int, seed: int = 4, lmin: int = 50, lmax: int = 500_000, repeat_frac: float = 0.1,
+                  band_above: int = 20_000) -> List[Request]:
+    """Interval requests of the serving workload: length ~ LogNormal(median 2 kb, sigma 1)
+    clipped to [lmin, lmax]; divergence and indels as the batched-full workload; repeat_frac of
+    them carry long-interval repeat structure.  Engine per request (a stand-in for AnchorWave's
+    exact-tier/fallback-tier selector, which stays on the caller's side): low-divergence
+    intervals up to 10 kb (d <= 5%, where the wavefront score stays small) go to WFA, intervals
+    longer than band_above to banded KSW2 with a 10% band, the rest to full KSW2."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        L = int(np.clip(np.exp(rng.normal(math.log(2000), 1.0)), lmin, lmax))
+        d = rng.uniform(0.01, 0.15)
+        t = random_dna(rng, L)
+        if rng.random() < repeat_frac and L >= 200:
+            q = repeat_query(rng, t, long_indels=(0, 2), long_max=max(1, L // 20), element=max(20, L // 10))
+            d = 1.0
+        else:
+            q = mutate(rng, t, 0.8 * d, 0.2 * d, 4.0)
+            if len(q) == 0:
+                q = random_dna(rng, 1)
+        method = 2 if (d <= 0.05 and L <= 10_000) else 0
+        band = int(0.1 * min(len(q), len(t))) if (method == 0 and max(len(q), len(t)) > band_above) else -1
+        out.append(Request(i, method, band, to_ascii(q), to_ascii(t)))
+    return out

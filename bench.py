@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=0,
+                    help="requests of the serving trace (0 skips the serving measurement)")
     return ap.parse_args()
 
 
@@ -209,6 +211,56 @@ def run_reference_arm(args):
     return 0
 
 
+def serving_measurement(nreq: int, rank: int):
+    """Serving trace (lengths log-normal, median 2 kb, sigma 1, clipped to 50 bp-50 kb here;
+    low-divergence intervals up to 10 kb on WFA, > 20 kb banded KSW2, the rest full KSW2; 10%
+    with repeat structure) through the
+    continuous-batching server: saturated throughput with all requests queued at once, then
+    p50/p99 latency with Poisson arrivals at 80% of that rate."""
+    import numpy as np
+
+    from anchorwave_b200 import ksw2, serve
+    from anchorwave_b200 import workloads as W
+    reqs = W.serving_trace(nreq, seed=4 + rank, lmax=50_000)
+    cells = sum(len(r.query) * len(r.target) for r in reqs)
+
+    def run(rate):
+        rng = np.random.default_rng(99)
+        with serve.AlignmentServer(ksw2.anchorwave_matrix(-4), 4, 2, 24, 1, slots=4, max_batch=512) as srv:
+            t0 = time.perf_counter()
+
+            def producer():
+                nxt = t0
+                for r in reqs:
+                    if rate:
+                        nxt += rng.exponential(1.0 / rate)
+                        d = nxt - time.perf_counter()
+                        if d > 0:
+                            time.sleep(d)
+                    srv.submit(r.id, r.method, r.query, r.target, r.band)
+
+            th = threading.Thread(target=producer)
+            th.start()
+            got = 0
+            while got < len(reqs):
+                got += len(srv.poll(4096, wait_ms=20))
+            th.join()
+            dt = time.perf_counter() - t0
+            st = srv.stats()
+        return dt, st
+
+    dt_sat, st_sat = run(None)
+    sat = len(reqs) / dt_sat
+    dt, st = run(0.8 * sat)
+    return {"requests": len(reqs), "cells": cells, "saturated_requests_per_s": sat,
+            "saturated_gcups": cells / dt_sat / 1e9, "offered_requests_per_s": 0.8 * sat,
+            "requests_per_s": len(reqs) / dt, "gcups": cells / dt / 1e9,
+            "latency_ms_p50": 1e3 * st["latency_p50_s"], "latency_ms_p99": 1e3 * st["latency_p99_s"],
+            "micro_batches": st["micro_batches"], "slots": 4, "max_batch": 512,
+            "trace": "log-normal lengths (median 2 kb, sigma 1) clipped to 50 bp-50 kb, WFA for d<=5% "
+                     "and <=10 kb, >20 kb banded (w=10%), 10% repeat-rich; Poisson arrivals at 80% of saturation"}
+
+
 def cpu_baseline(ps, budget):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
@@ -308,6 +360,8 @@ def main():
              "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
              "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)), "sample_pairs": len(lat)}
 
+    serving = serving_measurement(args.serve_requests, rank) if args.serve_requests > 0 else None
+
     if rank != 0:
         barrier(pg)
         return 0
@@ -328,6 +382,8 @@ def main():
                    "waves": st["waves"]},
         "latency_ms": {"batch_step_p50": float(np.percentile(step_ms, 50)),
                        "batch_step_p99": float(np.percentile(step_ms, 99)),
+                       "serving_p50": serving["latency_ms_p50"] if serving else None,
+                       "serving_p99": serving["latency_ms_p99"] if serving else None,
                        "plain_per_call_p50": plain["latency_ms_p50"], "plain_per_call_p99": plain["latency_ms_p99"]},
         "plain_per_call": plain,
         "batched_vs_plain_pairs_per_s": pairs_per_s / world / plain["pairs_per_s"],
@@ -341,6 +397,7 @@ def main():
         "e2e": {"value": world * cells / e2e_step / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "pairs_per_s": world * n / e2e_step,
                 "results_identical_to_device_path": identical},
+        "serving": serving,
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }

@@ -101,7 +101,7 @@ void aw_ksw_plan_free(aw_ksw_plan_t *plan);
 typedef struct {
     int mismatch, gap_opening1, gap_extension1, gap_opening2, gap_extension2;
     int singletrack;
-    int64_t max_memory_abort;   /* device pool cap in bytes (0 = half of free memory) */
+    int64_t max_memory_abort;   /* device pool cap in bytes (0 = 85% of free memory) */
 } wavefront_gpu_attr_t;
 
 typedef struct wavefront_aligner_gpu wavefront_aligner_gpu_t;
