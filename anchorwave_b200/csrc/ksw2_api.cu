@@ -12,6 +12,7 @@
 //     one-call-per-worker threading contract, SURVEY boundary table);
 //   * CIGAR ownership exactly as ksw_push_cigar (minimap2/ksw2.h:144-154).
 #include "aw_internal.h"
+#include "ksw2_band.h"
 #include "ksw2_exact.h"
 #include "../../include/anchorwave_b200.h"
 
@@ -76,6 +77,8 @@ struct PinBuf {
 struct Buffers {
     DevBuf qcodes, tcodes, pairs, order, out, cig, packed, packed_off, tb, bnd, queue, error;
     DevBuf exact_ws;
+    DevBuf band_pairs, band_strips, band_units, band_res, band_progress, band_bnd, band_queue;
+    PinBuf h_band;
     PinBuf h_codes, h_pairs, h_order, h_out, h_packed, h_packed_off, h_small;
     cudaStream_t st = nullptr, st2 = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
@@ -86,6 +89,8 @@ struct Buffers {
         qcodes.release(); tcodes.release(); pairs.release(); order.release(); out.release();
         cig.release(); packed.release(); packed_off.release(); tb.release(); bnd.release();
         queue.release(); error.release(); exact_ws.release();
+        band_pairs.release(); band_strips.release(); band_units.release(); band_res.release();
+        band_progress.release(); band_bnd.release(); band_queue.release(); h_band.release();
         h_codes.release(); h_pairs.release(); h_order.release(); h_out.release();
         h_packed.release(); h_packed_off.release(); h_small.release();
         for (auto e : ev_k) cudaEventDestroy(e);
@@ -205,6 +210,25 @@ static bool full_path_ok(const Params &P, int qlen, int tlen, int w) {
     return true;
 }
 
+// The banded strip kernel (ksw2_band.cu) restates the reference's padding-lane
+// semantics, so it takes any band and the Singletrack traceback; it shares the
+// strip kernel's scoring restrictions (no z-drop or max tracking: with mat <= 0
+// every H is <= 0, so ez->max stays 0 and max_t/max_q stay -1).
+static bool band_path_ok(const Params &P, int qlen, int tlen) {
+    if (exact_stop_enabled()) return false;
+    const int allowed = AW_EZ_SCORE_ONLY | AW_EZ_RIGHT | AW_EZ_GENERIC_SC | AW_EZ_REV_CIGAR |
+                        AW_EZ_SEMIGLOBAL_END | AW_EZ_SINGLETRACK;
+    if (P.flag & ~allowed) return false;
+    if (P.zdrop >= 0) return false;
+    if (P.max_sc > 0 || P.mat[0] < P.max_sc) return false;
+    if (P.q < 0 || P.e < 0 || P.q2 < 0 || P.e2 < 0) return false;
+    if (P.e2 > P.e || P.q2 < P.q) return false;
+    const int mag = (P.q2 + P.e2) + (P.q + P.e) + std::abs(P.min_sc) + std::abs((int)P.mat[0]);
+    if (mag > 100) return false;
+    if ((int64_t)qlen + tlen > INT_MAX / 4) return false;
+    return true;
+}
+
 static void reset_extz(ksw_extz_t *ez) {  // minimap2/ksw2.h:194-199
     ez->max_q = ez->max_t = ez->mqe_t = ez->mte_q = -1;
     ez->max = 0, ez->score = ez->mqe = ez->mte = AW_NEG_INF;
@@ -262,7 +286,7 @@ struct aw_ksw_plan {
     KswScore S;
     int n = 0;
     std::vector<int> qlen, tlen, w;
-    std::vector<int> route;   // 0 = no device work (early return), 1 = strip kernel, 2 = exact kernel
+    std::vector<int> route;   // 0 = no device work (early return), 1 = strip kernel, 2 = exact kernel, 3 = banded kernel
     std::vector<int> early_zdrop;
     std::vector<KswPair> pairs;
     std::vector<int64_t> qoff, toff;
@@ -275,6 +299,8 @@ struct aw_ksw_plan {
     std::vector<Wave> waves;
     std::vector<int32_t> order;      // strip-kernel processing order, wave by wave
     std::vector<int32_t> exact_ids;  // pairs for the exact kernel
+    std::vector<int32_t> band_ids;   // pairs for the banded kernel
+    BandPlan band;
     int64_t tb_cap = 0, bnd_cap = 0;
     int64_t cells = 0, tb_total = 0;
     int launches = 0;
@@ -304,7 +330,7 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
         if (P.m <= 1 || ql <= 0 || tl <= 0) continue;
         if (ql > INT_MAX - tl + 1) { pl->early_zdrop[i] = 1; continue; }
         if (P.early_return) continue;
-        pl->route[i] = full_path_ok(P, ql, tl, pl->w[i]) ? 1 : 2;
+        pl->route[i] = full_path_ok(P, ql, tl, pl->w[i]) ? 1 : band_path_ok(P, ql, tl) ? 3 : 2;
         KswPair &kp = pl->pairs[i];
         kp.qoff = pl->qoff[i], kp.toff = pl->toff[i];
         kp.qlen = ql, kp.tlen = tl;
@@ -319,6 +345,7 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
     for (int i = 0; i < n; ++i)
         if (pl->route[i] == 1) strip.push_back(i);
         else if (pl->route[i] == 2) pl->exact_ids.push_back(i);
+        else if (pl->route[i] == 3) pl->band_ids.push_back(i);
     std::sort(strip.begin(), strip.end(), [&](int a, int b) {
         const int64_t ca = (int64_t)pl->qlen[a] * pl->tlen[a], cb = (int64_t)pl->qlen[b] * pl->tlen[b];
         return ca != cb ? ca > cb : a < b;
@@ -383,6 +410,15 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
         pl->bnd_cap = std::max(pl->bnd_cap, W.bnd_words);
         pl->waves.push_back(W);
     }
+    if (!pl->band_ids.empty()) {
+        if (band_plan_build(pl->band, pl->band_ids, pl->qlen, pl->tlen, pl->w, pl->pairs, P.flag, exact_block(),
+                            budget)) {
+            set_error("pair traceback exceeds the HBM traceback budget");
+            return AW_E_NOMEM;
+        }
+        pl->tb_cap = std::max(pl->tb_cap, pl->band.tb_cap);
+        pl->tb_total += pl->band.tb_total;
+    }
     pl->S = make_score(P);
     return AW_OK;
 }
@@ -404,6 +440,16 @@ static int plan_alloc(aw_ksw_plan_t *pl) {
     AW_CUDA(B->bnd.ensure(4 * (size_t)pl->bnd_cap + 256));
     AW_CUDA(B->queue.ensure(sizeof(int32_t) * 64 * (2 * pl->waves.size() + 2)));  // two counters per wave
     AW_CUDA(B->error.ensure(sizeof(int32_t) * 4));
+    if (!pl->band_ids.empty()) {
+        const BandPlan &bp = pl->band;
+        AW_CUDA(B->band_pairs.ensure(sizeof(BandPairDev) * bp.pairs.size()));
+        AW_CUDA(B->band_strips.ensure(sizeof(BandStripDev) * bp.strips.size()));
+        AW_CUDA(B->band_units.ensure(sizeof(int2) * bp.units.size()));
+        AW_CUDA(B->band_res.ensure(sizeof(BandRes) * bp.pairs.size()));
+        AW_CUDA(B->band_progress.ensure(sizeof(int32_t) * PROG_STRIDE * bp.strips.size()));
+        AW_CUDA(B->band_bnd.ensure(sizeof(uint2) * (size_t)bp.bnd_cap + 256));
+        AW_CUDA(B->band_queue.ensure(sizeof(int32_t) * 64 * bp.waves.size()));
+    }
     AW_CUDA(B->h_pairs.ensure(sizeof(KswPair) * (size_t)std::max(n, 1)));
     AW_CUDA(B->h_order.ensure(sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size() + 1)));
     AW_CUDA(B->h_out.ensure(sizeof(KswOut) * (size_t)std::max(n, 1)));
@@ -429,6 +475,19 @@ static int plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uin
     AW_CUDA(cudaMemcpyAsync(B->pairs.p, B->h_pairs.p, sizeof(KswPair) * (size_t)n, cudaMemcpyHostToDevice, B->st));
     AW_CUDA(cudaMemcpyAsync(B->order.p, ho, sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size()),
                             cudaMemcpyHostToDevice, B->st));
+    if (!pl->band_ids.empty()) {
+        const BandPlan &bp = pl->band;
+        const size_t np = sizeof(BandPairDev) * bp.pairs.size(), ns = sizeof(BandStripDev) * bp.strips.size(),
+                     nu = sizeof(int2) * bp.units.size();
+        AW_CUDA(B->h_band.ensure(np + ns + nu));
+        uint8_t *h = B->h_band.as<uint8_t>();
+        memcpy(h, bp.pairs.data(), np);
+        memcpy(h + np, bp.strips.data(), ns);
+        memcpy(h + np + ns, bp.units.data(), nu);
+        AW_CUDA(cudaMemcpyAsync(B->band_pairs.p, h, np, cudaMemcpyHostToDevice, B->st));
+        AW_CUDA(cudaMemcpyAsync(B->band_strips.p, h + np, ns, cudaMemcpyHostToDevice, B->st));
+        AW_CUDA(cudaMemcpyAsync(B->band_units.p, h + np + ns, nu, cudaMemcpyHostToDevice, B->st));
+    }
     pl->uploaded = true;
     return AW_OK;
 }
@@ -450,7 +509,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         large_warps = g_large_warps;
     }
     // per-wave timing events: DP phase start, DP phase end (after the join), backtrack end
-    const size_t need_ev = 3 * pl->waves.size() + 3;
+    const size_t need_ev = 3 * (pl->waves.size() + pl->band.waves.size()) + 3;
     while (B->ev_k.size() < need_ev) {
         cudaEvent_t e;
         AW_CUDA(cudaEventCreate(&e));
@@ -499,6 +558,26 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         }
         AW_CUDA(cudaEventRecord(B->ev_k[3 * k + 2], B->st));
     }
+    const int nbw = pl->band_ids.empty() ? 0 : (int)pl->band.waves.size();
+    if (nbw > 0) {
+        BandDev D;
+        D.pairs = B->band_pairs.as<BandPairDev>(), D.strips = B->band_strips.as<BandStripDev>();
+        D.units = B->band_units.as<int2>(), D.res = B->band_res.as<BandRes>();
+        D.progress = B->band_progress.as<int32_t>(), D.queue = B->band_queue.as<int32_t>();
+        D.bnd = B->band_bnd.as<uint2>(), D.tb = B->tb.as<uint8_t>(), D.error = B->error.as<int32_t>();
+        const int ctas = band_occupancy(P.flag) * B->sms;
+        for (int k = 0; k < nbw; ++k) {
+            cudaEvent_t *ev = &B->ev_k[3 * (nw + k)];
+            AW_CUDA(cudaEventRecord(ev[0], B->st));
+            AW_CUDA(band_launch_dp(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S, P.flag,
+                                   ctas, B->st));
+            AW_CUDA(cudaEventRecord(ev[1], B->st));
+            AW_CUDA(band_launch_finish(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S,
+                                       P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), P.mat, P.m, B->st));
+            AW_CUDA(cudaEventRecord(ev[2], B->st));
+            launches += 2;
+        }
+    }
     if (!pl->exact_ids.empty()) {
         int rc = run_exact_ksw(pl->exact_ids.size(), B->order.as<int32_t>() + pl->order.size(),
                                B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), B->pairs.as<KswPair>(),
@@ -515,7 +594,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
 // Waits for plan_launch's work, checks the device error flag, collects timings.
 static int plan_finish(aw_ksw_plan_t *pl, float *ms) {
     Buffers *B = pl->B;
-    const int nw = (int)pl->waves.size();
+    const int nw = (int)(pl->waves.size() + (pl->band_ids.empty() ? 0 : pl->band.waves.size()));
     AW_CUDA(cudaStreamSynchronize(B->st));
     int32_t err = 0;
     AW_CUDA(cudaMemcpy(&err, B->error.p, 4, cudaMemcpyDeviceToHost));

@@ -1,0 +1,95 @@
+// Banded strip kernel for KSW2 extd2 (w >= 0, and the Singletrack traceback at any w):
+// host-side planning and launch interface.
+#pragma once
+#include "aw_internal.h"
+#include <vector>
+
+namespace aw {
+
+// One pair as the banded kernel sees it (device layout).
+struct BandPairDev {
+    int64_t qoff, toff;     // code offsets in the sequence arenas
+    int64_t cig_off;        // word offset of the CIGAR slot (capacity qlen+tlen+2)
+    int32_t qlen, tlen, w;  // w >= 0 (a full-width band is w = max(qlen, tlen))
+    int32_t rb;             // first anti-diagonal the reference does not compute (band break), else qlen+tlen-1
+    int32_t strip0;         // index of this pair's first strip descriptor
+    int32_t nstrip;
+    int32_t idx;            // pair index in the batch (KswOut / KswPair arrays)
+    int32_t pad;
+};
+
+// One 256-column strip: the rows it sweeps and where its traceback and its right-edge
+// column (read by the next strip) live.
+struct BandStripDev {
+    int64_t tb_off;   // bytes into the traceback arena (CIGAR modes)
+    int64_t bnd_off;  // uint2 entries into the boundary arena
+    int32_t jstart;   // first row swept (may be negative: score-fill rows above the matrix)
+    int32_t jlo;      // first stored row, max(0, jstart)
+    int32_t jend;     // last row swept (< jlo: empty strip)
+    int32_t pad;
+};
+
+// Per-pair end tracking merged across strips: (value, position) packed so that an
+// unsigned max keeps the largest value and, among equal values, the later position.
+struct BandRes {
+    unsigned long long mqe_key, mte_key;
+    int32_t score, has_score;
+    int32_t pad[2];
+};
+
+struct BandWave {
+    int pair0, npair;    // slots [pair0, pair0 + npair) of the pair table
+    int unit0, nunit;    // units [unit0, unit0 + nunit) of the unit table
+    int strip0, nstrip;  // strip descriptors used by this wave
+    int64_t tb_bytes, bnd_entries;
+};
+
+struct BandPlan {
+    std::vector<BandPairDev> pairs;
+    std::vector<BandStripDev> strips;
+    std::vector<int2> units;  // (pair slot, strip) in processing order
+    std::vector<BandWave> waves;
+    int64_t tb_cap = 0, bnd_cap = 0, tb_total = 0, cells = 0;
+    int block = 64;
+};
+
+// Geometry of the reference's band (ksw2_extd2_sse.c:147-154): the first anti-diagonal
+// whose band is empty (the reference stops there with zdropped = 1), or qlen+tlen-1.
+int band_break(int qlen, int tlen, int w);
+
+// Sum over anti-diagonals of the in-band cell count en0-st0+1 up to the band break.
+int64_t band_cells(int qlen, int tlen, int w);
+
+// Builds the strip geometry, traceback waves (each under tb_budget bytes) and the
+// processing order of the given pairs.  Returns AW_E_NOMEM_INTERNAL when one pair's
+// traceback alone exceeds the budget.
+int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::vector<int> &qlen,
+                    const std::vector<int> &tlen, const std::vector<int> &w, const std::vector<KswPair> &pairs,
+                    int flag, int block, int64_t tb_budget);
+
+// Progress counters sit one 128-byte line apart (one line per strip).
+constexpr int PROG_STRIDE = 32;
+
+struct BandDev {
+    BandPairDev *pairs;
+    BandStripDev *strips;
+    int2 *units;
+    BandRes *res;
+    int32_t *progress;  // one counter per strip descriptor, PROG_STRIDE ints apart
+    int32_t *queue;     // one counter per wave, 64 ints apart
+    uint2 *bnd;
+    uint8_t *tb;
+    int32_t *error;
+};
+
+int band_occupancy(int flag);
+
+// Enqueues wave k's counter resets and DP kernel.
+cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
+                           const uint8_t *tcodes, const KswScore &S, int flag, int ctas, cudaStream_t st);
+// Enqueues wave k's result records and tracebacks (one thread per pair).
+cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
+                               const uint8_t *tcodes, const KswScore &S, int flag, KswOut *out, uint32_t *cig,
+                               const int8_t *mat, int m, cudaStream_t st);
+
+}  // namespace aw

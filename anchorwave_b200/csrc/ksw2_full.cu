@@ -24,6 +24,7 @@
 // the host-provided order (largest first), so one persistent launch serves a
 // whole batch of uneven pairs.
 #include "aw_internal.h"
+#include "tb_walk.cuh"
 #include <cuda/atomic>
 
 namespace aw {
@@ -345,50 +346,77 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
 
 // ---- traceback -------------------------------------------------------------
 
-struct CigarWriter {
+// CIGAR under construction, replicated in every lane of the walking warp: the open
+// run stays in registers and lane 0 writes a run when the next op differs (the
+// merge rule of ksw_push_cigar, minimap2/ksw2.h:144-154).
+struct WarpCigar {
     uint32_t *buf;
     int n;
-    __device__ void push(uint32_t op, int len) {
-        if (n > 0 && (buf[n - 1] & 0xf) == op) buf[n - 1] += (uint32_t)len << 4;
-        else buf[n++] = (uint32_t)len << 4 | op;
+    uint32_t op;
+    int len;
+    __device__ void push(uint32_t o, int l) {
+        if (len > 0 && o == op) {
+            len += l;
+            return;
+        }
+        if (len > 0 && (threadIdx.x & 31) == 0) buf[n] = (uint32_t)len << 4 | op;
+        if (len > 0) ++n;
+        op = o, len = l;
+    }
+    __device__ int finish(bool reverse) {
+        if (len > 0) {
+            if ((threadIdx.x & 31) == 0) buf[n] = (uint32_t)len << 4 | op;
+            ++n, len = 0;
+        }
+        __syncwarp();
+        if (reverse) {
+            const int lane = threadIdx.x & 31;
+            for (int a = lane; a < n / 2; a += 32) {
+                const uint32_t t = buf[a];
+                buf[a] = buf[n - 1 - a], buf[n - 1 - a] = t;
+            }
+            __syncwarp();
+        }
+        return n;
     }
 };
 
+constexpr int BT_WARPS = 4;
+
 // ksw_backtrack of minimap2/ksw2.h:160-192 over the strip layout; in full mode
 // every visited cell is a stored cell, so the off/off_end forcing never fires.
-__global__ void ksw_backtrack_full_kernel(const KswPair *pairs, const int32_t *order, int n,
-                                          const uint8_t *tb_arena, KswOut *out, uint32_t *cig,
-                                          int flag) {
-    const int pi = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per pair walks in lockstep and fetches traceback tiles cooperatively.
+__global__ void __launch_bounds__(32 * BT_WARPS)
+    ksw_backtrack_full_kernel(const KswPair *pairs, const int32_t *order, int n, const uint8_t *tb_arena,
+                              KswOut *out, uint32_t *cig, int flag) {
+    using Cache = TileCache<8>;
+    __shared__ Cache::Word tiles[BT_WARPS][2 * Cache::NW];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pi = blockIdx.x * BT_WARPS + warp;
     if (pi >= n) return;
     const int idx = order[pi];
     const KswPair P = pairs[idx];
     KswOut o = out[idx];
     const int qlen = P.qlen, tlen = P.tlen;
     int i0 = tlen - 1, j0 = qlen - 1;
-    if (o.zdropped || o.stopped) {
-        out[idx] = o;
-        return;
-    }
+    if (o.zdropped || o.stopped) return;
     if (flag & AW_EZ_SEMIGLOBAL_END) {
         if (o.mqe > o.mte) o.score = o.mqe, i0 = o.mqe_t, j0 = qlen - 1;
         else o.score = o.mte, i0 = tlen - 1, j0 = o.mte_q;
     }
     const uint8_t *tb = tb_arena + P.tb_off;
     const int64_t stride_k = qlen + 31;
-    CigarWriter w{cig + P.cig_off, 0};
+    Cache cache;
+    cache.init(tiles[warp]);
+    auto load = [&](int gg, int jj) -> uint2 {
+        if (gg < 0 || jj < 0 || jj >= qlen || (gg << 3) >= tlen) return make_uint2(0, 0);
+        const int s = gg >> 5, L = gg & 31;
+        return __ldcs(reinterpret_cast<const uint2 *>(tb + (((int64_t)s * stride_k + jj + L) * 32 + L) * KSW_COLS));
+    };
+    WarpCigar w{cig + P.cig_off, 0, 0, 0};
     int i = i0, j = j0, state = 0;
-    int64_t cached_key = -1;
-    uint2 cached = make_uint2(0, 0);
     while (i >= 0 && j >= 0) {
-        const int s = i / KSW_STRIP, lane = (i % KSW_STRIP) / KSW_COLS, c = i % KSW_COLS;
-        const int64_t key = ((int64_t)s * stride_k + j + lane) * 32 + lane;
-        if (key != cached_key) {
-            cached = __ldcs(reinterpret_cast<const uint2 *>(tb + key * KSW_COLS));
-            cached_key = key;
-        }
-        const uint32_t word = c < 4 ? cached.x : cached.y;
-        const uint32_t cellv = (word >> (8 * (c & 3))) & 0xff;
+        const uint32_t cellv = cache.byte(i >> 3, j, i & 7, load);
         if (state == 0) state = cellv & 7;
         else if (!(cellv >> (state + 2) & 1)) state = 0;
         if (state == 0) state = cellv & 7;
@@ -398,14 +426,8 @@ __global__ void ksw_backtrack_full_kernel(const KswPair *pairs, const int32_t *o
     }
     if (i >= 0) w.push(2, i + 1);
     if (j >= 0) w.push(1, j + 1);
-    if (!(flag & AW_EZ_REV_CIGAR)) {
-        for (int a = 0, b = w.n - 1; a < b; ++a, --b) {
-            const uint32_t t = w.buf[a];
-            w.buf[a] = w.buf[b], w.buf[b] = t;
-        }
-    }
-    o.n_cigar = w.n;
-    out[idx] = o;
+    o.n_cigar = w.finish(!(flag & AW_EZ_REV_CIGAR));
+    if (lane == 0) out[idx] = o;
 }
 
 // Copy each pair's CIGAR from its slot to a packed buffer (one warp per pair).
@@ -475,7 +497,8 @@ cudaError_t launch_ksw_backtrack_full(const KswPair *pairs, const int32_t *order
                                       const uint8_t *tb, KswOut *out, uint32_t *cig, int flag,
                                       cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    ksw_backtrack_full_kernel<<<(n + 63) / 64, 64, 0, st>>>(pairs, order, n, tb, out, cig, flag);
+    ksw_backtrack_full_kernel<<<(n + BT_WARPS - 1) / BT_WARPS, 32 * BT_WARPS, 0, st>>>(pairs, order, n, tb, out,
+                                                                                       cig, flag);
     return cudaGetLastError();
 }
 
