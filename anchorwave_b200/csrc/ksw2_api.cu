@@ -51,6 +51,7 @@ static thread_local int64_t tls_tb_budget = 0;  // per-thread override (serving 
 static thread_local bool tls_all_large = false;  // single-pair calls: every pair gets a warp group
 static int g_large_warps = 8;
 static int g_large_tlen = 4096;
+static int g_band_nc = 0;  // banded kernel columns per lane: 0 = chosen per plan, 4 or 8
 static std::mutex g_cfg_mu;
 
 // ---- pooled buffers ----------------------------------------------------------
@@ -308,6 +309,27 @@ struct aw_ksw_plan {
     float dp_ms = 0.f, bt_ms = 0.f;
 };
 
+// Columns per lane of the banded kernel for this plan: 4 halves the pipeline lag between
+// strips (the band edge sweeps a strip in 32*nc rows) at a few percent more work per
+// cell; it pays when the plan is bound by the longest pair's chain of strips rather than
+// by total work.  Estimates: ~1 us per strip row-step on the chain, ~300 GCUPS of work.
+static int band_columns(const aw_ksw_plan_t *pl) {
+    int fixed;
+    {
+        std::lock_guard<std::mutex> lk(g_cfg_mu);
+        fixed = g_band_nc;
+    }
+    if (fixed == 4 || fixed == 8) return fixed;
+    double work = 0.0, chain = 0.0;
+    for (int32_t i : pl->band_ids) {
+        const int ql = pl->qlen[i], tl = pl->tlen[i];
+        const int ww = pl->w[i] < 0 ? std::max(ql, tl) : std::min(pl->w[i], std::max(ql, tl));
+        work += 2.0 * std::min<double>(ww, std::max(ql, tl)) * (double)std::max(ql, tl) / 3e11;
+        chain = std::max(chain, (1.25 * tl + 2.0 * ww + 300.0) * 1e-6);
+    }
+    return chain > work ? 4 : 8;
+}
+
 static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen, const int *w) {
     pl->n = n;
     pl->qlen.assign(qlen, qlen + n);
@@ -412,7 +434,7 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
     }
     if (!pl->band_ids.empty()) {
         if (band_plan_build(pl->band, pl->band_ids, pl->qlen, pl->tlen, pl->w, pl->pairs, P.flag, exact_block(),
-                            budget)) {
+                            budget, band_columns(pl))) {
             set_error("pair traceback exceeds the HBM traceback budget");
             return AW_E_NOMEM;
         }
@@ -673,6 +695,11 @@ int aw_device_count(void) {
 void aw_set_traceback_budget(int64_t bytes) {
     std::lock_guard<std::mutex> lk(g_cfg_mu);
     g_tb_budget = bytes;
+}
+
+void aw_set_band_columns(int columns) {
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    g_band_nc = (columns == 4 || columns == 8) ? columns : 0;
 }
 
 void aw_set_tuning(int large_warps, int large_tlen_threshold) {

@@ -154,16 +154,21 @@ struct BandArgs {
 
 constexpr uint64_t WAIT_NS = 20ull * 1000 * 1000 * 1000;  // bounded wait on the left strip
 
-template <bool CIGAR, bool RIGHT, bool ST>
+// NC target columns per lane (strips of 32*NC columns): 8 for throughput, 4 for a shorter
+// pipeline lag between strips when few long pairs run.
+template <bool CIGAR, bool RIGHT, bool ST, int NC>
 __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
+    constexpr int C = NC;
     // ARGMAX: the state byte is stored (CIGAR without Singletrack)
     constexpr bool ARGMAX = CIGAR && !ST;
     constexpr int CB = ST ? 2 * C : C;  // traceback bytes per lane-step
+    // the block wrap reads column stB+15: lane +D of the stB lane, its last column
+    constexpr int D = 16 / C - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __shared__ uint32_t ring[8][16][32];
     const KswScore &S = A.sc;
     const int B = A.block;
-    const bool src_lane = B > 16 && ((lane * C) & (B - 1)) == C;
+    const bool src_lane = B > 16 && lane >= D && (((lane - D) * C) & (B - 1)) == 0;
 
     for (;;) {
         int u = 0;
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         const int qlen = P.qlen, tlen = P.tlen, qm1 = qlen - 1, tm1 = tlen - 1;
         const int rlim = min(g.nd, g.rb);
         const uint8_t *qs = A.qcodes + P.qoff, *ts = A.tcodes + P.toff;
-        const int col0 = s * KSW_STRIP + lane * C;
+        const int col0 = s * 32 * C + lane * C;
         const bool last_strip = s + 1 == P.nstrip;
         // the strip on the left: its published rows and its final H (an empty strip
         // computes nothing, so its column keeps the initial values)
@@ -349,12 +354,13 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                                 if (st16 == 0) fx = -S.qe, fv = edge_diff(j, S), fx2 = -S.qe2;
                                 else if ((g.st0(r0 - 1) & ~15) == st16) fx = -S.qe, fv = -S.qe, fx2 = -S.qe2;
                             } else if (col0 == stB) {
-                                const uint32_t wv = ring[warp][(k + 1) & 15][lane + 1];
+                                const uint32_t wv = ring[warp][(k + D) & 15][lane + D];
                                 fx = sx8(wv), fv = sx8(wv >> 8), fx2 = sx8(wv >> 16);
                             }
                         }
-                        // score fill right of the band (st0 <= t <= fe, fe up to en0+15): per cell
-                        if (cE < C - 1) {
+                        // score fill right of the band (st0 <= t <= fe, fe <= en0+15 <= (r+w)/2+15,
+                        // i.e. t <= j+w+30): per cell, in the lanes that reach it
+                        if (cE < C - 1 && col0 + cE + 1 <= j + g.w + 30) {
 #pragma unroll
                             for (int c = 0; c < C; ++c) {
                                 const int t = col0 + c, r = r0 + c;
@@ -415,8 +421,13 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                 if (src_lane) ring[warp][k & 15][lane] = carry;
                 if (CIGAR && j >= jlo) {
                     uint8_t *dst = tbp + ((int64_t)(j - jlo + lane) * 32 + lane) * CB;
-                    if (ST) __stcs(reinterpret_cast<uint4 *>(dst), make_uint4(w0, w1, w2, w3));
-                    else __stcs(reinterpret_cast<uint2 *>(dst), make_uint2(w0, w1));
+                    if (C == 8) {
+                        if (ST) __stcs(reinterpret_cast<uint4 *>(dst), make_uint4(w0, w1, w2, w3));
+                        else __stcs(reinterpret_cast<uint2 *>(dst), make_uint2(w0, w1));
+                    } else {
+                        if (ST) __stcs(reinterpret_cast<uint2 *>(dst), make_uint2(w0, w2));
+                        else __stcs(reinterpret_cast<uint32_t *>(dst), w0);
+                    }
                 }
                 if (lane == 31 && !last_strip && j >= jlo) bnd_me[j - jlo] = make_uint2(carry & 0xffffffu, (uint32_t)Hcarry);
             }
@@ -424,7 +435,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                 const int jj = jstart + k - 31;
                 if (jj >= jlo && jj <= jend && (((jj - jlo) & 31) == 31 || jj == jend)) {
                     if (jj == jend) bnd_me[jend - jlo + 1] = make_uint2(init_pack, (uint32_t)Hcarry);
-                    __threadfence();
+                    // the release store orders this lane's boundary writes before the count
                     cuda::atomic_ref<int32_t, cuda::thread_scope_device> pw(*prog_me);
                     pw.store(jj == jend ? jj + 2 : jj + 1, cuda::memory_order_release);
                 }
@@ -497,10 +508,10 @@ constexpr int FIN_WARPS = 4;
 // Result record of one pair, then ksw_backtrack (minimap2/ksw2.h:160-192) with the
 // off/off_end forcing of the band, or the Singletrack reconstruction
 // (minimap2/ksw2_singletrack.cpp:63-176); one warp per pair walks with the tile cache.
-template <bool ST>
+template <bool ST, int NC>
 __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs A) {
-    constexpr int WB = ST ? 16 : 8;
-    using Cache = TileCache<WB, 32, 8>;  // 32 rows x 8 column groups of 8
+    constexpr int WB = ST ? 2 * NC : NC;  // bytes per lane-word: NC columns (v then u for Singletrack)
+    using Cache = TileCache<WB, 32, 64 / NC>;  // 32 rows x 64 columns
     __shared__ typename Cache::Word tiles[FIN_WARPS][2 * Cache::NW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pi = blockIdx.x * FIN_WARPS + warp;
@@ -522,10 +533,10 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
     const uint8_t *tb = A.tb;
     Cache cache;
     cache.init(tiles[warp]);
-    // the stored lane-word of column group gg, row jj (zero outside the stored rows)
+    // the stored lane-word of column group gg (NC columns), row jj (zero outside the stored rows)
     auto load = [&](int gg, int jj) -> typename Cache::Word {
         typename Cache::Word z{};
-        if (gg < 0 || jj < 0 || (gg << 3) >= tlen) return z;
+        if (gg < 0 || jj < 0 || gg * NC >= tlen) return z;
         const int s = gg >> 5, L = gg & 31;
         const BandStripDev St = strips[s];
         if (jj < St.jlo || jj > St.jend) return z;
@@ -547,7 +558,7 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
                 }
                 const int d = i + j;
                 if (i < stB(d) || i > en16(d)) return AW_NEG_INF;
-                return sx8(cache.byte(i >> 3, j, (i & 7) + 8 * part, load));
+                return sx8(cache.byte(i / NC, j, (i % NC) + NC * part, load));
             };
             auto fin = [](int v) { return v > AW_NEG_INF / 2 && v < -AW_NEG_INF / 2; };
             bool in_m = true, valid = true;
@@ -615,7 +626,7 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
                 int force = -1;
                 if (i < stB(r)) force = 2;
                 if (i > en16(r)) force = 1;
-                const uint32_t cellv = force < 0 ? cache.byte(i >> 3, j, i & 7, load) : 0u;
+                const uint32_t cellv = force < 0 ? cache.byte(i / NC, j, i % NC, load) : 0u;
                 if (state == 0) state = cellv & 7;
                 else if (!(cellv >> (state + 2) & 1)) state = 0;
                 if (state == 0) state = cellv & 7;
@@ -634,7 +645,7 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
 
 template <bool CIGAR, bool RIGHT, bool ST>
 void *kernel_ptr() {
-    return (void *)ksw_band_kernel<CIGAR, RIGHT, ST>;
+    return (void *)ksw_band_kernel<CIGAR, RIGHT, ST, 8>;
 }
 
 void *band_kernel_for(int flag, int block) {
@@ -685,12 +696,14 @@ int64_t band_cells(int qlen, int tlen, int w) {
 
 int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::vector<int> &qlen,
                     const std::vector<int> &tlen, const std::vector<int> &w, const std::vector<KswPair> &pairs,
-                    int flag, int block, int64_t tb_budget) {
+                    int flag, int block, int64_t tb_budget, int nc) {
     bp = BandPlan();
     bp.block = block;
+    bp.nc = nc == 4 ? 4 : 8;
+    const int SW = 32 * bp.nc;  // strip width
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY);
     const bool st = cigar && block > 16 && (flag & AW_EZ_SINGLETRACK);
-    const int CB = st ? 16 : 8;  // traceback bytes per lane-step
+    const int CB = st ? 2 * bp.nc : bp.nc;  // traceback bytes per lane-step
     const int B = block;
     struct PairGeo {
         int32_t id, ww, rb;
@@ -705,12 +718,12 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
         const int ww = w[i] < 0 ? std::max(ql, tl) : std::min(w[i], std::max(ql, tl));
         G.id = i, G.ww = ww, G.rb = band_break(ql, tl, ww);
         const int nd = ql + tl - 1;
-        const int nstrip = (int)ceil_div(tl, KSW_STRIP);
+        const int nstrip = (int)ceil_div(tl, SW);
         G.tb = 0, G.bnd = 0;
         int64_t T = 0;
         int prev_js = 0;
         for (int s = 0; s < nstrip; ++s) {
-            const int c0 = s * KSW_STRIP;
+            const int c0 = s * SW;
             BandStripDev sd;
             // rows the strip sweeps: from the first score-fill row of any of its columns
             // (fills reach 15 past en0, so no earlier than c0-w-31, and no row above -15)
@@ -718,7 +731,7 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             sd.jstart = (int)std::max<int64_t>(-15, (int64_t)c0 - ww - 32);
             sd.jlo = std::max(0, sd.jstart);
             int64_t jend = -1;
-            for (int tg = c0; tg < std::min(c0 + KSW_STRIP, tl); tg += B) {
+            for (int tg = c0; tg < std::min(c0 + SW, tl); tg += B) {
                 const int64_t X = (int64_t)tg + B - 1;
                 const int64_t b = std::min<int64_t>(std::min<int64_t>(nd - 1, (int64_t)G.rb - 1),
                                                     std::min<int64_t>(X + ql - 1, 2 * X + ww));
@@ -838,10 +851,17 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY), right = !!(flag & AW_EZ_RIGHT);
     const bool stk = cigar && bp.block > 16 && (flag & AW_EZ_SINGLETRACK);
     const int grid = std::max(1, std::min(ctas, (W.nunit + 7) / 8));
-    if (stk) ksw_band_kernel<true, false, true><<<grid, 256, 0, st>>>(a);
-    else if (cigar && right) ksw_band_kernel<true, true, false><<<grid, 256, 0, st>>>(a);
-    else if (cigar) ksw_band_kernel<true, false, false><<<grid, 256, 0, st>>>(a);
-    else ksw_band_kernel<false, false, false><<<grid, 256, 0, st>>>(a);
+#define AW_BAND_LAUNCH(NCV)                                                                   \
+    if (stk) ksw_band_kernel<true, false, true, NCV><<<grid, 256, 0, st>>>(a);               \
+    else if (cigar && right) ksw_band_kernel<true, true, false, NCV><<<grid, 256, 0, st>>>(a); \
+    else if (cigar) ksw_band_kernel<true, false, false, NCV><<<grid, 256, 0, st>>>(a);        \
+    else ksw_band_kernel<false, false, false, NCV><<<grid, 256, 0, st>>>(a);
+    if (bp.nc == 4) {
+        AW_BAND_LAUNCH(4)
+    } else {
+        AW_BAND_LAUNCH(8)
+    }
+#undef AW_BAND_LAUNCH
     return cudaGetLastError();
 }
 
@@ -856,10 +876,14 @@ cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, cons
     memcpy(b.mat, mat, (size_t)m * m);
     b.m = m, b.flag = flag, b.block = bp.block;
     const int grid = (W.npair + FIN_WARPS - 1) / FIN_WARPS;
-    if (b.block > 16 && (flag & AW_EZ_SINGLETRACK) && !(flag & AW_EZ_SCORE_ONLY))
-        ksw_band_finish_kernel<true><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
-    else
-        ksw_band_finish_kernel<false><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
+    const bool stk = b.block > 16 && (flag & AW_EZ_SINGLETRACK) && !(flag & AW_EZ_SCORE_ONLY);
+    if (bp.nc == 4) {
+        if (stk) ksw_band_finish_kernel<true, 4><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
+        else ksw_band_finish_kernel<false, 4><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
+    } else {
+        if (stk) ksw_band_finish_kernel<true, 8><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
+        else ksw_band_finish_kernel<false, 8><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
+    }
     return cudaGetLastError();
 }
 

@@ -51,6 +51,7 @@ struct BandPlan {
     std::vector<BandWave> waves;
     int64_t tb_cap = 0, bnd_cap = 0, tb_total = 0, cells = 0;
     int block = 64;
+    int nc = 8;  // target columns per lane: strips of 32*nc columns
 };
 
 // Geometry of the reference's band (ksw2_extd2_sse.c:147-154): the first anti-diagonal
@@ -65,7 +66,7 @@ int64_t band_cells(int qlen, int tlen, int w);
 // traceback alone exceeds the budget.
 int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::vector<int> &qlen,
                     const std::vector<int> &tlen, const std::vector<int> &w, const std::vector<KswPair> &pairs,
-                    int flag, int block, int64_t tb_budget);
+                    int flag, int block, int64_t tb_budget, int nc);
 
 // Progress counters sit one 128-byte line apart (one line per strip).
 constexpr int PROG_STRIDE = 32;

@@ -15,12 +15,13 @@
 
 namespace aw {
 
-// WB: bytes per lane-word, 8 (state bytes) or 16 (Singletrack v|u tracks); a tile is
+// WB: bytes per lane-word, 4 or 8 (state bytes) or 16 (Singletrack v|u tracks); a tile is
 // TR_ rows (matrix rows, or anti-diagonals for the anti-diagonal layout) x TG_ groups.
 template <int WB, int TR_ = 32, int TG_ = 8>
 struct TileCache {
     static constexpr int TR = TR_, TG = TG_, NW = TR * TG;
-    using Word = typename std::conditional<WB == 16, uint4, uint2>::type;
+    using Word = typename std::conditional<WB == 16, uint4,
+                                           typename std::conditional<WB == 8, uint2, uint32_t>::type>::type;
     Word *slot[2];  // shared memory, NW words each
     int g0[2], j0[2];
     int next;
@@ -55,9 +56,11 @@ struct TileCache {
         if (WB == 16) {
             const uint4 &q = reinterpret_cast<const uint4 &>(wd);
             x = c < 4 ? q.x : c < 8 ? q.y : c < 12 ? q.z : q.w;
-        } else {
+        } else if (WB == 8) {
             const uint2 &q = reinterpret_cast<const uint2 &>(wd);
             x = c < 4 ? q.x : q.y;
+        } else {
+            x = reinterpret_cast<const uint32_t &>(wd);
         }
         return (x >> (8 * (c & 3))) & 0xffu;
     }

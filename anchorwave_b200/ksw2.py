@@ -229,6 +229,11 @@ def set_traceback_budget(nbytes: int):
     lib.aw_set_traceback_budget(int(nbytes))
 
 
+def set_band_columns(columns: int = 0):
+    """Target columns per lane of the banded kernel: 4, 8, or 0 to choose per batch."""
+    lib.aw_set_band_columns(int(columns))
+
+
 def set_tuning(large_warps: int = 0, large_tlen_threshold: int = 0):
     lib.aw_set_tuning(int(large_warps), int(large_tlen_threshold))
 

@@ -221,6 +221,9 @@ void aw_set_traceback_budget(int64_t bytes);
 /* Warps that cooperate on one pair for pairs with tlen >= threshold, and the
  * threshold (autotuner knobs; 0 keeps the current value). */
 void aw_set_tuning(int large_warps, int large_tlen_threshold);
+/* Target columns per lane of the banded kernel (4 or 8; 0 = chosen per batch from
+ * its work and its longest pair).  No counterpart in the reference (tuning knob). */
+void aw_set_band_columns(int columns);
 const char *aw_last_error(void);
 int aw_device_count(void);
 /* Integer-ALU peak probe: IADD3/IMNMX-class 32-bit ops per second measured on

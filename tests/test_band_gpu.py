@@ -45,22 +45,29 @@ def _check(gpu, restatement, qs, ts, ws, pen, flag, mat=None):
     assert not bad, f"{len(bad)} of {len(qs)} differ, first {bad[:4]} flag={hex(flag)} pen={pen}"
 
 
+@pytest.fixture(params=[8, 4], ids=["cols8", "cols4"])
+def columns(request, gpu):
+    gpu.set_band_columns(request.param)
+    yield request.param
+    gpu.set_band_columns(0)
+
+
 @pytest.mark.parametrize("pen", PEN)
 @pytest.mark.parametrize("flag", [0, SCORE_ONLY, RIGHT, REV, SEMI])
-def test_banded_batch_vs_restatement(gpu, restatement, pen, flag):
+def test_banded_batch_vs_restatement(gpu, restatement, columns, pen, flag):
     qs, ts, ws = _pairs(1000 + flag + pen[0], 48, 1, 1500)
     _check(gpu, restatement, qs, ts, ws, pen, flag)
 
 
 @pytest.mark.parametrize("flag", [0, RIGHT])
-def test_banded_generic_scoring_with_n(gpu, restatement, flag):
+def test_banded_generic_scoring_with_n(gpu, restatement, columns, flag):
     qs, ts, ws = _pairs(77 + flag, 40, 10, 1200, nfrac=0.6)
     _check(gpu, restatement, qs, ts, ws, (4, 2, 24, 1), GENERIC | flag)
 
 
 @pytest.mark.parametrize("pen", PEN[:3])
 @pytest.mark.parametrize("banded", [False, True])
-def test_singletrack_vs_restatement(gpu, restatement, pen, banded):
+def test_singletrack_vs_restatement(gpu, restatement, columns, pen, banded):
     qs, ts, ws = _pairs(300 + pen[0] + banded, 40, 1, 1500, wfrac=(0.02, 0.6) if banded else (1.0, 1.0))
     _check(gpu, restatement, qs, ts, ws if banded else [-1] * len(qs), pen, ST)
 
@@ -74,7 +81,7 @@ def test_singletrack_single_calls(gpu, restatement):
         assert r.key() == o.key(), (len(q), len(t), w)
 
 
-def test_band_break_and_tiny(gpu, restatement):
+def test_band_break_and_tiny(gpu, restatement, columns):
     """Bands too narrow to reach the end (zdropped, KSW_NEG_INF score), w = 0..3 and
     one-base sequences."""
     rng = np.random.default_rng(11)
@@ -89,7 +96,7 @@ def test_band_break_and_tiny(gpu, restatement):
         _check(gpu, restatement, qs, ts, ws, (4, 2, 24, 1), flag)
 
 
-def test_long_banded_vs_restatement(gpu, restatement):
+def test_long_banded_vs_restatement(gpu, restatement, columns):
     """Multi-strip pairs whose strips run on many warps at once, with long indels."""
     rng = np.random.default_rng(21)
     qs, ts, ws = [], [], []
