@@ -185,17 +185,17 @@ def long_banded_set(n: int = 64, seed: int = 3, lmin: int = 100_000, lmax: int =
 
 
 def band_cells(qlen: int, tlen: int, w: int) -> int:
-    """Sum over anti-diagonals of the in-band cell count en0-st0+1 (ksw2_extd2_sse.c:147-150)."""
-    if w < 0:
+    """Sum over anti-diagonals of the in-band cell count en0-st0+1 (ksw2_extd2_sse.c:147-150),
+    up to the first empty band (where the reference stops)."""
+    if w < 0 or w > max(qlen, tlen):
         w = max(qlen, tlen)
-    total = 0
-    for r in range(qlen + tlen - 1):
-        st = max(0, r - qlen + 1, (r - w + 1) >> 1)
-        en = min(tlen - 1, r, (r + w) >> 1)
-        if st > en:
-            break
-        total += en - st + 1
-    return total
+    r = np.arange(qlen + tlen - 1, dtype=np.int64)
+    st = np.maximum(np.maximum(0, r - qlen + 1), (r - w + 1) >> 1)
+    en = np.minimum(np.minimum(tlen - 1, r), (r + w) >> 1)
+    bad = np.nonzero(st > en)[0]
+    if len(bad):
+        st, en = st[: bad[0]], en[: bad[0]]
+    return int((en - st + 1).sum())
 
 
 @dataclass

@@ -52,8 +52,9 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-sample", type=int, default=64)
-    ap.add_argument("--serve-requests", type=int, default=0,
+    ap.add_argument("--serve-requests", type=int, default=20000,
                     help="requests of the serving trace (0 skips the serving measurement)")
+    ap.add_argument("--no-long-banded", action="store_true", help="skip the long banded/Singletrack sample")
     return ap.parse_args()
 
 
@@ -261,6 +262,55 @@ def serving_measurement(nreq: int, rank: int):
                      "and <=10 kb, >20 kb banded (w=10%), 10% repeat-rich; Poisson arrivals at 80% of saturation"}
 
 
+def long_banded_measurement(rank: int, cpu: bool):
+    """The long-interval banded and Singletrack workload at reduced lengths (16 pairs,
+    100-150 kb, w = 10% of the shorter length, repeat-rich queries with long indels): band
+    GCUPS on the GPU for both tracebacks, and the reference's own CPU code on the same
+    pairs (one thread per pair) with a per-pair result-hash comparison."""
+    import numpy as np
+
+    from anchorwave_b200 import ksw2
+    from anchorwave_b200 import workloads as W
+    ps = W.long_banded_set(16, seed=3 + rank, lmin=100_000, lmax=150_000, long_max=10_000)
+    mat = ksw2.anchorwave_matrix(-4)
+    bcells = sum(W.band_cells(len(q), len(t), w) for q, t, w in zip(ps.queries, ps.targets, ps.band))
+    out = {"workload": ps.name, "pairs": len(ps), "band_cells": bcells,
+           "shape": "target U(100 kb, 150 kb), 30% repeats, 3% substitutions, long indels up to 10 kb, w = 10%"}
+    results = {}
+    for name, flag in (("banded", 0), ("singletrack", 0x1000)):
+        plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1, w=ps.band, flag=flag)
+        plan.upload()
+        plan.execute()
+        ms = min(plan.execute() for _ in range(2))
+        dp, bt = plan.timing()
+        results[name] = plan.download()
+        plan.close()
+        out[name] = {"ms": ms, "dp_ms": dp, "traceback_ms": bt, "gcups": bcells / (ms * 1e-3) / 1e9}
+    if cpu:
+        from concurrent.futures import ThreadPoolExecutor
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        try:
+            ref = oracle.Reference()
+        except FileNotFoundError as e:
+            out["cpu_reference"] = {"unavailable": str(e)}
+            return out
+        for name, variant in (("banded", 0), ("singletrack", 2)):
+            def one(i):
+                r = ref.ksw_batch([ps.queries[i].tobytes()], [ps.targets[i].tobytes()], mat, 4, 2, 24, 1,
+                                  w=ps.band[i], variant=variant, nthreads=1)
+                return int(r["hash"][0])
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(len(ps)) as ex:
+                hashes = list(ex.map(one, range(len(ps))))
+            secs = time.perf_counter() - t0
+            same = all(oracle.result_hash(g) == h for g, h in zip(results[name], hashes))
+            out[name]["cpu_reference"] = {"seconds": secs, "gcups": bcells / secs / 1e9, "threads": len(ps),
+                                          "isa": ref.isa, "results_identical": same}
+            out[name]["vs_cpu_reference"] = out[name]["gcups"] / (bcells / secs / 1e9)
+    return out
+
+
 def cpu_baseline(ps, budget):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
@@ -361,6 +411,7 @@ def main():
              "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)), "sample_pairs": len(lat)}
 
     serving = serving_measurement(args.serve_requests, rank) if args.serve_requests > 0 else None
+    long_banded = None if args.no_long_banded else long_banded_measurement(rank, rank == 0 and not args.no_cpu_baseline)
 
     if rank != 0:
         barrier(pg)
@@ -398,6 +449,7 @@ def main():
                 "d2h_bytes_per_step": d2h, "pairs_per_s": world * n / e2e_step,
                 "results_identical_to_device_path": identical},
         "serving": serving,
+        "long_banded": long_banded,
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }
