@@ -50,7 +50,13 @@ struct Req {
     std::string q, t;  // ASCII
     int64_t pred;
     double t_submit;
+    int generic;  // KSW2: a base outside ACGT (generic scoring), computed at submit
+    int bucket;   // length class: requests of one class share a micro-batch
 };
+
+// Length classes keep short intervals out of micro-batches that a long interval
+// would hold for the whole of its (much longer) alignment.
+int length_bucket(int64_t len) { return len <= 4000 ? 0 : len <= 20000 ? 1 : 2; }
 
 struct Res {
     aw_serve_result_t r;
@@ -109,19 +115,16 @@ struct aw_server {
 namespace {
 
 // Pops one micro-batch: the oldest request plus later ones of the same class
-// (engine, scoring flag) while they fit the batch size and the budget.
+// (engine, scoring flag, length class) while they fit the batch size and the budget.
 bool take_batch(aw_server *S, std::vector<Req> &batch) {
     batch.clear();
     if (S->queue.empty()) return false;
     const Req &head = S->queue.front();
     const int64_t budget = S->cfg.hbm_budget;
     if (S->inflight_bytes > 0 && S->inflight_bytes + head.pred > budget) return false;
-    std::vector<uint8_t> tmp;
-    // requests of one class share a launch: same engine and KSW2 scoring flag (bands may differ)
-    auto klass = [&](const Req &r) {
-        const bool gen = r.method <= AW_ROUTE_KSW2_SINGLETRACK && (encode(r.q, tmp) | encode(r.t, tmp));
-        return std::make_tuple(r.method, gen);
-    };
+    // requests of one class share a launch: same engine, KSW2 scoring flag and length class
+    // (bands may differ)
+    auto klass = [](const Req &r) { return std::make_tuple(r.method, r.generic, r.bucket); };
     const auto k0 = klass(head);
     int64_t bytes = 0;
     for (auto it = S->queue.begin(); it != S->queue.end() && (int)batch.size() < S->cfg.max_batch;) {
@@ -281,6 +284,12 @@ int aw_serve_submit(aw_server_t *S, uint64_t id, int method, int band, const cha
     r.q.assign(query ? query : "", (size_t)qlen);
     r.t.assign(target ? target : "", (size_t)tlen);
     r.pred = predict_bytes(r);
+    r.generic = 0;
+    if (method <= AW_ROUTE_KSW2_SINGLETRACK) {
+        std::vector<uint8_t> tmp;
+        r.generic = (encode(r.q, tmp) | encode(r.t, tmp)) ? 1 : 0;
+    }
+    r.bucket = length_bucket(std::max<int64_t>(qlen, tlen));
     r.t_submit = now_s();
     {
         std::lock_guard<std::mutex> lk(S->mu);
