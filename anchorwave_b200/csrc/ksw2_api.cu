@@ -78,7 +78,7 @@ struct PinBuf {
 struct Buffers {
     DevBuf qcodes, tcodes, pairs, order, out, cig, packed, packed_off, tb, bnd, queue, error;
     DevBuf exact_ws;
-    DevBuf band_pairs, band_strips, band_units, band_res, band_progress, band_bnd, band_queue;
+    DevBuf band_pairs, band_strips, band_units, band_res, band_progress, band_bnd, band_queue, band_walk;
     PinBuf h_band;
     PinBuf h_codes, h_pairs, h_order, h_out, h_packed, h_packed_off, h_small;
     cudaStream_t st = nullptr, st2 = nullptr;
@@ -91,7 +91,7 @@ struct Buffers {
         cig.release(); packed.release(); packed_off.release(); tb.release(); bnd.release();
         queue.release(); error.release(); exact_ws.release();
         band_pairs.release(); band_strips.release(); band_units.release(); band_res.release();
-        band_progress.release(); band_bnd.release(); band_queue.release(); h_band.release();
+        band_progress.release(); band_bnd.release(); band_queue.release(); band_walk.release(); h_band.release();
         h_codes.release(); h_pairs.release(); h_order.release(); h_out.release();
         h_packed.release(); h_packed_off.release(); h_small.release();
         for (auto e : ev_k) cudaEventDestroy(e);
@@ -468,6 +468,7 @@ static int plan_alloc(aw_ksw_plan_t *pl) {
         AW_CUDA(B->band_strips.ensure(sizeof(BandStripDev) * bp.strips.size()));
         AW_CUDA(B->band_units.ensure(sizeof(int2) * bp.units.size()));
         AW_CUDA(B->band_res.ensure(sizeof(BandRes) * bp.pairs.size()));
+        AW_CUDA(B->band_walk.ensure(sizeof(BandWalkState) * bp.pairs.size()));
         AW_CUDA(B->band_progress.ensure(sizeof(int32_t) * PROG_STRIDE * bp.strips.size()));
         AW_CUDA(B->band_bnd.ensure(sizeof(uint2) * (size_t)bp.bnd_cap + 256));
         AW_CUDA(B->band_queue.ensure(sizeof(int32_t) * 64 * bp.waves.size()));
@@ -585,6 +586,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         BandDev D;
         D.pairs = B->band_pairs.as<BandPairDev>(), D.strips = B->band_strips.as<BandStripDev>();
         D.units = B->band_units.as<int2>(), D.res = B->band_res.as<BandRes>();
+        D.walk = B->band_walk.as<BandWalkState>();
         D.progress = B->band_progress.as<int32_t>(), D.queue = B->band_queue.as<int32_t>();
         D.bnd = B->band_bnd.as<uint2>(), D.tb = B->tb.as<uint8_t>(), D.error = B->error.as<int32_t>();
         const int ctas = band_occupancy(P.flag) * B->sms;
@@ -596,8 +598,17 @@ static int plan_launch(aw_ksw_plan_t *pl) {
             AW_CUDA(cudaEventRecord(ev[1], B->st));
             AW_CUDA(band_launch_finish(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S,
                                        P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), P.mat, P.m, B->st));
-            AW_CUDA(cudaEventRecord(ev[2], B->st));
             launches += 2;
+            const BandWave &BW = pl->band.waves[k];
+            if (BW.ngroup > 0) {
+                AW_CUDA(band_launch_groups(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S,
+                                           P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), P.mat, P.m, ctas,
+                                           B->st));
+                int lasts = 0;
+                for (int gi = BW.group0; gi < BW.group0 + BW.ngroup; ++gi) lasts += pl->band.groups[gi].last;
+                launches += 3 * BW.ngroup + lasts;  // counters, strips, walk per group; tail per pair
+            }
+            AW_CUDA(cudaEventRecord(ev[2], B->st));
         }
     }
     if (!pl->exact_ids.empty()) {

@@ -150,6 +150,7 @@ struct BandArgs {
     BandRes *res;
     KswScore sc;
     int block, generic;
+    int store_ckpt;  // 1: store the traceback of recomputed pairs too (their group passes)
 };
 
 constexpr uint64_t WAIT_NS = 20ull * 1000 * 1000 * 1000;  // bounded wait on the left strip
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                     Hcarry = Hf;
                 }
                 if (src_lane) ring[warp][k & 15][lane] = carry;
-                if (CIGAR && j >= jlo) {
+                if (CIGAR && j >= jlo && (!P.ckpt || A.store_ckpt)) {
                     uint8_t *dst = tbp + ((int64_t)(j - jlo + lane) * 32 + lane) * CB;
                     if (C == 8) {
                         if (ST) __stcs(reinterpret_cast<uint4 *>(dst), make_uint4(w0, w1, w2, w3));
@@ -495,6 +496,7 @@ struct BtArgs {
     const BandStripDev *strips;
     const uint8_t *tb;
     const BandRes *res;
+    BandWalkState *walk;
     const uint8_t *qcodes, *tcodes;
     KswOut *out;
     uint32_t *cig;
@@ -502,6 +504,28 @@ struct BtArgs {
     int8_t mat[64];
     int m, flag, block;
 };
+
+// ksw_backtrack (minimap2/ksw2.h:160-192) over the strip layout with the band's
+// off/off_end forcing, run in lockstep by a warp; stops when the walk ends or leaves the
+// columns >= col_lo.
+template <int NC, class Cache, class Load>
+__device__ void band_walk(int &i, int &j, int &state, int col_lo, WarpCig &cg, Cache &cache, Load &load,
+                          const Geom &g) {
+    while (i >= 0 && j >= 0 && i >= col_lo) {
+        const int r = i + j;
+        int force = -1;
+        if (i < (g.st0(r) & g.bmask)) force = 2;
+        if (i > (g.en0(r) | 15)) force = 1;
+        const uint32_t cellv = force < 0 ? cache.byte(i / NC, j, i % NC, load) : 0u;
+        if (state == 0) state = cellv & 7;
+        else if (!(cellv >> (state + 2) & 1)) state = 0;
+        if (state == 0) state = cellv & 7;
+        if (force >= 0) state = force;
+        if (state == 0) cg.push(0, 1), --i, --j;
+        else if (state == 1 || state == 3) cg.push(2, 1), --i;
+        else cg.push(1, 1), --j;
+    }
+}
 
 constexpr int FIN_WARPS = 4;
 
@@ -619,28 +643,76 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
         } else if (!o.zdropped && !(flag & AW_EZ_EXTZ_ONLY)) {
             i0 = tlen - 1, j0 = qlen - 1;
         }
-        if (i0 >= 0 || j0 >= 0) {
-            int i = i0, j = j0, state = 0;
-            while (i >= 0 && j >= 0) {
-                const int r = i + j;
-                int force = -1;
-                if (i < stB(r)) force = 2;
-                if (i > en16(r)) force = 1;
-                const uint32_t cellv = force < 0 ? cache.byte(i / NC, j, i % NC, load) : 0u;
-                if (state == 0) state = cellv & 7;
-                else if (!(cellv >> (state + 2) & 1)) state = 0;
-                if (state == 0) state = cellv & 7;
-                if (force >= 0) state = force;
-                if (state == 0) cg.push(0, 1), --i, --j;
-                else if (state == 1 || state == 3) cg.push(2, 1), --i;
-                else cg.push(1, 1), --j;
+        if (P.ckpt) {
+            // traceback recomputed group by group (ksw_band_walk_kernel); start state only
+            if (lane == 0) {
+                BandWalkState w;
+                w.i = i0, w.j = j0, w.state = 0, w.n = 0, w.op = 0, w.len = 0, w.pad = 0;
+                w.done = (i0 >= 0 || j0 >= 0) ? 0 : 1;
+                A.walk[pi] = w;
             }
+        } else if (i0 >= 0 || j0 >= 0) {
+            int i = i0, j = j0, state = 0;
+            band_walk<NC>(i, j, state, 0, cg, cache, load, g);
             if (i >= 0) cg.push(2, i + 1);
             if (j >= 0) cg.push(1, j + 1);
             o.n_cigar = cg.finish(!(flag & AW_EZ_REV_CIGAR));
         }
     }
     if (lane == 0) A.out[P.idx] = o;
+}
+
+// One group of a recomputed pair: continue the ksw_backtrack walk through the group's
+// freshly stored traceback until it leaves the group on the left (or ends).
+template <int NC>
+__global__ void __launch_bounds__(32) ksw_band_walk_kernel(BtArgs A, int slot, int col_lo) {
+    using Cache = TileCache<NC, 32, 64 / NC>;
+    __shared__ typename Cache::Word tiles[2 * Cache::NW];
+    BandWalkState w = A.walk[slot];
+    if (w.done) return;
+    const BandPairDev P = A.pairs[slot];
+    const Geom g{P.qlen, P.tlen, P.w, P.qlen + P.tlen - 1, P.rb, ~(A.block - 1)};
+    const int tlen = P.tlen;
+    const BandStripDev *strips = A.strips + P.strip0;
+    const uint8_t *tb = A.tb;
+    Cache cache;
+    cache.init(tiles);
+    auto load = [&](int gg, int jj) -> typename Cache::Word {
+        typename Cache::Word z{};
+        if (gg < 0 || jj < 0 || gg * NC >= tlen || gg * NC < col_lo) return z;
+        const int s = gg >> 5, L = gg & 31;
+        const BandStripDev St = strips[s];
+        if (jj < St.jlo || jj > St.jend) return z;
+        const uint8_t *p = tb + St.tb_off + ((int64_t)(jj - St.jlo + L) * 32 + L) * NC;
+        return __ldcs(reinterpret_cast<const typename Cache::Word *>(p));
+    };
+    WarpCig cg{A.cig + P.cig_off, w.n, (uint32_t)w.op, w.len};
+    int i = w.i, j = w.j, state = w.state;
+    band_walk<NC>(i, j, state, col_lo, cg, cache, load, g);
+    if ((threadIdx.x & 31) == 0) {
+        w.i = i, w.j = j, w.state = state, w.n = cg.n, w.op = (int)cg.op, w.len = cg.len;
+        A.walk[slot] = w;
+    }
+}
+
+// The end of a recomputed pair's walk: the leading gap, the reversal, the CIGAR length.
+__global__ void __launch_bounds__(32) ksw_band_walk_finish_kernel(BtArgs A, int slot) {
+    BandWalkState w = A.walk[slot];
+    if (w.done) return;
+    const BandPairDev P = A.pairs[slot];
+    WarpCig cg{A.cig + P.cig_off, w.n, (uint32_t)w.op, w.len};
+    if (w.i >= 0) cg.push(2, w.i + 1);
+    if (w.j >= 0) cg.push(1, w.j + 1);
+    const int n = cg.finish(!(A.flag & AW_EZ_REV_CIGAR));
+    if ((threadIdx.x & 31) == 0) A.out[P.idx].n_cigar = n;
+}
+
+// Progress counters of a group pass: the group's strips start from zero, the strip on its
+// left (not recomputed: its boundary column is stored from the first pass) counts as done.
+__global__ void band_group_progress_kernel(int32_t *progress, int s_first, int s_end, int left) {
+    const int k = s_first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < s_end) progress[PROG_STRIDE * k] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && left >= 0) progress[PROG_STRIDE * left] = INT_MAX / 2;
 }
 
 template <bool CIGAR, bool RIGHT, bool ST>
@@ -708,8 +780,12 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
     struct PairGeo {
         int32_t id, ww, rb;
         int64_t tb, bnd;
+        bool ckpt = false;
         std::vector<BandStripDev> strips;
         std::vector<int64_t> start;  // estimated start step of each strip
+        std::vector<int64_t> stb;    // traceback bytes of each strip
+        std::vector<std::pair<int, int>> groups;  // recomputed pairs: strip groups [s0, s1)
+        std::vector<int64_t> gtb;
     };
     std::vector<PairGeo> geo(ids.size());
     for (size_t a = 0; a < ids.size(); ++a) {
@@ -741,10 +817,13 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             const int64_t rows = sd.jend >= sd.jlo ? (int64_t)sd.jend - sd.jlo + 1 : 0;
             sd.tb_off = G.tb;  // relative to the pair until the wave is packed
             sd.bnd_off = G.bnd;
+            int64_t stb = 0;
             if (rows > 0) {
-                if (cigar) G.tb += (rows + 31) * 32 * CB;
+                if (cigar) stb = (rows + 31) * 32 * CB;
+                G.tb += stb;
                 G.bnd += rows + 1;
             }
+            G.stb.push_back(stb);
             // estimated start: the left strip must have swept this strip's first rows
             T += (s == 0 ? 0 : std::max(0, sd.jstart - prev_js) + 64);
             prev_js = sd.jstart;
@@ -754,7 +833,30 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
         G.tb = (G.tb + 255) / 256 * 256;
         bp.tb_total += G.tb;
         bp.cells += band_cells(ql, tl, ww);
-        if (G.tb > tb_budget) return AW_E_NOMEM_INTERNAL;
+        if (G.tb > tb_budget) {
+            // Traceback beyond the budget: the first pass stores only the strips' boundary
+            // columns; the walk then recomputes groups of strips that fit the budget, from
+            // the last group to the first, each from the stored column on its left.  The
+            // Singletrack reconstruction probes arbitrarily far left in one gap search, so it
+            // is not split this way.
+            if (st) return AW_E_NOMEM_INTERNAL;
+            G.ckpt = true;
+            int s0 = 0;
+            int64_t acc = 0;
+            for (int s = 0; s < (int)G.strips.size(); ++s) {
+                if (G.stb[s] > tb_budget) return AW_E_NOMEM_INTERNAL;
+                if (acc + G.stb[s] > tb_budget) {
+                    G.groups.push_back({s0, s});
+                    G.gtb.push_back(acc);
+                    s0 = s, acc = 0;
+                }
+                G.strips[s].tb_off = acc;  // relative to the group's buffer
+                acc += G.stb[s];
+            }
+            G.groups.push_back({s0, (int)G.strips.size()});
+            G.gtb.push_back(acc);
+            G.tb = 0;  // the first pass stores no traceback
+        }
     }
     // pairs largest first into the fewest waves under the budget (LPT multiway fit)
     std::vector<size_t> ord(ids.size());
@@ -795,12 +897,12 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             pd.qlen = kp.qlen, pd.tlen = kp.tlen, pd.w = G.ww, pd.rb = G.rb;
             pd.strip0 = (int)bp.strips.size();
             pd.nstrip = (int)G.strips.size();
-            pd.idx = G.id, pd.pad = 0;
+            pd.idx = G.id, pd.ckpt = G.ckpt ? 1 : 0;
             const int slot = (int)bp.pairs.size();
             bp.pairs.push_back(pd);
             for (size_t s = 0; s < G.strips.size(); ++s) {
                 BandStripDev sd = G.strips[s];
-                sd.tb_off += tb;
+                if (!G.ckpt) sd.tb_off += tb;
                 sd.bnd_off += bnd;
                 bp.strips.push_back(sd);
                 us.push_back(U{G.start[s], slot, (int)s});
@@ -818,6 +920,26 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
         W.tb_bytes = tb, W.bnd_entries = bnd;
         bp.tb_cap = std::max(bp.tb_cap, tb);
         bp.bnd_cap = std::max(bp.bnd_cap, bnd);
+        // checkpoint groups of this wave's recomputed pairs, last group first
+        W.group0 = (int)bp.groups.size();
+        for (int slot = W.pair0; slot < W.pair0 + W.npair; ++slot) {
+            const BandPairDev &pd = bp.pairs[slot];
+            if (!pd.ckpt) continue;
+            const PairGeo &G = *std::find_if(geo.begin(), geo.end(), [&](const PairGeo &x) { return x.id == pd.idx; });
+            for (int gi = (int)G.groups.size() - 1; gi >= 0; --gi) {
+                BandGroup gr;
+                gr.slot = slot, gr.s0 = G.groups[gi].first, gr.s1 = G.groups[gi].second;
+                gr.unit0 = (int)bp.units.size();
+                for (int s = gr.s0; s < gr.s1; ++s) bp.units.push_back(make_int2(slot, s));
+                gr.nunit = gr.s1 - gr.s0;
+                gr.col_lo = gr.s0 * SW;
+                gr.last = gi == 0 ? 1 : 0;
+                gr.tb_bytes = G.gtb[gi];
+                bp.tb_cap = std::max(bp.tb_cap, G.gtb[gi]);
+                bp.groups.push_back(gr);
+            }
+        }
+        W.ngroup = (int)bp.groups.size() - W.group0;
         bp.waves.push_back(W);
     }
     return 0;
@@ -828,6 +950,8 @@ int band_occupancy(int flag) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, band_kernel_for(flag, 64), 256, 0) != cudaSuccess) return 1;
     return std::max(nb, 1);
 }
+
+cudaError_t band_launch_units(const BandPlan &bp, const BandArgs &a, int flag, int ctas, cudaStream_t st);
 
 cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
                            const uint8_t *tcodes, const KswScore &S, int flag, int ctas, cudaStream_t st) {
@@ -848,9 +972,14 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
     a.sc = S;
     a.block = bp.block;
     a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
+    a.store_ckpt = 0;
+    return band_launch_units(bp, a, flag, ctas, st);
+}
+
+cudaError_t band_launch_units(const BandPlan &bp, const BandArgs &a, int flag, int ctas, cudaStream_t st) {
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY), right = !!(flag & AW_EZ_RIGHT);
     const bool stk = cigar && bp.block > 16 && (flag & AW_EZ_SINGLETRACK);
-    const int grid = std::max(1, std::min(ctas, (W.nunit + 7) / 8));
+    const int grid = std::max(1, std::min(ctas, (a.n_units + 7) / 8));
 #define AW_BAND_LAUNCH(NCV)                                                                   \
     if (stk) ksw_band_kernel<true, false, true, NCV><<<grid, 256, 0, st>>>(a);               \
     else if (cigar && right) ksw_band_kernel<true, true, false, NCV><<<grid, 256, 0, st>>>(a); \
@@ -871,6 +1000,7 @@ cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, cons
     const BandWave &W = bp.waves[k];
     BtArgs b;
     b.pairs = D.pairs + W.pair0, b.npair = W.npair, b.strips = D.strips, b.tb = D.tb, b.res = D.res + W.pair0;
+    b.walk = D.walk + W.pair0;
     b.qcodes = qcodes, b.tcodes = tcodes, b.out = out, b.cig = cig, b.sc = S;
     memset(b.mat, 0, sizeof(b.mat));
     memcpy(b.mat, mat, (size_t)m * m);
@@ -885,6 +1015,49 @@ cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, cons
         else ksw_band_finish_kernel<false, 8><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
     }
     return cudaGetLastError();
+}
+
+cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
+                               const uint8_t *tcodes, const KswScore &S, int flag, KswOut *out, uint32_t *cig,
+                               const int8_t *mat, int m, int ctas, cudaStream_t st) {
+    const BandWave &W = bp.waves[k];
+    cudaError_t e;
+    BtArgs b;
+    b.pairs = D.pairs, b.npair = (int)bp.pairs.size(), b.strips = D.strips, b.tb = D.tb, b.res = D.res;
+    b.walk = D.walk;
+    b.qcodes = qcodes, b.tcodes = tcodes, b.out = out, b.cig = cig, b.sc = S;
+    memset(b.mat, 0, sizeof(b.mat));
+    memcpy(b.mat, mat, (size_t)m * m);
+    b.m = m, b.flag = flag, b.block = bp.block;
+    for (int gi = W.group0; gi < W.group0 + W.ngroup; ++gi) {
+        const BandGroup &G = bp.groups[gi];
+        const BandPairDev &P = bp.pairs[G.slot];
+        const int sfirst = P.strip0 + G.s0, send = P.strip0 + G.s1;
+        band_group_progress_kernel<<<(G.nunit + 255) / 256, 256, 0, st>>>(D.progress, sfirst, send,
+                                                                          G.s0 > 0 ? sfirst - 1 : -1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        // this group's counter of the work queue: the wave's slot, reused per group
+        if ((e = cudaMemsetAsync(D.queue + 64 * k, 0, sizeof(int32_t), st)) != cudaSuccess) return e;
+        BandArgs a;
+        a.qcodes = qcodes, a.tcodes = tcodes;
+        a.pairs = D.pairs, a.strips = D.strips, a.units = D.units + G.unit0;
+        a.n_units = G.nunit;
+        a.queue = D.queue + 64 * k, a.progress = D.progress, a.error = D.error;
+        a.tb = D.tb, a.bnd = D.bnd, a.res = D.res;
+        a.sc = S;
+        a.block = bp.block;
+        a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
+        a.store_ckpt = 1;
+        if ((e = band_launch_units(bp, a, flag, ctas, st)) != cudaSuccess) return e;
+        if (bp.nc == 4) ksw_band_walk_kernel<4><<<1, 32, 0, st>>>(b, G.slot, G.col_lo);
+        else ksw_band_walk_kernel<8><<<1, 32, 0, st>>>(b, G.slot, G.col_lo);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (G.last) {
+            ksw_band_walk_finish_kernel<<<1, 32, 0, st>>>(b, G.slot);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
 }  // namespace aw

@@ -15,7 +15,7 @@ struct BandPairDev {
     int32_t strip0;         // index of this pair's first strip descriptor
     int32_t nstrip;
     int32_t idx;            // pair index in the batch (KswOut / KswPair arrays)
-    int32_t pad;
+    int32_t ckpt;           // 1: traceback too large for the budget; recomputed strip group by group
 };
 
 // One 256-column strip: the rows it sweeps and where its traceback and its right-edge
@@ -42,10 +42,30 @@ struct BandWave {
     int unit0, nunit;    // units [unit0, unit0 + nunit) of the unit table
     int strip0, nstrip;  // strip descriptors used by this wave
     int64_t tb_bytes, bnd_entries;
+    int group0, ngroup;  // checkpoint groups of this wave's recomputed pairs, in walk order
+};
+
+// Walk state of a pair whose traceback is recomputed group by group (see band_plan_build).
+struct BandWalkState {
+    int32_t i, j, state;   // ksw_backtrack position and state
+    int32_t n, op, len;    // CIGAR runs written, the open run
+    int32_t done, pad;     // 1: nothing (left) to walk
+};
+
+// A group of consecutive strips [s0, s1) of one recomputed pair: its traceback fits the
+// budget; the walk visits groups from the last to the first.
+struct BandGroup {
+    int slot;           // pair slot
+    int s0, s1;
+    int unit0, nunit;   // units of this group (its strips, left to right)
+    int col_lo;         // first target column of the group
+    int last;           // 1: the pair's first group (the walk ends here)
+    int64_t tb_bytes;
 };
 
 struct BandPlan {
     std::vector<BandPairDev> pairs;
+    std::vector<BandGroup> groups;
     std::vector<BandStripDev> strips;
     std::vector<int2> units;  // (pair slot, strip) in processing order
     std::vector<BandWave> waves;
@@ -76,6 +96,7 @@ struct BandDev {
     BandStripDev *strips;
     int2 *units;
     BandRes *res;
+    BandWalkState *walk;  // per pair slot
     int32_t *progress;  // one counter per strip descriptor, PROG_STRIDE ints apart
     int32_t *queue;     // one counter per wave, 64 ints apart
     uint2 *bnd;
@@ -88,9 +109,14 @@ int band_occupancy(int flag);
 // Enqueues wave k's counter resets and DP kernel.
 cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
                            const uint8_t *tcodes, const KswScore &S, int flag, int ctas, cudaStream_t st);
-// Enqueues wave k's result records and tracebacks (one thread per pair).
+// Enqueues wave k's result records and tracebacks (one warp per pair).
 cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
                                const uint8_t *tcodes, const KswScore &S, int flag, KswOut *out, uint32_t *cig,
                                const int8_t *mat, int m, cudaStream_t st);
+// Enqueues the group-by-group traceback of wave k's recomputed pairs: for each group,
+// its strips again with their traceback stored, then the walk through them.
+cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
+                               const uint8_t *tcodes, const KswScore &S, int flag, KswOut *out, uint32_t *cig,
+                               const int8_t *mat, int m, int ctas, cudaStream_t st);
 
 }  // namespace aw

@@ -148,3 +148,20 @@ def test_banded_repeatable_and_waves(gpu, restatement):
             assert [r.key() for r in res] == exp, budget
     finally:
         gpu.set_traceback_budget(0)
+
+
+@pytest.mark.parametrize("flag", [0, RIGHT, REV, SEMI])
+def test_checkpointed_traceback(gpu, restatement, columns, flag):
+    """Pairs whose traceback exceeds the budget: boundary columns on the first pass, then
+    the walk recomputes strip groups from the last to the first.  A 2 MB budget splits each
+    pair into several groups."""
+    qs, ts, ws = _pairs(88 + flag, 10, 2000, 9000, wfrac=(0.05, 0.3))
+    mat = oracle.anchorwave_matrix(-4)
+    try:
+        gpu.set_traceback_budget(2 << 20)
+        res = gpu.ksw_extd2_batch(qs, ts, mat, 4, 2, 24, 1, w=ws, flag=flag)
+    finally:
+        gpu.set_traceback_budget(0)
+    for q, t, w, r in zip(qs, ts, ws, res):
+        o = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, w=w, flag=flag)
+        assert r.key() == o.key(), (len(q), len(t), w)
