@@ -80,6 +80,18 @@ __device__ __forceinline__ ScoreHdr *hdr_ptr(const WfaArgs &A, const int64_t *ct
     return (ScoreHdr *)(A.pool + ctab[s / HDR_CHUNK]) + (s % HDR_CHUNK);
 }
 
+// The forward pass reads the headers of the last max_score_scope scores only; each warp
+// keeps them in a shared-memory ring of RS (a power of two above the scope) as well as in
+// the pool (the backtrace reads all of them from the pool).  RS = 0: pool only.
+struct HdrRing {
+    ScoreHdr *ring;
+    int rs;
+    __device__ __forceinline__ const ScoreHdr *get(const WfaArgs &A, const int64_t *ctab, int sc, int s) const {
+        if (rs && sc > s - rs) return ring + (sc & (rs - 1));
+        return hdr_ptr(A, ctab, sc);
+    }
+};
+
 __device__ __forceinline__ int32_t getv(const WfaArgs &A, const CompHdr &h, int k) {
     if (k < h.lo || k > h.hi) return WF_NULL;
     return ((const int32_t *)(A.pool + h.off))[k - h.base];
@@ -98,31 +110,6 @@ __device__ __forceinline__ bool in_matrix(int32_t o, int k, int plen, int tlen) 
     return (uint32_t)o <= (uint32_t)tlen && (uint32_t)(o - k) <= (uint32_t)plen;
 }
 
-// Trim [lo, hi] of one component (wavefront/wavefront_compute.c:654-690), warp-parallel.
-__device__ void warp_trim(const int32_t *d, int base, int &lo, int &hi, int plen, int tlen, int lane) {
-    int nh = lo - 1;
-    for (int top = hi; top >= lo; top -= 32) {
-        const int k = top - lane;
-        const bool ok = k >= lo && in_matrix(d[k - base], k, plen, tlen);
-        const unsigned b = __ballot_sync(0xffffffffu, ok);
-        if (b) {
-            nh = top - (__ffs(b) - 1);
-            break;
-        }
-    }
-    int nl = nh + 1;
-    for (int bot = lo; bot <= nh; bot += 32) {
-        const int k = bot + lane;
-        const bool ok = k <= nh && in_matrix(d[k - base], k, plen, tlen);
-        const unsigned b = __ballot_sync(0xffffffffu, ok);
-        if (b) {
-            nl = bot + (__ffs(b) - 1);
-            break;
-        }
-    }
-    lo = nl, hi = nh;
-}
-
 __device__ __forceinline__ int64_t pb(int32_t o, int t) {
     return (int64_t)((((uint64_t)(int64_t)o) << 4) | (uint64_t)t);
 }
@@ -139,9 +126,11 @@ struct OpsWriter {
     }
 };
 
-__global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
+__global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
     const int lane = threadIdx.x & 31;
     const WfaPen P = A.pen;
+    extern __shared__ ScoreHdr hring_all[];
+    const HdrRing HR{hring_all + (threadIdx.x >> 5) * rs, rs};
     for (;;) {
         int pi = 0;
         if (lane == 0) pi = atomicAdd(A.queue, 1);
@@ -181,6 +170,7 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
             for (int c = 0; c < 5; ++c) H->c[c] = CompHdr{1, -1, 0, 0, 0};
             H->c[CM] = CompHdr{0, 0, 0, 0, d0};
             *(int32_t *)(A.pool + d0) = 0;
+            if (HR.rs) HR.ring[0] = *H;
         }
         __syncwarp();
         const int k_end = tlen - plen;
@@ -189,27 +179,50 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
         while (status == 0) {
             // ---- extend M[s] and check the end
             {
-                const ScoreHdr *H = hdr_ptr(A, ctab, s);
-                const CompHdr m = H->c[CM];
+                const CompHdr m = HR.get(A, ctab, s, s)->c[CM];
+                bool reached = false;
                 if (m.lo <= m.hi) {
                     int32_t *d = (int32_t *)(A.pool + m.off);
-                    for (int k = m.lo + lane; k <= m.hi; k += 32) {
-                        const int32_t o = d[k - m.base];
-                        if (o == WF_NULL) continue;
-                        int64_t v = (int64_t)o - k, h = o;
-                        for (;;) {
-                            const uint64_t x = load8(pat, v) ^ load8(txt, h);
-                            if (x) {
-                                const int nb = (__ffsll((long long)x) - 1) >> 3;
-                                v += nb, h += nb;
-                                break;
-                            }
-                            v += 8, h += 8;
+                    // four diagonals per lane at a time, so their loads overlap
+                    for (int k0 = m.lo + lane; k0 <= m.hi; k0 += 128) {
+                        int32_t o[4];
+                        int64_t v[4], h[4];
+                        bool run[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int k = k0 + 32 * u;
+                            o[u] = k <= m.hi ? d[k - m.base] : WF_NULL;
+                            run[u] = o[u] != WF_NULL;
+                            v[u] = (int64_t)o[u] - k, h[u] = o[u];
                         }
-                        d[k - m.base] = (int32_t)h;
+                        bool any = run[0] || run[1] || run[2] || run[3];
+                        while (any) {
+                            uint64_t x[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) x[u] = run[u] ? (load8(pat, v[u]) ^ load8(txt, h[u])) : 0;
+                            any = false;
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                if (!run[u]) continue;
+                                if (x[u]) {
+                                    const int nb = (__ffsll((long long)x[u]) - 1) >> 3;
+                                    v[u] += nb, h[u] += nb;
+                                    run[u] = false;
+                                } else {
+                                    v[u] += 8, h[u] += 8;
+                                    any = true;
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int k = k0 + 32 * u;
+                            if (k <= m.hi && o[u] != WF_NULL) d[k - m.base] = (int32_t)h[u];
+                            // end-to-end check on the lane that holds diagonal tlen-plen
+                            if (k == k_end && o[u] != WF_NULL && h[u] >= tlen) reached = true;
+                        }
                     }
-                    __syncwarp();
-                    if (m.lo <= k_end && k_end <= m.hi && d[k_end - m.base] >= tlen) {
+                    if (__any_sync(0xffffffffu, reached)) {
                         end_score = s;
                         break;
                     }
@@ -236,19 +249,22 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
             ScoreHdr *OH = hdr_ptr(A, ctab, s);
             const CompHdr NUL{1, -1, 0, 0, 0};
             const int sm = s - P.x, so1 = s - P.o1 - P.e1, se1 = s - P.e1, so2 = s - P.o2 - P.e2, se2 = s - P.e2;
-            const CompHdr m_misms = sm >= 0 ? hdr_ptr(A, ctab, sm)->c[CM] : NUL;
-            const CompHdr m_open1 = so1 >= 0 ? hdr_ptr(A, ctab, so1)->c[CM] : NUL;
-            const CompHdr i1 = se1 >= 0 ? hdr_ptr(A, ctab, se1)->c[CI1] : NUL;
-            const CompHdr d1 = se1 >= 0 ? hdr_ptr(A, ctab, se1)->c[CD1] : NUL;
-            const CompHdr m_open2 = so2 >= 0 ? hdr_ptr(A, ctab, so2)->c[CM] : NUL;
-            const CompHdr i2 = se2 >= 0 ? hdr_ptr(A, ctab, se2)->c[CI2] : NUL;
-            const CompHdr d2 = se2 >= 0 ? hdr_ptr(A, ctab, se2)->c[CD2] : NUL;
+            const CompHdr m_misms = sm >= 0 ? HR.get(A, ctab, sm, s)->c[CM] : NUL;
+            const CompHdr m_open1 = so1 >= 0 ? HR.get(A, ctab, so1, s)->c[CM] : NUL;
+            const CompHdr i1 = se1 >= 0 ? HR.get(A, ctab, se1, s)->c[CI1] : NUL;
+            const CompHdr d1 = se1 >= 0 ? HR.get(A, ctab, se1, s)->c[CD1] : NUL;
+            const CompHdr m_open2 = so2 >= 0 ? HR.get(A, ctab, so2, s)->c[CM] : NUL;
+            const CompHdr i2 = se2 >= 0 ? HR.get(A, ctab, se2, s)->c[CI2] : NUL;
+            const CompHdr d2 = se2 >= 0 ? HR.get(A, ctab, se2, s)->c[CD2] : NUL;
             const bool n_mm = m_misms.lo > m_misms.hi, n_o1 = m_open1.lo > m_open1.hi, n_i1 = i1.lo > i1.hi,
                        n_d1 = d1.lo > d1.hi, n_o2 = m_open2.lo > m_open2.hi, n_i2 = i2.lo > i2.hi,
                        n_d2 = d2.lo > d2.hi;
             if (n_mm && n_o1 && n_i1 && n_d1 && n_o2 && n_i2 && n_d2) {
-                if (lane == 0)
+                if (lane == 0) {
                     for (int c = 0; c < 5; ++c) OH->c[c] = NUL;
+                    if (HR.rs)
+                        for (int c = 0; c < 5; ++c) HR.ring[s & (HR.rs - 1)].c[c] = NUL;
+                }
                 __syncwarp();
                 ++num_null;
                 continue;
@@ -294,29 +310,55 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
             int32_t *oD1 = a_d1 ? (int32_t *)(A.pool + out[CD1].off) : nullptr;
             int32_t *oI2 = a_i2 ? (int32_t *)(A.pool + out[CI2].off) : nullptr;
             int32_t *oD2 = a_d2 ? (int32_t *)(A.pool + out[CD2].off) : nullptr;
-            for (int k = lo + lane; k <= hi; k += 32) {
-                const int32_t ins1 = max(getv(A, m_open1, k - 1), getv(A, i1, k - 1)) + 1;
-                const int32_t ins2 = max(getv(A, m_open2, k - 1), getv(A, i2, k - 1)) + 1;
-                const int32_t del1 = max(getv(A, m_open1, k + 1), getv(A, d1, k + 1));
-                const int32_t del2 = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
-                const int32_t misms = getv(A, m_misms, k) + 1;
-                int32_t best = max(max(del1, del2), max(misms, max(ins1, ins2)));
-                if (!in_matrix(best, k, plen, tlen)) best = WF_NULL;
-                oM[k - lo] = best;
-                if (oI1) oI1[k - lo] = ins1;
-                if (oD1) oD1[k - lo] = del1;
-                if (oI2) oI2[k - lo] = ins2;
-                if (oD2) oD2[k - lo] = del2;
+            // trimmed ends (wavefront/wavefront_compute.c:654-690): the lowest and highest
+            // diagonal whose offset lies in the matrix, per component, from the lanes' values
+            int kmin[5], kmax[5];
+#pragma unroll
+            for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
+            // four diagonals per lane at a time: all input loads before any output store
+            for (int k0 = lo + lane; k0 <= hi; k0 += 128) {
+                int32_t ins1[4], ins2[4], del1[4], del2[4], misms[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = k0 + 32 * u;
+                    ins1[u] = max(getv(A, m_open1, k - 1), getv(A, i1, k - 1)) + 1;
+                    ins2[u] = max(getv(A, m_open2, k - 1), getv(A, i2, k - 1)) + 1;
+                    del1[u] = max(getv(A, m_open1, k + 1), getv(A, d1, k + 1));
+                    del2[u] = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
+                    misms[u] = getv(A, m_misms, k) + 1;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = k0 + 32 * u;
+                    if (k > hi) break;
+                    int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
+                    if (!in_matrix(best, k, plen, tlen)) best = WF_NULL;
+                    oM[k - lo] = best;
+                    if (oI1) oI1[k - lo] = ins1[u];
+                    if (oD1) oD1[k - lo] = del1[u];
+                    if (oI2) oI2[k - lo] = ins2[u];
+                    if (oD2) oD2[k - lo] = del2[u];
+                    const int32_t vals[5] = {best, ins1[u], del1[u], ins2[u], del2[u]};
+#pragma unroll
+                    for (int c = 0; c < 5; ++c)
+                        if (in_matrix(vals[c], k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
+                }
             }
             __syncwarp();
+#pragma unroll
             for (int c = 0; c < 5; ++c) {
                 if (!alloc_c[c]) continue;
-                int tl = out[c].lo, th = out[c].hi;
-                warp_trim((const int32_t *)(A.pool + out[c].off), out[c].base, tl, th, plen, tlen, lane);
-                out[c].lo = tl, out[c].hi = th;
+                const int th = __reduce_max_sync(0xffffffffu, kmax[c]);
+                const int tl = __reduce_min_sync(0xffffffffu, kmin[c]);
+                // no diagonal in the matrix: the empty range [lo, lo-1] of the scan
+                if (th == INT_MIN) out[c].hi = out[c].lo - 1;
+                else out[c].lo = tl, out[c].hi = th;
             }
-            if (lane == 0)
+            if (lane == 0) {
                 for (int c = 0; c < 5; ++c) OH->c[c] = out[c];
+                if (HR.rs)
+                    for (int c = 0; c < 5; ++c) HR.ring[s & (HR.rs - 1)].c[c] = out[c];
+            }
             __syncwarp();
         }
         // ---- backtrace (lane 0)
@@ -468,14 +510,29 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A) {
 
 }  // namespace
 
+// Header ring size for a score scope: the smallest power of two above it, 32..128
+// (shared memory of 4 warps x 128 x 120 B at most), or 0 (pool reads) beyond.
+static int ring_size(int scope) {
+    int rs = 32;
+    while (rs <= scope && rs < 256) rs <<= 1;
+    return rs <= 128 ? rs : 0;
+}
+
 cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st) {
-    wfa_kernel<<<ctas, 128, 0, st>>>(a);
+    const int rs = ring_size(a.max_score_scope);
+    const size_t smem = (size_t)4 * rs * sizeof(ScoreHdr);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(wfa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    wfa_kernel<<<ctas, 128, smem, st>>>(a, rs);
     return cudaGetLastError();
 }
 
 int wfa_occupancy() {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_kernel, 128, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_kernel, 128, 4 * 32 * sizeof(ScoreHdr)) != cudaSuccess)
+        return 1;
     return nb;
 }
 
