@@ -708,6 +708,13 @@ void aw_set_traceback_budget(int64_t bytes) {
     g_tb_budget = bytes;
 }
 
+void aw_release_thread_buffers(void) {
+    if (tls_buf) {
+        delete tls_buf;
+        tls_buf = nullptr;
+    }
+}
+
 void aw_set_band_columns(int columns) {
     std::lock_guard<std::mutex> lk(g_cfg_mu);
     g_band_nc = (columns == 4 || columns == 8) ? columns : 0;

@@ -229,6 +229,11 @@ def set_traceback_budget(nbytes: int):
     lib.aw_set_traceback_budget(int(nbytes))
 
 
+def release_thread_buffers():
+    """Free the device/pinned buffers this thread's batch calls keep pooled."""
+    lib.aw_release_thread_buffers()
+
+
 def set_band_columns(columns: int = 0):
     """Target columns per lane of the banded kernel: 4, 8, or 0 to choose per batch."""
     lib.aw_set_band_columns(int(columns))

@@ -48,6 +48,33 @@ class WfaAligner:
         lib.wavefront_gpu_cigar(self.h, C.byref(ops), C.byref(n), C.byref(score))
         return (C.string_at(ops, n.value).decode() if n.value else ""), score.value
 
+    def align_batch_raw(self, patterns: Sequence[bytes], texts: Sequence[bytes]):
+        """One submission of n alignments without decoding: (status, score, ops offsets, ops
+        lengths, ops buffer, device ms, seconds spent in the C call)."""
+        import time
+        n = len(patterns)
+        pbufs = [C.create_string_buffer(p, len(p) + 1) for p in patterns]
+        tbufs = [C.create_string_buffer(t, len(t) + 1) for t in texts]
+        pp = (C.c_void_p * n)(*[C.addressof(b) for b in pbufs])
+        tp = (C.c_void_p * n)(*[C.addressof(b) for b in tbufs])
+        pl = np.array([len(p) for p in patterns], dtype=np.int32)
+        tl = np.array([len(t) for t in texts], dtype=np.int32)
+        status = np.zeros(n, dtype=np.int32)
+        score = np.zeros(n, dtype=np.int32)
+        offs = np.zeros(n, dtype=np.int64)
+        nops = np.zeros(n, dtype=np.int32)
+        cap = int(pl.sum() + tl.sum()) + 1
+        ops = C.create_string_buffer(cap)
+        ms = C.c_float(0.0)
+        t0 = time.perf_counter()
+        rc = lib.wavefront_align_batch_gpu(self.h, n, pp, pl.ctypes.data, tp, tl.ctypes.data, status.ctypes.data,
+                                           score.ctypes.data, offs.ctypes.data, nops.ctypes.data, ops, cap,
+                                           C.byref(ms))
+        secs = time.perf_counter() - t0
+        if rc != 0:
+            raise AwError(f"wavefront_align_batch_gpu failed ({rc}): {last_error()}")
+        return status, score, offs, nops, ops, ms.value, secs
+
     def align_batch(self, patterns: Sequence[bytes], texts: Sequence[bytes]):
         """n alignments in one submission: list of (status, score, ops) plus device ms."""
         n = len(patterns)

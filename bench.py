@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=20000,
                     help="requests of the serving trace (0 skips the serving measurement)")
     ap.add_argument("--no-long-banded", action="store_true", help="skip the long banded/Singletrack sample")
+    ap.add_argument("--long-banded-pairs", type=int, default=16)
+    ap.add_argument("--long-banded-min", type=int, default=100_000)
+    ap.add_argument("--long-banded-max", type=int, default=150_000)
+    ap.add_argument("--wfa-pairs", type=int, default=16384, help="pairs of the batched WFA workload (0 skips it)")
     return ap.parse_args()
 
 
@@ -263,7 +267,53 @@ def serving_measurement(nreq: int, rank: int):
                      "cells = sum of qlen*tlen"}
 
 
-def long_banded_measurement(rank: int, cpu: bool):
+def wfa_measurement(npairs: int, rank: int, cpu: bool):
+    """The batched gap-affine-2p WFA workload (lengths log-uniform 100 bp-10 kb, divergence
+    0.5-5%, penalties x=4, o1=4, e1=2, o2=24, e2=1), standard and Singletrack: pairs/s on the
+    device and through the C call with host buffers, and the reference's WFA2 code on the host
+    cores on the same pairs (scores and CIGAR lengths compared)."""
+    import numpy as np
+
+    from anchorwave_b200 import wfa
+    from anchorwave_b200 import workloads as W
+    ps = W.batched_wfa_set(npairs, seed=2 + rank)
+    pats = [W.to_ascii(t) for t in ps.targets]
+    txts = [W.to_ascii(q) for q in ps.queries]
+    out = {"workload": ps.name, "pairs": len(ps), "matrix_cells": ps.cells()}
+    dev = {}
+    for name, stk in (("standard", False), ("singletrack", True)):
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=stk)
+        al.align_batch_raw(pats[:64], txts[:64])
+        runs = [al.align_batch_raw(pats, txts) for _ in range(2)]
+        al.close()
+        st, sc, offs, nops, ops, ms, secs = min(runs, key=lambda r: r[5])
+        dev[name] = (st, sc, nops)
+        out[name] = {"device_ms": ms, "pairs_per_s": len(ps) / (ms * 1e-3),
+                     "e2e_pairs_per_s": len(ps) / min(r[6] for r in runs),
+                     "gcups_equivalent": ps.cells() / (ms * 1e-3) / 1e9,
+                     "completed": int(np.sum(st == 0))}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        try:
+            ref = oracle.Reference()
+        except FileNotFoundError as e:
+            out["cpu_reference"] = {"unavailable": str(e)}
+            return out
+        for name, stk in (("standard", False), ("singletrack", True)):
+            # the helper takes (queries, targets) and aligns pattern = target, text = query
+            r = ref.wfa_batch(txts, pats, 4, 4, 2, 24, 1, singletrack=stk, time_budget_s=10.0)
+            done = [i for i in range(len(ps)) if r["n_ops"][i] > 0]
+            st, sc, nops = dev[name]
+            same = all(st[i] == 0 and sc[i] == r["score"][i] and nops[i] == r["n_ops"][i] for i in done)
+            cpu_pps = r["done"] / r["seconds"]
+            out[name]["cpu_reference"] = {"pairs_per_s": cpu_pps, "threads": r["threads"], "pairs": len(done),
+                                          "scores_and_cigar_lengths_identical": same}
+            out[name]["vs_cpu_reference"] = out[name]["pairs_per_s"] / cpu_pps
+    return out
+
+
+def long_banded_measurement(rank: int, cpu: bool, npairs: int = 16, lmin: int = 100_000, lmax: int = 150_000):
     """The long-interval banded and Singletrack workload at reduced lengths (16 pairs,
     100-150 kb, w = 10% of the shorter length, repeat-rich queries with long indels): band
     GCUPS on the GPU for both tracebacks, and the reference's own CPU code on the same
@@ -272,11 +322,12 @@ def long_banded_measurement(rank: int, cpu: bool):
 
     from anchorwave_b200 import ksw2
     from anchorwave_b200 import workloads as W
-    ps = W.long_banded_set(16, seed=3 + rank, lmin=100_000, lmax=150_000, long_max=10_000)
+    ps = W.long_banded_set(npairs, seed=3 + rank, lmin=lmin, lmax=lmax, long_max=max(1, lmin // 10))
     mat = ksw2.anchorwave_matrix(-4)
     bcells = sum(W.band_cells(len(q), len(t), w) for q, t, w in zip(ps.queries, ps.targets, ps.band))
     out = {"workload": ps.name, "pairs": len(ps), "band_cells": bcells,
-           "shape": "target U(100 kb, 150 kb), 30% repeats, 3% substitutions, long indels up to 10 kb, w = 10%"}
+           "shape": f"target U({lmin // 1000} kb, {lmax // 1000} kb), 30% repeats, 3% substitutions, "
+                    f"long indels up to {max(1, lmin // 10) // 1000} kb, w = 10%"}
     results = {}
     for name, flag in (("banded", 0), ("singletrack", 0x1000)):
         plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1, w=ps.band, flag=flag)
@@ -411,8 +462,14 @@ def main():
              "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
              "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)), "sample_pairs": len(lat)}
 
+    # the batch calls above keep ~100 GB of traceback arena pooled on this thread; give it
+    # back before the other workloads size their own device pools
+    ksw2.release_thread_buffers()
     serving = serving_measurement(args.serve_requests, rank) if args.serve_requests > 0 else None
-    long_banded = None if args.no_long_banded else long_banded_measurement(rank, rank == 0 and not args.no_cpu_baseline)
+    long_banded = None if args.no_long_banded else long_banded_measurement(
+        rank, rank == 0 and not args.no_cpu_baseline, args.long_banded_pairs, args.long_banded_min,
+        args.long_banded_max)
+    wfa_res = wfa_measurement(args.wfa_pairs, rank, rank == 0 and not args.no_cpu_baseline) if args.wfa_pairs > 0 else None
 
     if rank != 0:
         barrier(pg)
@@ -451,6 +508,7 @@ def main():
                 "results_identical_to_device_path": identical},
         "serving": serving,
         "long_banded": long_banded,
+        "wfa": wfa_res,
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }

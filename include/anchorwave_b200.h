@@ -224,6 +224,10 @@ void aw_set_tuning(int large_warps, int large_tlen_threshold);
 /* Target columns per lane of the banded kernel (4 or 8; 0 = chosen per batch from
  * its work and its longest pair).  No counterpart in the reference (tuning knob). */
 void aw_set_band_columns(int columns);
+/* Frees the device and pinned buffers that the calling thread's KSW2 calls keep pooled
+ * between calls (they grow to the largest batch seen; the next call re-creates them).
+ * No counterpart in the reference (its work arrays are per call). */
+void aw_release_thread_buffers(void);
 const char *aw_last_error(void);
 int aw_device_count(void);
 /* Integer-ALU peak probe: IADD3/IMNMX-class 32-bit ops per second measured on
