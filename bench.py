@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--long-banded-min", type=int, default=100_000)
     ap.add_argument("--long-banded-max", type=int, default=150_000)
     ap.add_argument("--wfa-pairs", type=int, default=16384, help="pairs of the batched WFA workload (0 skips it)")
+    ap.add_argument("--wfa-pool-gb", type=float, default=0.0,
+                    help="device wavefront pool of the WFA workload (0: most of the free memory)")
     return ap.parse_args()
 
 
@@ -267,7 +269,7 @@ def serving_measurement(nreq: int, rank: int):
                      "cells = sum of qlen*tlen"}
 
 
-def wfa_measurement(npairs: int, rank: int, cpu: bool):
+def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
     """The batched gap-affine-2p WFA workload (lengths log-uniform 100 bp-10 kb, divergence
     0.5-5%, penalties x=4, o1=4, e1=2, o2=24, e2=1), standard and Singletrack: pairs/s on the
     device and through the C call with host buffers, and the reference's WFA2 code on the host
@@ -282,7 +284,7 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool):
     out = {"workload": ps.name, "pairs": len(ps), "matrix_cells": ps.cells()}
     dev = {}
     for name, stk in (("standard", False), ("singletrack", True)):
-        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=stk)
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=stk, max_memory_abort=int(pool_gb * 2**30))
         al.align_batch_raw(pats[:64], txts[:64])
         runs = [al.align_batch_raw(pats, txts) for _ in range(2)]
         al.close()
@@ -469,7 +471,8 @@ def main():
     long_banded = None if args.no_long_banded else long_banded_measurement(
         rank, rank == 0 and not args.no_cpu_baseline, args.long_banded_pairs, args.long_banded_min,
         args.long_banded_max)
-    wfa_res = wfa_measurement(args.wfa_pairs, rank, rank == 0 and not args.no_cpu_baseline) if args.wfa_pairs > 0 else None
+    wfa_res = (wfa_measurement(args.wfa_pairs, rank, rank == 0 and not args.no_cpu_baseline, args.wfa_pool_gb)
+               if args.wfa_pairs > 0 else None)
 
     if rank != 0:
         barrier(pg)
