@@ -26,7 +26,8 @@ EXPORTS = [
     "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "aw_ksw_extd2_batch",
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_free",
-    "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_release_thread_buffers", "aw_last_error", "aw_device_count",
+    "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_release_thread_buffers",
+    "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops", "aw_ksw_extd2_device_noalloc",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
     "wavefront_align_batch_gpu", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
@@ -96,6 +97,10 @@ def _load(path: str = LIB_PATH):
     lib.aw_set_band_columns.restype = None
     lib.aw_release_thread_buffers.argtypes = []
     lib.aw_release_thread_buffers.restype = None
+    lib.aw_ksw_set_deadline.argtypes = [C.c_double]
+    lib.aw_ksw_set_deadline.restype = None
+    lib.aw_ksw_set_stop_antidiagonal.argtypes = [i32, i32]
+    lib.aw_ksw_set_stop_antidiagonal.restype = None
     lib.aw_last_error.argtypes = []
     lib.aw_last_error.restype = C.c_char_p
     lib.aw_device_count.argtypes = []

@@ -59,7 +59,19 @@ struct KswFullArgs {
     int32_t *queue;           // work-queue head (device counter)
     int32_t *error;           // set non-zero if a bounded wait gave up
     KswScore sc;
+    // the calling thread's deadline (globaltimer ns) or null: pairs still running when it
+    // passes stop with ez->stopped = 1 (the cooperative stop of minimap2/ksw2_progress.c)
+    const unsigned long long *deadline = nullptr;
 };
+
+#ifdef __CUDACC__
+__device__ __forceinline__ bool aw_deadline_passed(const unsigned long long *d) {
+    if (!d) return false;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t >= *(const volatile unsigned long long *)d;
+}
+#endif
 
 // Traceback geometry of the strip kernel: 32 lanes x KSW_COLS target columns per
 // strip; one byte per cell at  ((strip * (qlen + 31) + step) * 32 + lane) * KSW_COLS + col
@@ -113,6 +125,9 @@ cudaError_t launch_ksw_full(const KswFullArgs &a, int flag, int warps_per_pair,
 cudaError_t launch_ksw_backtrack_full(const KswPair *pairs, const int32_t *order, int n,
                                       const uint8_t *tb, KswOut *out, uint32_t *cig,
                                       int flag, cudaStream_t st);
+// Writes globaltimer + remaining_ns (or "never" for ~0) to *deadline on the stream, so
+// the deadline counts from when the stream reaches this call.
+cudaError_t launch_set_deadline(unsigned long long *deadline, unsigned long long remaining_ns, cudaStream_t st);
 cudaError_t launch_ksw_pack_cigar(const KswPair *pairs, int n, const KswOut *out,
                                   const uint32_t *cig, const int64_t *packed_off,
                                   uint32_t *packed, cudaStream_t st);

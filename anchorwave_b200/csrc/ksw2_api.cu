@@ -17,6 +17,7 @@
 #include "../../include/anchorwave_b200.h"
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -36,6 +37,13 @@ void set_error(const char *s) {
     if (getenv("AW_VERBOSE")) fprintf(stderr, "[aw_b200] %s\n", s);
 }
 static void set_error(const std::string &s) { set_error(s.c_str()); }
+
+// ---- cooperative stop ------------------------------------------------------
+// The calling thread's deadline, the state ksw_set_progress_callback keeps per thread
+// (minimap2/ksw2_progress.c:11-13) when AnchorWave's ScopedKswDeadline installs its
+// probe (alignSlidingWindow.cpp:593-640).
+static thread_local bool tls_has_deadline = false;
+static thread_local std::chrono::steady_clock::time_point tls_deadline;
 #define AW_CUDA(call)                                                                   \
     do {                                                                                \
         cudaError_t _e = (call);                                                        \
@@ -77,7 +85,7 @@ struct PinBuf {
 
 struct Buffers {
     DevBuf qcodes, tcodes, pairs, order, out, cig, packed, packed_off, tb, bnd, queue, error;
-    DevBuf exact_ws;
+    DevBuf exact_ws, deadline;
     DevBuf band_pairs, band_strips, band_units, band_res, band_progress, band_bnd, band_queue, band_walk;
     PinBuf h_band;
     PinBuf h_codes, h_pairs, h_order, h_out, h_packed, h_packed_off, h_small;
@@ -89,7 +97,7 @@ struct Buffers {
     ~Buffers() {
         qcodes.release(); tcodes.release(); pairs.release(); order.release(); out.release();
         cig.release(); packed.release(); packed_off.release(); tb.release(); bnd.release();
-        queue.release(); error.release(); exact_ws.release();
+        queue.release(); error.release(); exact_ws.release(); deadline.release();
         band_pairs.release(); band_strips.release(); band_units.release(); band_res.release();
         band_progress.release(); band_bnd.release(); band_queue.release(); band_walk.release(); h_band.release();
         h_codes.release(); h_pairs.release(); h_order.release(); h_out.release();
@@ -526,6 +534,17 @@ static int plan_launch(aw_ksw_plan_t *pl) {
     AW_CUDA(cudaMemsetAsync(B->error.p, 0, sizeof(int32_t) * 4, B->st));
     AW_CUDA(cudaMemsetAsync(B->out.p, 0, sizeof(KswOut) * (size_t)std::max(pl->n, 1), B->st));
     AW_CUDA(cudaEventRecord(B->ev_t0, B->st));
+    // the deadline word: globaltimer at the start of this work + the time left
+    const unsigned long long *deadline = nullptr;
+    if (tls_has_deadline) {
+        const long long left = std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                   tls_deadline - std::chrono::steady_clock::now()).count();
+        AW_CUDA(B->deadline.ensure(sizeof(unsigned long long)));
+        AW_CUDA(launch_set_deadline(B->deadline.as<unsigned long long>(),
+                                    (unsigned long long)std::max(left, 0LL), B->st));
+        deadline = B->deadline.as<unsigned long long>();
+        ++launches;
+    }
     int large_warps;
     {
         std::lock_guard<std::mutex> lk(g_cfg_mu);
@@ -547,6 +566,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         a.tb = B->tb.as<uint8_t>(), a.bnd = B->bnd.as<uint32_t>();
         a.error = B->error.as<int32_t>();
         a.sc = pl->S;
+        a.deadline = deadline;
         AW_CUDA(cudaEventRecord(B->ev_k[3 * k], B->st));
         // fork: large pairs on st2 (groups of large_warps warps), small on st (single warps)
         AW_CUDA(cudaEventRecord(B->ev_a, B->st));
@@ -589,6 +609,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         D.walk = B->band_walk.as<BandWalkState>();
         D.progress = B->band_progress.as<int32_t>(), D.queue = B->band_queue.as<int32_t>();
         D.bnd = B->band_bnd.as<uint2>(), D.tb = B->tb.as<uint8_t>(), D.error = B->error.as<int32_t>();
+        D.deadline = deadline;
         const int ctas = band_occupancy(P.flag) * B->sms;
         for (int k = 0; k < nbw; ++k) {
             cudaEvent_t *ev = &B->ev_k[3 * (nw + k)];
@@ -616,7 +637,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
                                B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), B->pairs.as<KswPair>(),
                                pl->pairs, pl->exact_ids, pl->w, P.m, P.mat, pl->S, P.zdrop, P.end_bonus,
                                P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), B->exact_ws,
-                               B->st, &launches);
+                               B->st, &launches, deadline);
         if (rc) return rc;
     }
     AW_CUDA(cudaEventRecord(B->ev_t1, B->st));
@@ -714,6 +735,19 @@ void aw_release_thread_buffers(void) {
         tls_buf = nullptr;
     }
 }
+
+void aw_ksw_set_deadline(double seconds) {
+    if (seconds > 0.0 && seconds < 1e9) {
+        tls_has_deadline = true;
+        tls_deadline = std::chrono::steady_clock::now() +
+                       std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                           std::chrono::duration<double>(seconds));
+    } else {
+        tls_has_deadline = false;
+    }
+}
+
+void aw_ksw_set_stop_antidiagonal(int interval, int antidiagonal) { set_exact_stop(interval, antidiagonal); }
 
 void aw_set_band_columns(int columns) {
     std::lock_guard<std::mutex> lk(g_cfg_mu);

@@ -151,6 +151,7 @@ struct BandArgs {
     KswScore sc;
     int block, generic;
     int store_ckpt;  // 1: store the traceback of recomputed pairs too (their group passes)
+    const unsigned long long *deadline;  // null: no deadline
 };
 
 constexpr uint64_t WAIT_NS = 20ull * 1000 * 1000 * 1000;  // bounded wait on the left strip
@@ -182,6 +183,8 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         const BandStripDev St = A.strips[P.strip0 + s];
         const int jstart = St.jstart, jlo = St.jlo, jend = St.jend;
         if (jend < jlo) continue;  // nothing of this strip is computed
+        volatile int32_t *stop_word = &A.res[un.x].stopped;
+        if (A.deadline && *stop_word) continue;  // the pair stopped at the deadline
         const Geom g{P.qlen, P.tlen, P.w, P.qlen + P.tlen - 1, P.rb, ~(B - 1)};
         const int qlen = P.qlen, tlen = P.tlen, qm1 = qlen - 1, tm1 = tlen - 1;
         const int rlim = min(g.nd, g.rb);
@@ -228,6 +231,16 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         bool failed = false;
         const int nsteps = jend - jstart + 32;
         for (int k = 0; k < nsteps; ++k) {
+            if ((k & 31) == 0 && A.deadline) {
+                // cooperative stop, polled every 32 rows (ksw2_progress.c:30-38 polls every
+                // 256 anti-diagonals); the pair's other strips see the flag and stop too
+                int st = 0;
+                if (lane == 0) {
+                    st = *stop_word;
+                    if (!st && aw_deadline_passed(A.deadline)) st = 1, atomicExch((int32_t *)stop_word, 1);
+                }
+                if (__shfl_sync(FULL, st, 0)) break;
+            }
             if ((k & 31) == 0) {
                 const int J = jstart + k, jr = J + lane;
                 qchunk = (jr >= 0 && jr < qlen) ? qs[jr] : 0u;
@@ -245,6 +258,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                             while (pr.load(cuda::memory_order_acquire) < need) {
                                 __nanosleep(ns);
                                 ns = ns < 1024 ? ns * 2 : ns;
+                                if (A.deadline && *stop_word) break;  // the left strip stopped
                                 if ((++polls & 31) == 0 &&
                                     (globaltimer() - t0 > WAIT_NS || *(volatile int32_t *)A.error)) {
                                     failed = true;
@@ -258,6 +272,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                         if (lane == 0) atomicExch(A.error, 1);
                         break;
                     }
+                    if (A.deadline && __shfl_sync(FULL, lane == 0 ? *stop_word : 0, 0)) break;
                     if (jr >= prod_lo && jr <= prod_hi) bchunk = __ldcg(bnd_prod + (jr - prod_lo));
                     else if (jr > prod_hi) bchunk = make_uint2(init_pack, __ldcg(bnd_prod + (prod_hi - prod_lo + 1)).y);
                     else bchunk = make_uint2(init_pack, (uint32_t)AW_NEG_INF);
@@ -552,6 +567,15 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
     o.mte = R.mte_key ? (int)((uint32_t)(R.mte_key >> 32) ^ 0x80000000u) : AW_NEG_INF;
     o.mte_q = R.mte_key ? (int)(uint32_t)R.mte_key : -1;
     o.zdropped = P.rb < g.nd ? 1 : 0;
+    if (R.stopped) {
+        // stopped at the deadline: no score and no traceback (ksw2_extd2_sse.c:136-139, :400-409)
+        o.stopped = 1, o.score = AW_NEG_INF;
+        if (lane == 0) {
+            if (P.ckpt) A.walk[pi].done = 1;
+            A.out[P.idx] = o;
+        }
+        return;
+    }
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY);
     const BandStripDev *strips = A.strips + P.strip0;
     const uint8_t *tb = A.tb;
@@ -671,6 +695,14 @@ __global__ void __launch_bounds__(32) ksw_band_walk_kernel(BtArgs A, int slot, i
     BandWalkState w = A.walk[slot];
     if (w.done) return;
     const BandPairDev P = A.pairs[slot];
+    if (A.res[slot].stopped) {
+        // the group's recomputation stopped at the deadline: its traceback is incomplete
+        if ((threadIdx.x & 31) == 0) {
+            A.walk[slot].done = 1;
+            A.out[P.idx].stopped = 1, A.out[P.idx].score = AW_NEG_INF, A.out[P.idx].n_cigar = 0;
+        }
+        return;
+    }
     const Geom g{P.qlen, P.tlen, P.w, P.qlen + P.tlen - 1, P.rb, ~(A.block - 1)};
     const int tlen = P.tlen;
     const BandStripDev *strips = A.strips + P.strip0;
@@ -973,6 +1005,7 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
     a.block = bp.block;
     a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
     a.store_ckpt = 0;
+    a.deadline = D.deadline;
     return band_launch_units(bp, a, flag, ctas, st);
 }
 
@@ -1048,6 +1081,7 @@ cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, cons
         a.block = bp.block;
         a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
         a.store_ckpt = 1;
+        a.deadline = D.deadline;
         if ((e = band_launch_units(bp, a, flag, ctas, st)) != cudaSuccess) return e;
         if (bp.nc == 4) ksw_band_walk_kernel<4><<<1, 32, 0, st>>>(b, G.slot, G.col_lo);
         else ksw_band_walk_kernel<8><<<1, 32, 0, st>>>(b, G.slot, G.col_lo);

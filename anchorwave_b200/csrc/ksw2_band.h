@@ -34,7 +34,8 @@ struct BandStripDev {
 struct BandRes {
     unsigned long long mqe_key, mte_key;
     int32_t score, has_score;
-    int32_t pad[2];
+    int32_t stopped;  // a strip of the pair saw the calling thread's deadline pass
+    int32_t pad;
 };
 
 struct BandWave {
@@ -102,6 +103,7 @@ struct BandDev {
     uint2 *bnd;
     uint8_t *tb;
     int32_t *error;
+    const unsigned long long *deadline = nullptr;  // the calling thread's deadline word, or null
 };
 
 int band_occupancy(int flag);

@@ -47,6 +47,7 @@ struct ExactArgs {
     int8_t mat[64];
     int m, zdrop, end_bonus, flag, B;
     int stop_interval, stop_at;
+    const unsigned long long *deadline;  // the calling thread's deadline word, or null
 };
 
 __device__ __forceinline__ int8_t w8(int v) { return (int8_t)(uint8_t)(v & 0xff); }
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
 
     __shared__ int8_t s_carry[2][3];
     __shared__ int s_red_v[NT / 32][4], s_red_p[NT / 32][4];
-    __shared__ int s_brk;
+    __shared__ int s_brk, s_stop;
     __shared__ Ez s_ez;
     __shared__ int s_H0, s_H0t;
 
@@ -277,10 +278,19 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
 
     int last_st = -1, last_en = -1;
     const int nd = qlen + tlen - 1;
+    const bool polled = A.stop_at >= 0 || A.deadline;
+    const int interval = A.stop_interval > 0 ? A.stop_interval : 256;
     for (int r = 0; r < nd; ++r) {
-        if (A.stop_at >= 0 && A.stop_interval > 0 && r % A.stop_interval == 0 && r >= A.stop_at) {
-            if (tid == 0) s_ez.stopped = 1;
-            break;
+        // ksw_progress_continue (minimap2/ksw2_progress.c:30-38) before anti-diagonal r:
+        // a scheduled stop, or the calling thread's deadline, sets ez->stopped
+        if (polled && r % interval == 0) {
+            if (tid == 0)
+                s_stop = (A.stop_at >= 0 && r >= A.stop_at) || aw_deadline_passed(A.deadline);
+            __syncthreads();
+            if (s_stop) {
+                if (tid == 0) s_ez.stopped = 1;
+                break;
+            }
         }
         int st = 0, en = tlen - 1;
         if (st < r - qlen + 1) st = r - qlen + 1;
@@ -515,7 +525,8 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
 
 std::mutex g_mu;
 int g_block = 64;
-int g_stop_interval = 0, g_stop_at = -1;
+// thread-local like the reference's callback state (ksw2_progress.c:11-13)
+thread_local int t_stop_interval = 0, t_stop_at = -1;
 
 int64_t host_al256(int64_t v) { return (v + 255) & ~(int64_t)255; }
 
@@ -530,26 +541,24 @@ void set_exact_block(int b) {
     if (b == 16 || b == 32 || b == 64) g_block = b;
 }
 void set_exact_stop(int interval, int stop_at) {
-    std::lock_guard<std::mutex> lk(g_mu);
-    g_stop_interval = interval > 0 ? interval : 1;
-    g_stop_at = stop_at;
+    t_stop_interval = interval > 0 ? interval : 1;
+    t_stop_at = stop_at < 0 ? -1 : stop_at;
 }
-bool exact_stop_enabled() {
-    std::lock_guard<std::mutex> lk(g_mu);
-    return g_stop_at >= 0;
-}
+bool exact_stop_enabled() { return t_stop_at >= 0; }
 
 int run_exact_ksw(size_t n_exact, const int32_t *d_ids, const uint8_t *d_q, const uint8_t *d_t,
                   const KswPair *d_pairs, const std::vector<KswPair> &h_pairs, const std::vector<int32_t> &ids,
                   const std::vector<int> &w, int m, const int8_t *mat, const KswScore &S, int zdrop, int end_bonus,
-                  int flag, KswOut *d_out, uint32_t *d_cig, DevBuf &ws, cudaStream_t st, int *launches) {
+                  int flag, KswOut *d_out, uint32_t *d_cig, DevBuf &ws, cudaStream_t st, int *launches,
+                  const unsigned long long *deadline) {
     (void)d_ids;
     if (n_exact == 0) return 0;
-    int B, stop_interval, stop_at;
+    int B;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        B = g_block, stop_interval = g_stop_interval, stop_at = g_stop_at;
+        B = g_block;
     }
+    const int stop_interval = t_stop_interval, stop_at = t_stop_at;
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY);
     const bool stk = B > 16 && (flag & AW_EZ_SINGLETRACK);
     // per-pair workspace sizes
@@ -612,7 +621,7 @@ int run_exact_ksw(size_t n_exact, const int32_t *d_ids, const uint8_t *d_q, cons
         memset(A.mat, 0, sizeof(A.mat));
         memcpy(A.mat, mat, (size_t)m * m);
         A.m = m, A.zdrop = zdrop, A.end_bonus = end_bonus, A.flag = flag, A.B = B;
-        A.stop_interval = stop_interval, A.stop_at = stop_at;
+        A.stop_interval = stop_interval, A.stop_at = stop_at, A.deadline = deadline;
         ksw_exact_kernel<<<(unsigned)(b - a), NT, 0, st>>>(A);
         if (cudaGetLastError() != cudaSuccess) {
             set_error("exact KSW2 kernel launch failed");

@@ -186,13 +186,16 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
     __shared__ int s_pair[MAX_GROUP_WARPS];
     __shared__ int s_prog[MAX_GROUP_WARPS];           // rows published, per warp (monotone per pair)
     __shared__ int s_red[MAX_GROUP_WARPS][5];
+    __shared__ int s_stop[MAX_GROUP_WARPS];           // the group's pair passed the deadline
     int *prog = s_prog + g * W;
+    volatile int *stop_flag = s_stop + g;
 
     for (;;) {
         group_sync(g, W * 32);
         if (wg == 0 && lane == 0) {
             s_pair[g] = atomicAdd(A.queue, 1);
             for (int i = 0; i < W; ++i) prog[i] = -1;
+            *stop_flag = 0;
         }
         group_sync(g, W * 32);
         const int pi = s_pair[g];
@@ -207,8 +210,9 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
         const int nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
         const int stride_k = qlen + 31;
         int mqe = AW_NEG_INF, mqe_t = -1, mte = AW_NEG_INF, mte_q = -1, score = AW_NEG_INF;
+        bool stopped = false;
 
-        for (int s = wg; s < nstrip; s += W) {
+        for (int s = wg; s < nstrip && !stopped; s += W) {
             const int col0 = s * KSW_STRIP + lane * C;
             int ut[C], yt[C], y2t[C], H[C];
             uint32_t rlo[C], rhi[C];
@@ -228,6 +232,18 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
             uint32_t carry = 0, qchunk = 0, bchunk = 0;
             const int last_k = qlen + 31;
             for (int k = 0; k < last_k; ++k) {
+                if ((k & 31) == 0 && A.deadline) {
+                    // cooperative stop, polled every 32 rows (ksw2_progress.c:30-38 polls
+                    // every 256 anti-diagonals); any warp of the group stops the pair
+                    int st = 0;
+                    if (lane == 0) st = (*stop_flag || aw_deadline_passed(A.deadline)) ? 1 : 0;
+                    st = __shfl_sync(0xffffffffu, st, 0);
+                    if (st) {
+                        if (lane == 0) *stop_flag = 1;
+                        stopped = true;
+                        break;
+                    }
+                }
                 if ((k & 31) == 0 && k < qlen) {
                     const int J = k;
                     qchunk = (J + lane < qlen) ? qs[J + lane] : 0u;
@@ -238,11 +254,20 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
                         // the producer publishes (strip, rows) as strip*(qlen+1)+rows
                         const int target = (s - 1) * (qlen + 1) + need;
                         while (pr.load(cuda::memory_order_acquire) < target) {
+                            if (*stop_flag) break;  // the producer stopped at the deadline
                             if (++spins > (1 << 26)) {
                                 atomicExch(A.error, 1);
                                 break;
                             }
                             __nanosleep(32);
+                        }
+                        if (A.deadline) {
+                            int st = lane == 0 ? *stop_flag : 0;
+                            st = __shfl_sync(0xffffffffu, st, 0);
+                            if (st) {
+                                stopped = true;
+                                break;
+                            }
                         }
                         bchunk = (J + lane < qlen) ? __ldcg(bnd + (int64_t)(s - 1) * qlen + J + lane) : 0u;
                     }
@@ -336,9 +361,10 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
                 score = max(score, rr[4]);
             }
             KswOut o;
-            o.score = score, o.max = 0, o.max_q = -1, o.max_t = -1;
+            const int stop = *stop_flag;
+            o.score = stop ? AW_NEG_INF : score, o.max = 0, o.max_q = -1, o.max_t = -1;
             o.mqe = mqe, o.mqe_t = mqe_t, o.mte = mte, o.mte_q = mte_q;
-            o.n_cigar = 0, o.zdropped = 0, o.reach_end = 0, o.stopped = 0;
+            o.n_cigar = 0, o.zdropped = 0, o.reach_end = 0, o.stopped = stop;
             A.out[idx] = o;
         }
     }
@@ -499,6 +525,17 @@ cudaError_t launch_ksw_backtrack_full(const KswPair *pairs, const int32_t *order
     if (n <= 0) return cudaSuccess;
     ksw_backtrack_full_kernel<<<(n + BT_WARPS - 1) / BT_WARPS, 32 * BT_WARPS, 0, st>>>(pairs, order, n, tb, out,
                                                                                        cig, flag);
+    return cudaGetLastError();
+}
+
+__global__ void set_deadline_kernel(unsigned long long *d, unsigned long long remaining_ns) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *d = remaining_ns == ~0ull ? ~0ull : t + remaining_ns;
+}
+
+cudaError_t launch_set_deadline(unsigned long long *deadline, unsigned long long remaining_ns, cudaStream_t st) {
+    set_deadline_kernel<<<1, 1, 0, st>>>(deadline, remaining_ns);
     return cudaGetLastError();
 }
 

@@ -234,6 +234,33 @@ def release_thread_buffers():
     lib.aw_release_thread_buffers()
 
 
+def set_deadline(seconds: float = 0.0):
+    """Cooperative stop for this thread's KSW2 calls: pairs still running `seconds` from
+    now come back with stopped=1 (AnchorWave's ScopedKswDeadline); <= 0 clears it."""
+    lib.aw_ksw_set_deadline(float(seconds))
+
+
+def set_stop_antidiagonal(interval: int = 256, antidiagonal: int = -1):
+    """Deterministic stop for this thread: as a ksw2 progress callback that returns 0 at
+    the first probed anti-diagonal >= antidiagonal; < 0 clears it."""
+    lib.aw_ksw_set_stop_antidiagonal(int(interval), int(antidiagonal))
+
+
+class deadline:
+    """Context manager mirroring ScopedKswDeadline (alignSlidingWindow.cpp:612-638)."""
+
+    def __init__(self, seconds: float):
+        self.seconds = seconds
+
+    def __enter__(self):
+        set_deadline(self.seconds)
+        return self
+
+    def __exit__(self, *exc):
+        set_deadline(0.0)
+        return False
+
+
 def set_band_columns(columns: int = 0):
     """Target columns per lane of the banded kernel: 4, 8, or 0 to choose per batch."""
     lib.aw_set_band_columns(int(columns))

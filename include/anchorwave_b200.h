@@ -228,6 +228,21 @@ void aw_set_band_columns(int columns);
  * between calls (they grow to the largest batch seen; the next call re-creates them).
  * No counterpart in the reference (its work arrays are per call). */
 void aw_release_thread_buffers(void);
+/* Cooperative stop for the calling thread's KSW2 calls (single, batched, plan
+ * executions): pairs still being aligned `seconds` from now stop with ez->stopped = 1,
+ * score KSW_NEG_INF and no CIGAR; seconds <= 0 clears it.  Replaces the deadline probe
+ * that AnchorWave installs with ksw_set_progress_callback (ScopedKswDeadline,
+ * src/myImportandFunction/alignSlidingWindow.cpp:593-640; minimap2/ksw2_progress.c:15-38),
+ * which the device cannot call back into: the kernels poll a device copy of the deadline
+ * every 32 rows (strip kernels) or 256 anti-diagonals (exact kernel).  The deadline
+ * counts from the call; the device copy is armed when the stream reaches the work. */
+void aw_ksw_set_deadline(double seconds);
+/* Deterministic form of the same stop for the calling thread: as a progress callback
+ * (interval `interval`) that returns 0 at the first probed anti-diagonal >= antidiagonal;
+ * antidiagonal < 0 clears it.  While set, every pair runs on the anti-diagonal kernel, so
+ * a stopped pair's fields and partial traceback are those of ksw_extd2 with that callback
+ * (minimap2/ksw2_extd2_sse.c:136-139, :400-414). */
+void aw_ksw_set_stop_antidiagonal(int interval, int antidiagonal);
 const char *aw_last_error(void);
 int aw_device_count(void);
 /* Integer-ALU peak probe: IADD3/IMNMX-class 32-bit ops per second measured on
