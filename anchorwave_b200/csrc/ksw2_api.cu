@@ -389,6 +389,10 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
     if (budget <= 0) {
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = (size_t)16 << 30;
+        // the traceback arena this thread already holds is reused (or freed) by this
+        // batch, so it counts as available: otherwise every call after the first would
+        // see the pooled arena as used memory and split the batch into more waves
+        if (pl->B) fr += pl->B->tb.cap;
         budget = (int64_t)(fr * 0.6);
     }
     // LPT multiway partition of traceback bytes into the fewest waves that fit
