@@ -28,7 +28,7 @@ EXPORTS = [
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_release_thread_buffers",
     "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
-    "aw_int32_peak_ops", "aw_ksw_extd2_device_noalloc",
+    "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
     "wavefront_align_batch_gpu", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
     "aw_serve_result_free", "aw_serve_close",
@@ -107,6 +107,8 @@ def _load(path: str = LIB_PATH):
     lib.aw_device_count.restype = i32
     lib.aw_int32_peak_ops.argtypes = []
     lib.aw_int32_peak_ops.restype = C.c_double
+    lib.aw_int16x2_peak_ops.argtypes = []
+    lib.aw_int16x2_peak_ops.restype = C.c_double
     lib.aw_ksw_extd2_device_noalloc.argtypes = [i32, vp, i32, vp, i8, vp, i8, i8, i8, i8, i32, vp, vp, i32, vp]
     lib.aw_ksw_extd2_device_noalloc.restype = i32
     lib.wavefront_aligner_new_gpu.argtypes = [C.POINTER(WfaAttr)]

@@ -73,19 +73,23 @@ __device__ __forceinline__ bool aw_deadline_passed(const unsigned long long *d) 
 }
 #endif
 
-// Traceback geometry of the strip kernel: 32 lanes x KSW_COLS target columns per
-// strip; one byte per cell at  ((strip * (qlen + 31) + step) * 32 + lane) * KSW_COLS + col
-// where step = row + lane (the lane skew).
+// Traceback geometry of the full-matrix strip kernel: strips of KSW_STRIP = 512 target
+// columns in KSW_GROUPS = 64 groups of KSW_COLS = 8; a step of a strip stores one
+// KSW_COLS-byte word per group, the word of group g at row r being stored at step r + g:
+// byte ((strip * (qlen + KSW_LAG) + r + g) * KSW_GROUPS + g) * KSW_COLS + (col & 7).
 constexpr int KSW_COLS = 8;
-constexpr int KSW_STRIP = 32 * KSW_COLS;
+constexpr int KSW_GROUPS = 64;
+constexpr int KSW_STRIP = KSW_GROUPS * KSW_COLS;
+constexpr int KSW_LAG = KSW_GROUPS - 1;
 
 inline int64_t ksw_full_tb_bytes(int qlen, int tlen) {
     const int64_t nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
-    return nstrip * (int64_t)(qlen + 31) * KSW_STRIP;
+    return nstrip * (int64_t)(qlen + KSW_LAG) * KSW_STRIP;
 }
+// boundary column of a strip: one 8-byte entry per row and one for the strip's last-row H
 inline int64_t ksw_full_bnd_words(int qlen, int tlen) {
     const int64_t nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
-    return nstrip * (int64_t)qlen;
+    return nstrip * ((int64_t)qlen + 1) * 2;
 }
 
 // Grow-only device allocation (pooled per host thread or per plan).

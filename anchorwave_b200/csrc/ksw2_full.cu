@@ -2,27 +2,42 @@
 //
 // Same recurrence as minimap2/ksw2_extd2_sse.c:43-71 + :237-330 (difference-
 // encoded u, v, x, y, x2, y2 cells; state byte d with the 3-bit argmax and the
-// four continuation bits), computed cell by cell in 32-bit registers.  In full
-// mode every cell the recurrence reads is a real matrix cell or a matrix edge,
-// so the SIMD padding lanes of the reference never influence the result and
-// are not computed here.  The host only routes parameter sets to this kernel
-// whose int8 intermediates provably cannot wrap (ksw2_api.cu: full_path_ok).
+// four continuation bits).  In full mode every cell the recurrence reads is a real
+// matrix cell or a matrix edge, so the SIMD padding lanes of the reference never
+// influence the result and are not computed here.  The host only routes parameter
+// sets to this kernel whose int8 intermediates provably cannot wrap
+// (ksw2_api.cu: full_path_ok).
+//
+// Two cells per instruction.  Every register holds two 16-bit fields, each a cell
+// value stored as 16*value + bias; the two fields are cells of two different rows
+// (below), so a cell is DPX SIMD (vimax3 / viaddmin .s16x2, vmax / vmin .s16x2) plus
+// 32-bit adds whose per-field results stay inside [0, 65536), which the biases
+// guarantee, so no carry crosses from one field into the other.  The low 4 bits of a
+// field are free: the five candidates of the max carry a priority tag there, so one
+// max yields both z and the arg-max under the reference's tie rule (left-aligned: the
+// first candidate wins a tie, ksw2_extd2_sse.c:244-251; right-aligned: the last,
+// :291-298).
 //
 // Work decomposition (one pair per group of W warps):
-//   * target columns are cut into strips of 256 (32 lanes x 8 columns);
-//   * a warp sweeps the query rows of its strip with a one-row skew per lane:
-//     at step k lane L owns row j = k - L, so the (x, v, x2) values of a lane's
-//     last column reach the next lane by one __shfl_up per step, together with
-//     the query code of that row;
-//   * strip s+1 takes its left edge (column 256(s+1)-1 of strip s) from a
-//     global boundary buffer that strip s fills row by row; with W > 1 the W
-//     warps of a group run consecutive strips concurrently, the consumer warp
-//     polling the producer's published row count in shared memory (bounded);
-//   * traceback bytes go to HBM as one coalesced 256-byte store per warp-step,
-//     with evict-first policy (they are read back only along one path).
-// Pairs are pulled from a device work queue (atomicAdd on a head counter) in
-// the host-provided order (largest first), so one persistent launch serves a
-// whole batch of uneven pairs.
+//   * target columns are cut into strips of 512 (32 lanes x 16 columns); lane L owns
+//     columns 16L..16L+7 in its low fields and 16L+8..16L+15 in its high fields;
+//   * a warp sweeps the query rows of its strip with a skew of two steps per lane and
+//     one step between the halves: at step k lane L computes row k-2L in its low fields
+//     and row k-2L-1 in its high fields, so the (x, v, x2) of its low column 7 feed its
+//     high column 8 at the next step, and its high column 15 reaches lane L+1 by one
+//     __shfl_up per step, together with the query code of that row;
+//   * strip s+1 takes its left edge (column 512(s+1)-1 of strip s) from a global
+//     boundary buffer that strip s fills row by row; with W > 1 the W warps of a group
+//     run consecutive strips concurrently, the consumer warp polling the producer's
+//     published row count in shared memory (bounded);
+//   * the traceback bytes of a step go to HBM as one coalesced 512-byte store per warp
+//     (16 bytes per lane), with evict-first policy (they are read back along one path);
+//   * H is not carried per cell: the last row's H (mqe, the score) is a prefix sum of
+//     the last row's u along the strip after the sweep, and the last column's H (mte)
+//     is accumulated by the lane that owns that column.
+// Pairs are pulled from a device work queue (atomicAdd on a head counter) in the
+// host-provided order (largest first), so one persistent launch serves a whole batch
+// of uneven pairs.
 #include "aw_internal.h"
 #include "tb_walk.cuh"
 #include <cuda/atomic>
@@ -32,18 +47,12 @@ namespace aw {
 namespace {
 
 constexpr int MAX_GROUP_WARPS = 32;
+constexpr unsigned FULLMASK = 0xffffffffu;
 
-__device__ __forceinline__ int prmt_sx(uint32_t lo, uint32_t hi, uint32_t sel) {
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     uint32_t r;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(lo), "r"(hi), "r"(sel));
-    return (int)r;
-}
-
-__device__ __forceinline__ int sx8(uint32_t w) { return (int)(int8_t)(uint8_t)w; }
-
-__device__ __forceinline__ uint32_t pack3(int a, int b, int c, uint32_t top) {
-    return (uint32_t)(a & 0xff) | ((uint32_t)(b & 0xff) << 8) | ((uint32_t)(c & 0xff) << 16) |
-           (top << 24);
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
 }
 
 // Difference along a matrix edge for edge cell index r (ksw2_extd2_sse.c:167,171).
@@ -51,8 +60,8 @@ __device__ __forceinline__ int edge_diff(int r, const KswScore &S) {
     return r == 0 ? -S.qe : r < S.long_thres ? -S.e : r == S.long_thres ? S.long_diff : -S.e2;
 }
 
-// H(t, -1): sum of edge_diff(0..t), the score of a leading gap of length t+1,
-// offset as the reference's H[0] = v[0] - qe with qe taken before the swap.
+// H(t, -1) (= H(-1, t)): sum of edge_diff(0..t), the score of a leading gap of length
+// t+1, offset as the reference's H[0] = v[0] - qe with qe taken before the swap.
 __device__ __forceinline__ int htop(int t, const KswScore &S) {
     const int L = S.long_thres;
     int A = min(t, L - 1);
@@ -67,107 +76,86 @@ __device__ __forceinline__ void group_sync(int g, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(nthreads) : "memory");
 }
 
-#ifndef AW_CELL_DPX
-#define AW_CELL_DPX 2
-#endif
-#ifndef AW_ARGMAX_DPX
-#define AW_ARGMAX_DPX 1
-#endif
+// ---- packed cell fields ------------------------------------------------------------
+// Field biases.  With the magnitude bound of full_path_ok (every |u|, |v|, |x|, ... <= 300
+// even for the bounded excursions of masked-off fields) every 32-bit add below keeps each
+// field inside [0, 65536) and every value a DPX op compares inside [0, 32768).
+constexpr int FB = 8192;    // u, v, z, the score and the max candidates
+constexpr int FBX = 16384;  // x, y, x2, y2
+// A constant in both fields: for 32-bit adds (c * 65537, so that a negative c borrows
+// exactly what the field sum carries back) and for SIMD operands (each field = c).
+__host__ __device__ constexpr uint32_t add2(int c) { return (uint32_t)c * 0x10001u; }
+__host__ __device__ constexpr uint32_t rep2(int c) { return ((uint32_t)c & 0xffffu) * 0x10001u; }
+
+// Priority tags of the candidates s, a, b, a2, b2 (the larger tag wins a tie of values),
+// and the XOR that turns the winning tag into the reference's state code d (0 = s, 1 = a,
+// 2 = b, 3 = a2, 4 = b2).  Score-only sweeps need no arg-max: no tags.
+template <bool CIGAR, bool RIGHT>
+struct Tags {
+    static constexpr int s = !CIGAR ? 0 : RIGHT ? 0 : 7;
+    static constexpr int a = !CIGAR ? 0 : RIGHT ? 1 : 6;
+    static constexpr int b = !CIGAR ? 0 : RIGHT ? 2 : 5;
+    static constexpr int a2 = !CIGAR ? 0 : RIGHT ? 3 : 4;
+    static constexpr int b2 = !CIGAR ? 0 : RIGHT ? 4 : 3;
+    static constexpr uint32_t dx = (CIGAR && !RIGHT) ? 0x00070007u : 0u;
+};
+
+// Per-launch packed constants of the cell.
+struct CellK {
+    uint32_t cA, cB, cA2, cB2;      // candidate = left/up values + c (rebias + tag)
+    uint32_t cS;                    // score field = 16 * (s + 128) + cS
+    uint32_t nzA, nzB, nzA2, nzB2;  // W = candidate + nz - Z = 16 (cand - z - e) + FBX
+    uint32_t kqe, kqe2;             // x' = max(W, kqe)                       (SIMD)
+    uint32_t cq, cq2;               // continuation bit = relu(min(W + cq, 1)) (SIMD)
+    uint32_t mch;                   // z = min(z, mch)                        (SIMD)
+};
 
 template <bool CIGAR, bool RIGHT>
-__device__ __forceinline__ void cell(int s, int &xs, int &vs, int &x2s, int &ut, int &yt, int &y2t,
-                                     int &d, const KswScore &S) {
-    int a = xs + vs, b = yt + ut, a2 = x2s + vs, b2 = y2t + ut;
-    int z = s;
-#if AW_CELL_DPX && AW_ARGMAX_DPX
-    // Arg-max chain with the reference's tie rules, one DPX max+predicate per step:
-    // left-aligned takes a candidate only if strictly greater (ksw2_extd2_sse.c:244-251),
-    // right-aligned also on equality (:291-298).
-    bool p;
-    if (!CIGAR) {
-        z = __vimax3_s32(z, a, b);
-        z = __vimax3_s32(z, a2, b2);
-    } else if (!RIGHT) {
-        z = __vibmax_s32(z, a, &p);  // p = z >= a
-        d = p ? 0 : 1;
-        z = __vibmax_s32(z, b, &p);
-        d = p ? d : 2;
-        z = __vibmax_s32(z, a2, &p);
-        d = p ? d : 3;
-        z = __vibmax_s32(z, b2, &p);
-        d = p ? d : 4;
-    } else {
-        z = __vibmax_s32(a, z, &p);  // p = a >= z
-        d = p ? 1 : 0;
-        z = __vibmax_s32(b, z, &p);
-        d = p ? 2 : d;
-        z = __vibmax_s32(a2, z, &p);
-        d = p ? 3 : d;
-        z = __vibmax_s32(b2, z, &p);
-        d = p ? 4 : d;
-    }
-#else
-    if (!CIGAR) {
-        z = max(max(max(z, a), max(b, a2)), b2);
-    } else if (!RIGHT) {
-        d = a > z ? 1 : 0;
-        z = max(z, a);
-        d = b > z ? 2 : d;
-        z = max(z, b);
-        d = a2 > z ? 3 : d;
-        z = max(z, a2);
-        d = b2 > z ? 4 : d;
-        z = max(z, b2);
-    } else {
-        d = z > a ? 0 : 1;
-        z = max(z, a);
-        d = z > b ? d : 2;
-        z = max(z, b);
-        d = z > a2 ? d : 3;
-        z = max(z, a2);
-        d = z > b2 ? d : 4;
-        z = max(z, b2);
-    }
-#endif
-    z = min(z, S.mch);
-    const int un = z - vs, vn = z - ut;
-#if AW_CELL_DPX >= 2
-    if (!(CIGAR && RIGHT)) {
-        // x' = max(a - z + q, 0) - (q + e) = max(a + (-e - z), -(q + e)): one add+max each
-        const int nez = -S.e - z, nez2 = -S.e2 - z;
-        xs = __viaddmax_s32(a, nez, -S.qe);
-        yt = __viaddmax_s32(b, nez, -S.qe);
-        x2s = __viaddmax_s32(a2, nez2, -S.qe2);
-        y2t = __viaddmax_s32(b2, nez2, -S.qe2);
-        if (CIGAR) {
-            // continuation bit (a - z + q > 0) == (x' + q + e > 0) == min(x' + q + e, 1)
-            d += 0x08 * __viaddmin_s32(xs, S.qe, 1);
-            d += 0x10 * __viaddmin_s32(yt, S.qe, 1);
-            d += 0x20 * __viaddmin_s32(x2s, S.qe2, 1);
-            d += 0x40 * __viaddmin_s32(y2t, S.qe2, 1);
-        }
-        ut = un;
-        vs = vn;
-        return;
-    }
-#endif
-    a = a - z + S.q;
-    b = b - z + S.q;
-    a2 = a2 - z + S.q2;
-    b2 = b2 - z + S.q2;
-    xs = max(a, 0) - S.qe;
-    yt = max(b, 0) - S.qe;
-    x2s = max(a2, 0) - S.qe2;
-    y2t = max(b2, 0) - S.qe2;
-    if (CIGAR) {
-        if (!RIGHT)
-            d |= (a > 0 ? 0x08 : 0) | (b > 0 ? 0x10 : 0) | (a2 > 0 ? 0x20 : 0) | (b2 > 0 ? 0x40 : 0);
-        else
-            d |= (a >= 0 ? 0x08 : 0) | (b >= 0 ? 0x10 : 0) | (a2 >= 0 ? 0x20 : 0) | (b2 >= 0 ? 0x40 : 0);
-    }
-    ut = un;
-    vs = vn;
+__device__ __forceinline__ CellK make_cellk(const KswScore &S) {
+    using T = Tags<CIGAR, RIGHT>;
+    CellK K;
+    K.cA = add2(T::a - FBX), K.cB = add2(T::b - FBX), K.cA2 = add2(T::a2 - FBX), K.cB2 = add2(T::b2 - FBX);
+    K.cS = add2(T::s + FB - 16 * 128);
+    K.nzA = add2(FBX - 16 * S.e - T::a), K.nzB = add2(FBX - 16 * S.e - T::b);
+    K.nzA2 = add2(FBX - 16 * S.e2 - T::a2), K.nzB2 = add2(FBX - 16 * S.e2 - T::b2);
+    K.kqe = rep2(FBX - 16 * S.qe), K.kqe2 = rep2(FBX - 16 * S.qe2);
+    // left-aligned: a - z + q > 0 (ksw2_extd2_sse.c:268-271); right-aligned: >= 0 (:315-318)
+    K.cq = rep2(16 * S.qe - FBX + (RIGHT ? 1 : 0)), K.cq2 = rep2(16 * S.qe2 - FBX + (RIGHT ? 1 : 0));
+    K.mch = rep2(16 * S.mch + FB);
+    return K;
 }
+
+// Two cells, one per field.  In: sc (tagged score), X/V/X2 from the left column, U/Y/Y2
+// the column state from the row above.  Out: X/V/X2 for the next column, U/Y/Y2 for
+// the next row, D the two state bytes (one per field).
+template <bool CIGAR, bool RIGHT>
+__device__ __forceinline__ void cell2(uint32_t sc, uint32_t &X, uint32_t &V, uint32_t &X2, uint32_t &U,
+                                      uint32_t &Y, uint32_t &Y2, uint32_t &D, const CellK &K) {
+    // a = x + v, b = y + u, a2 = x2 + v, b2 = y2 + u (ksw2_extd2_sse.c:240-243), tagged
+    const uint32_t A = X + V + K.cA, Bv = Y + U + K.cB, A2 = X2 + V + K.cA2, B2 = Y2 + U + K.cB2;
+    uint32_t Z = __vimax3_s16x2(__vimax3_s16x2(sc, A, Bv), A2, B2);
+    if (CIGAR) {
+        D = (Z & 0x000f000fu) ^ Tags<CIGAR, RIGHT>::dx;
+        Z &= 0xfff0fff0u;
+    }
+    Z = __vmins2(Z, K.mch);  // ksw2_extd2_sse.c:252
+    const uint32_t Un = Z - V + add2(FB), Vn = Z - U + add2(FB);
+    const uint32_t Wa = A + K.nzA - Z, Wb = Bv + K.nzB - Z, Wa2 = A2 + K.nzA2 - Z, Wb2 = B2 + K.nzB2 - Z;
+    X = __vmaxs2(Wa, K.kqe);
+    Y = __vmaxs2(Wb, K.kqe);
+    X2 = __vmaxs2(Wa2, K.kqe2);
+    Y2 = __vmaxs2(Wb2, K.kqe2);
+    if (CIGAR) {
+        D += 0x08u * __viaddmin_s16x2_relu(Wa, K.cq, 0x00010001u);
+        D += 0x10u * __viaddmin_s16x2_relu(Wb, K.cq, 0x00010001u);
+        D += 0x20u * __viaddmin_s16x2_relu(Wa2, K.cq2, 0x00010001u);
+        D += 0x40u * __viaddmin_s16x2_relu(Wb2, K.cq2, 0x00010001u);
+    }
+    U = Un;
+    V = Vn;
+}
+
+__device__ __forceinline__ int fld(uint32_t w, int f) { return f ? (int)(w >> 16) : (int)(w & 0xffffu); }
 
 // Lexicographic (value, position) maximum: later positions win ties, the
 // ">=" end-tracking rule of ksw2_extd2_sse.c:369-372.
@@ -175,18 +163,75 @@ __device__ __forceinline__ void best_merge(int &v, int &p, int ov, int op) {
     if (ov > v || (ov == v && op > p)) v = ov, p = op;
 }
 
+// State of one warp's sweep over one strip.
+struct Sweep {
+    uint32_t rlo[16], rhi[16];  // score rows of the 16 columns: bytes s+128 for query codes 0..6, byte 7 = 0
+    uint32_t U[8], Y[8], Y2[8];  // column state, column pair c = (col0 + c, col0 + 8 + c)
+    uint32_t X, V, X2;           // values flowing right; after a step: the outputs of column pair 7
+    uint32_t qlo, qhi;           // query codes of the rows of the low / high fields at the last step
+    uint32_t vcap;               // last strip: v of the pair's last column at the last step
+};
+
+// One step of a warp: rows jlo = k - 2*lane (low fields) and jlo - 1 (high fields).
+// MASKED: some field of the warp is outside [0, qlen): those fields start from safe
+// left values and keep their column state.  LAST: capture v of column pair cc.
+template <bool CIGAR, bool RIGHT, bool MASKED, bool LAST>
+__device__ __forceinline__ void sweep_step(Sweep &w, uint32_t r0, uint32_t r1, uint32_t qlo, uint32_t M, int cc,
+                                           const CellK &K, uint8_t *tbdst) {
+    uint32_t X = prmt(r0, w.X, 0x5410), V = prmt(r0, w.V, 0x5432), X2 = prmt(r1, w.X2, 0x5410);
+    if (MASKED) {
+        X = (X & M) | (rep2(FBX) & ~M);
+        V = (V & M) | (rep2(FB) & ~M);
+        X2 = (X2 & M) | (rep2(FBX) & ~M);
+    }
+    const uint32_t qhi = w.qlo;
+    const uint32_t sel_lo = 0x7770u | qlo, sel_hi = 0x7077u | (qhi << 8);
+    uint32_t D[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint32_t plo = prmt(w.rlo[c], w.rhi[c], sel_lo), phi = prmt(w.rlo[8 + c], w.rhi[8 + c], sel_hi);
+        const uint32_t sc = (plo + phi) * 16u + K.cS;
+        uint32_t u = w.U[c], y = w.Y[c], y2 = w.Y2[c];
+        cell2<CIGAR, RIGHT>(sc, X, V, X2, u, y, y2, D[c], K);
+        if (MASKED) {
+            w.U[c] = (u & M) | (w.U[c] & ~M);
+            w.Y[c] = (y & M) | (w.Y[c] & ~M);
+            w.Y2[c] = (y2 & M) | (w.Y2[c] & ~M);
+        } else {
+            w.U[c] = u, w.Y[c] = y, w.Y2[c] = y2;
+        }
+        if (LAST && c == cc) w.vcap = V;
+    }
+    w.X = X, w.V = V, w.X2 = X2;
+    w.qlo = qlo, w.qhi = qhi;
+    if (CIGAR) {
+        const uint32_t e01 = D[0] + D[1] * 256u, e23 = D[2] + D[3] * 256u;
+        const uint32_t e45 = D[4] + D[5] * 256u, e67 = D[6] + D[7] * 256u;
+        const uint4 v = make_uint4(prmt(e01, e23, 0x5410), prmt(e45, e67, 0x5410), prmt(e01, e23, 0x7632),
+                                   prmt(e45, e67, 0x7632));
+        __stcs(reinterpret_cast<uint4 *>(tbdst), v);
+    }
+}
+
+template <bool CIGAR, bool RIGHT, bool LAST>
+__device__ __forceinline__ void sweep_dispatch(bool masked, Sweep &w, uint32_t r0, uint32_t r1, uint32_t qlo,
+                                               uint32_t M, int cc, const CellK &K, uint8_t *tbdst) {
+    if (masked) sweep_step<CIGAR, RIGHT, true, LAST>(w, r0, r1, qlo, M, cc, K, tbdst);
+    else sweep_step<CIGAR, RIGHT, false, LAST>(w, r0, r1, qlo, M, cc, K, tbdst);
+}
+
 template <bool CIGAR, bool RIGHT, int W>
-__global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
-    constexpr int C = KSW_COLS;
+__global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int g = warp / W;
     const int wg = warp % W;
     const KswScore &S = A.sc;
+    const CellK K = make_cellk<CIGAR, RIGHT>(S);
     __shared__ int s_pair[MAX_GROUP_WARPS];
-    __shared__ int s_prog[MAX_GROUP_WARPS];           // rows published, per warp (monotone per pair)
+    __shared__ int s_prog[MAX_GROUP_WARPS];  // progress published, per warp (monotone per pair)
     __shared__ int s_red[MAX_GROUP_WARPS][5];
-    __shared__ int s_stop[MAX_GROUP_WARPS];           // the group's pair passed the deadline
+    __shared__ int s_stop[MAX_GROUP_WARPS];  // the group's pair passed the deadline
     int *prog = s_prog + g * W;
     volatile int *stop_flag = s_stop + g;
 
@@ -205,39 +250,53 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
         const int qlen = P.qlen, tlen = P.tlen;
         const uint8_t *qs = A.qcodes + P.qoff;
         const uint8_t *ts = A.tcodes + P.toff;
-        uint32_t *bnd = A.bnd + P.bnd_off;
+        // boundary column of strip s: rows at [s * (qlen + 1), +qlen), its last-row H after them
+        uint2 *bnd = reinterpret_cast<uint2 *>(A.bnd + P.bnd_off);
+        const int64_t bstride = qlen + 1;
         uint8_t *tb = CIGAR ? A.tb + P.tb_off : nullptr;
         const int nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
-        const int stride_k = qlen + 31;
-        int mqe = AW_NEG_INF, mqe_t = -1, mte = AW_NEG_INF, mte_q = -1, score = AW_NEG_INF;
+        const int64_t stride_k = qlen + KSW_LAG;
+        // progress of a warp: strip * pstride + (rows published, then +1 for the last-row H)
+        const int pstride = qlen + 2;
+        // the pair's last column: owning strip, lane, field and column pair
+        const int tl1 = tlen - 1;
+        const int c_lane = (tl1 % KSW_STRIP) >> 4, c_fld = (tl1 >> 3) & 1, c_cc = tl1 & 7;
+        int mqe16 = INT_MIN, mqe_t = -1, mte16 = INT_MIN, mte_q = -1, score16 = INT_MIN;
         bool stopped = false;
 
         for (int s = wg; s < nstrip && !stopped; s += W) {
-            const int col0 = s * KSW_STRIP + lane * C;
-            int ut[C], yt[C], y2t[C], H[C];
-            uint32_t rlo[C], rhi[C];
+            const int col0 = s * KSW_STRIP + lane * 16;
+            const bool last = s == nstrip - 1;
+            Sweep w;
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
+            for (int c = 0; c < 16; ++c) {
                 const int col = col0 + c;
                 const int tc = col < tlen ? (ts[col] & 7) : 0;
-                rlo[c] = S.tab_lo[tc];
-                rhi[c] = S.tab_hi[tc];
-                ut[c] = edge_diff(col, S);
-                yt[c] = -S.qe;
-                y2t[c] = -S.qe2;
-                H[c] = htop(col, S);
+                w.rlo[c] = S.tab_lo[tc] ^ 0x80808080u;
+                w.rhi[c] = (S.tab_hi[tc] ^ 0x80808080u) & 0x00ffffffu;
             }
-            // rows of the previous strip must be published before we read them
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                w.U[c] = (uint32_t)(16 * edge_diff(col0 + c, S) + FB) |
+                         ((uint32_t)(16 * edge_diff(col0 + 8 + c, S) + FB) << 16);
+                w.Y[c] = rep2(FBX - 16 * S.qe);
+                w.Y2[c] = rep2(FBX - 16 * S.qe2);
+            }
+            w.X = rep2(FBX), w.V = rep2(FB), w.X2 = rep2(FBX);
+            w.qlo = 0, w.qhi = 0, w.vcap = rep2(FB);
+            int hm16 = 16 * htop(tl1, S);  // H(-1, tlen-1), then down the last column
             const int src_prog_warp = (wg + W - 1) % W;
-            uint32_t carry = 0, qchunk = 0, bchunk = 0;
-            const int last_k = qlen + 31;
+            uint32_t qchunk = 0;
+            uint2 bchunk = make_uint2(0, 0);
+            const uint32_t edge_x = (uint32_t)(FBX - 16 * S.qe), edge_x2 = (uint32_t)(FBX - 16 * S.qe2);
+            const int last_k = qlen + KSW_LAG;
             for (int k = 0; k < last_k; ++k) {
                 if ((k & 31) == 0 && A.deadline) {
                     // cooperative stop, polled every 32 rows (ksw2_progress.c:30-38 polls
                     // every 256 anti-diagonals); any warp of the group stops the pair
                     int st = 0;
                     if (lane == 0) st = (*stop_flag || aw_deadline_passed(A.deadline)) ? 1 : 0;
-                    st = __shfl_sync(0xffffffffu, st, 0);
+                    st = __shfl_sync(FULLMASK, st, 0);
                     if (st) {
                         if (lane == 0) *stop_flag = 1;
                         stopped = true;
@@ -246,13 +305,12 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
                 }
                 if ((k & 31) == 0 && k < qlen) {
                     const int J = k;
-                    qchunk = (J + lane < qlen) ? qs[J + lane] : 0u;
+                    qchunk = (J + lane < qlen) ? (qs[J + lane] & 7u) : 0u;
                     if (s > 0) {
                         const int need = min(J + 32, qlen);
                         int spins = 0;
                         cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[src_prog_warp]);
-                        // the producer publishes (strip, rows) as strip*(qlen+1)+rows
-                        const int target = (s - 1) * (qlen + 1) + need;
+                        const int target = (s - 1) * pstride + need;
                         while (pr.load(cuda::memory_order_acquire) < target) {
                             if (*stop_flag) break;  // the producer stopped at the deadline
                             if (++spins > (1 << 26)) {
@@ -263,90 +321,145 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
                         }
                         if (A.deadline) {
                             int st = lane == 0 ? *stop_flag : 0;
-                            st = __shfl_sync(0xffffffffu, st, 0);
+                            st = __shfl_sync(FULLMASK, st, 0);
                             if (st) {
                                 stopped = true;
                                 break;
                             }
                         }
-                        bchunk = (J + lane < qlen) ? __ldcg(bnd + (int64_t)(s - 1) * qlen + J + lane) : 0u;
+                        bchunk = (J + lane < qlen) ? __ldcg(bnd + (int64_t)(s - 1) * bstride + J + lane)
+                                                   : make_uint2(0, 0);
                     }
                 }
-                const uint32_t qv = __shfl_sync(0xffffffffu, qchunk, k & 31);
-                const uint32_t bv = __shfl_sync(0xffffffffu, bchunk, k & 31);
-                const uint32_t in = __shfl_up_sync(0xffffffffu, carry, 1);
-                const int j = k - lane;
-                int xs, vs, x2s;
-                uint32_t qc;
+                // left values of the low fields: lane L-1's high column 15 (row k-2L), or the
+                // strip's left edge for lane 0 (row k)
+                const uint32_t w0 = prmt(w.X, w.V, 0x7632), w1 = prmt(w.X2, w.qhi, 0x5432);
+                uint32_t r0 = __shfl_up_sync(FULLMASK, w0, 1), r1 = __shfl_up_sync(FULLMASK, w1, 1);
+                const uint32_t qv = __shfl_sync(FULLMASK, qchunk, k & 31);
+                uint32_t bx = 0, by = 0;
+                if (s > 0) {
+                    bx = __shfl_sync(FULLMASK, bchunk.x, k & 31);
+                    by = __shfl_sync(FULLMASK, bchunk.y, k & 31);
+                }
+                uint32_t qlo = r1 >> 16;
                 if (lane == 0) {
-                    qc = qv & 7u;
+                    qlo = qv;
                     if (s == 0) {
-                        xs = -S.qe, x2s = -S.qe2, vs = edge_diff(j, S);
+                        r0 = edge_x | ((uint32_t)(16 * edge_diff(k, S) + FB) << 16);
+                        r1 = edge_x2;
                     } else {
-                        xs = sx8(bv), vs = sx8(bv >> 8), x2s = sx8(bv >> 16);
+                        r0 = bx, r1 = by;
+                    }
+                }
+                const int jlo = k - 2 * lane;
+                const bool masked = k < KSW_LAG || k >= qlen;  // warp-uniform
+                uint32_t M = 0xffffffffu;
+                if (masked)
+                    M = ((unsigned)jlo < (unsigned)qlen ? 0x0000ffffu : 0u) |
+                        ((unsigned)(jlo - 1) < (unsigned)qlen ? 0xffff0000u : 0u);
+                uint8_t *tbdst = CIGAR ? tb + (((int64_t)s * stride_k + k) * 32 + lane) * 16 : nullptr;
+                if (last) {
+                    sweep_dispatch<CIGAR, RIGHT, true>(masked, w, r0, r1, qlo, M, c_cc, K, tbdst);
+                    if (lane == c_lane) {
+                        const int row = jlo - c_fld;
+                        if ((unsigned)row < (unsigned)qlen) {
+                            hm16 += fld(w.vcap, c_fld) - FB;
+                            if (hm16 >= mte16) mte16 = hm16, mte_q = row;
+                        }
                     }
                 } else {
-                    qc = in >> 24;
-                    xs = sx8(in), vs = sx8(in >> 8), x2s = sx8(in >> 16);
-                }
-                if (j >= 0 && j < qlen) {
-                    const uint32_t sel = qc * 0x1111u + 0x8880u;
-                    uint32_t dlo = 0, dhi = 0;
-#pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        int d = 0;
-                        const int sc = prmt_sx(rlo[c], rhi[c], sel);
-                        cell<CIGAR, RIGHT>(sc, xs, vs, x2s, ut[c], yt[c], y2t[c], d, S);
-                        H[c] += vs;
-                        if (CIGAR) {
-                            if (c < 4) dlo |= (uint32_t)d << (8 * c);
-                            else dhi |= (uint32_t)d << (8 * (c - 4));
-                        }
-                    }
-                    carry = pack3(xs, vs, x2s, qc);
-                    if (CIGAR) {
-                        uint2 *dst = reinterpret_cast<uint2 *>(tb + (((int64_t)s * stride_k + k) * 32 + lane) * C);
-                        __stcs(dst, make_uint2(dlo, dhi));
-                    }
-                    if (j == qlen - 1) {
-#pragma unroll
-                        for (int c = 0; c < C; ++c) {
-                            const int col = col0 + c;
-                            if (col < tlen && H[c] >= mqe) mqe = H[c], mqe_t = col;
-                        }
-                    }
-                    const int cl = tlen - 1 - col0;
-                    if (cl >= 0 && cl < C) {
-                        int hv = H[0];
-#pragma unroll
-                        for (int c = 1; c < C; ++c)
-                            if (c == cl) hv = H[c];
-                        if (hv >= mte) mte = hv, mte_q = j;
-                        if (j == qlen - 1) score = hv;
-                    }
-                    if (lane == 31 && s + 1 < nstrip) bnd[(int64_t)s * qlen + j] = pack3(xs, vs, x2s, 0);
+                    sweep_dispatch<CIGAR, RIGHT, false>(masked, w, r0, r1, qlo, M, c_cc, K, tbdst);
                 }
                 if (lane == 31 && s + 1 < nstrip) {
-                    const int jj = k - 31;
-                    if (jj >= 0 && ((jj & 31) == 31 || jj == qlen - 1)) {
-                        // the consumer reads these rows from L2 (ld.cg), so they must be
-                        // visible at device scope before the row count is published
-                        __threadfence();
-                        cuda::atomic_ref<int, cuda::thread_scope_block> pw(prog[wg]);
-                        pw.store(s * (qlen + 1) + jj + 1, cuda::memory_order_release);
+                    const int jj = k - KSW_LAG;  // row of the high fields of lane 31
+                    if (jj >= 0 && jj < qlen) {
+                        bnd[(int64_t)s * bstride + jj] = make_uint2(prmt(w.X, w.V, 0x7632), w.X2 >> 16);
+                        if ((jj & 31) == 31 || jj == qlen - 1) {
+                            // the consumer reads these rows from L2 (ld.cg), so they must be
+                            // visible at device scope before the row count is published
+                            __threadfence();
+                            cuda::atomic_ref<int, cuda::thread_scope_block> pw(prog[wg]);
+                            pw.store(s * pstride + jj + 1, cuda::memory_order_release);
+                        }
                     }
                 }
             }
             __syncwarp();
+            if (stopped) break;
+            // last row: H(qlen-1, col) = H(qlen-1, col0 - 1) + the prefix sum of the last
+            // row's u (the column state after the sweep) along the strip
+            int lsum = 0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) lsum += fld(w.U[c], 0) + fld(w.U[c], 1) - 2 * FB;
+            int incl = lsum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULLMASK, incl, o);
+                if (lane >= o) incl += t;
+            }
+            int base16 = 0;
+            if (s == 0) {
+                base16 = 16 * htop(qlen - 1, S);
+            } else {
+                if (lane == 0) {
+                    int spins = 0;
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[src_prog_warp]);
+                    const int target = (s - 1) * pstride + qlen + 1;
+                    while (pr.load(cuda::memory_order_acquire) < target) {
+                        if (*stop_flag) break;
+                        if (++spins > (1 << 26)) {
+                            atomicExch(A.error, 1);
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                    base16 = (int)__ldcg(bnd + (int64_t)(s - 1) * bstride + qlen).x;
+                }
+                base16 = __shfl_sync(FULLMASK, base16, 0);
+                if (A.deadline) {
+                    int st = lane == 0 ? *stop_flag : 0;
+                    if (__shfl_sync(FULLMASK, st, 0)) {
+                        stopped = true;
+                        break;
+                    }
+                }
+            }
+            int h = base16 + incl - lsum;
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    h += fld(w.U[c], f) - FB;
+                    const int col = col0 + 8 * f + c;
+                    if (col < tlen) {
+                        if (h >= mqe16) mqe16 = h, mqe_t = col;
+                        if (col == tl1) score16 = h;
+                    }
+                }
+            }
+            if (lane == 31 && s + 1 < nstrip) {
+                bnd[(int64_t)s * bstride + qlen] = make_uint2((uint32_t)h, 0u);
+                __threadfence();
+                cuda::atomic_ref<int, cuda::thread_scope_block> pw(prog[wg]);
+                pw.store(s * pstride + qlen + 1, cuda::memory_order_release);
+            }
+            if (last) {
+                // mte over the last column, tracked by its lane
+                mte16 = __shfl_sync(FULLMASK, mte16, c_lane);
+                mte_q = __shfl_sync(FULLMASK, mte_q, c_lane);
+            }
         }
+        int mqe = mqe_t >= 0 ? mqe16 >> 4 : AW_NEG_INF;
+        int mte = mte_q >= 0 ? mte16 >> 4 : AW_NEG_INF;
+        int score = score16 != INT_MIN ? score16 >> 4 : AW_NEG_INF;
         // reduce end tracking over lanes, then over the warps of the group
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            const int ov = __shfl_xor_sync(0xffffffffu, mqe, o), op = __shfl_xor_sync(0xffffffffu, mqe_t, o);
+            const int ov = __shfl_xor_sync(FULLMASK, mqe, o), op = __shfl_xor_sync(FULLMASK, mqe_t, o);
             best_merge(mqe, mqe_t, ov, op);
-            const int tv = __shfl_xor_sync(0xffffffffu, mte, o), tp = __shfl_xor_sync(0xffffffffu, mte_q, o);
+            const int tv = __shfl_xor_sync(FULLMASK, mte, o), tp = __shfl_xor_sync(FULLMASK, mte_q, o);
             best_merge(mte, mte_q, tv, tp);
-            score = max(score, __shfl_xor_sync(0xffffffffu, score, o));
+            score = max(score, __shfl_xor_sync(FULLMASK, score, o));
         }
         if (lane == 0) {
             s_red[warp][0] = mqe, s_red[warp][1] = mqe_t, s_red[warp][2] = mte, s_red[warp][3] = mte_q;
@@ -354,8 +467,8 @@ __global__ void __launch_bounds__(256) ksw_full_kernel(KswFullArgs A) {
         }
         group_sync(g, W * 32);
         if (wg == 0 && lane == 0) {
-            for (int w = 1; w < W; ++w) {
-                const int *rr = s_red[g * W + w];
+            for (int w2 = 1; w2 < W; ++w2) {
+                const int *rr = s_red[g * W + w2];
                 best_merge(mqe, mqe_t, rr[0], rr[1]);
                 best_merge(mte, mte_q, rr[2], rr[3]);
                 score = max(score, rr[4]);
@@ -431,13 +544,14 @@ __global__ void __launch_bounds__(32 * BT_WARPS)
         else o.score = o.mte, i0 = tlen - 1, j0 = o.mte_q;
     }
     const uint8_t *tb = tb_arena + P.tb_off;
-    const int64_t stride_k = qlen + 31;
+    const int64_t stride_k = qlen + KSW_LAG;
     Cache cache;
     cache.init(tiles[warp]);
     auto load = [&](int gg, int jj) -> uint2 {
         if (gg < 0 || jj < 0 || jj >= qlen || (gg << 3) >= tlen) return make_uint2(0, 0);
-        const int s = gg >> 5, L = gg & 31;
-        return __ldcs(reinterpret_cast<const uint2 *>(tb + (((int64_t)s * stride_k + jj + L) * 32 + L) * KSW_COLS));
+        const int s = gg / KSW_GROUPS, L = gg % KSW_GROUPS;
+        return __ldcs(reinterpret_cast<const uint2 *>(
+            tb + (((int64_t)s * stride_k + jj + L) * KSW_GROUPS + L) * KSW_COLS));
     };
     WarpCigar w{cig + P.cig_off, 0, 0, 0};
     int i = i0, j = j0, state = 0;

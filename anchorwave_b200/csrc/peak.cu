@@ -32,13 +32,36 @@ __global__ void __launch_bounds__(256) int_peak_kernel(int32_t *sink, int seed) 
     if (acc == 0x7fffffff) sink[0] = acc;  // never true in practice; keeps the chains live
 }
 
-}  // namespace
+// The same chains on two 16-bit fields per register (the packed cells of the KSW2 strip
+// kernel): a 32-bit add of a per-field constant (the clamps keep every field far from a
+// carry), SIMD max / min of the fields, xor.  Each instruction is two field operations.
+__global__ void __launch_bounds__(256) int16x2_peak_kernel(uint32_t *sink, int seed) {
+    uint32_t v[CHAINS];
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) v[c] = ((threadIdx.x * 7u + c * 13u + seed) & 0x0fffu) * 0x10001u + 0x10001000u;
+    const uint32_t a = 0x00030003u, lo = 0x08000800u + (uint32_t)(seed & 7), hi = 0x60006000u, x = 0x00050005u;
+#pragma unroll 1
+    for (int it = 0; it < ITERS; ++it) {
+#pragma unroll
+        for (int c = 0; c < CHAINS; ++c) {
+            uint32_t t = v[c] + a;
+            t = __vmaxs2(t, lo);
+            t = __vmins2(t, hi);
+            v[c] = t ^ x;
+        }
+    }
+    uint32_t acc = 0;
+#pragma unroll
+    for (int c = 0; c < CHAINS; ++c) acc += v[c];
+    if (acc == 0x7fffffffu) sink[0] = acc;  // never true in practice; keeps the chains live
+}
 
-extern "C" double aw_int32_peak_ops(void) {
+template <class K, class T>
+double probe(K kernel, double ops_per_chain_iter) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0.0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0.0;
-    int32_t *sink = nullptr;
+    T *sink = nullptr;
     if (cudaMalloc(&sink, 4) != cudaSuccess) return 0.0;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -47,12 +70,12 @@ extern "C" double aw_int32_peak_ops(void) {
     double best = 0.0;
     for (int rep = 0; rep < 4; ++rep) {
         cudaEventRecord(e0);
-        int_peak_kernel<<<blocks, threads>>>(sink, rep + 1);
+        kernel<<<blocks, threads>>>(sink, rep + 1);
         cudaEventRecord(e1);
         if (cudaEventSynchronize(e1) != cudaSuccess) break;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        const double ops = (double)blocks * threads * ITERS * CHAINS * 4.0;
+        const double ops = (double)blocks * threads * ITERS * CHAINS * ops_per_chain_iter;
         if (rep > 0 && ms > 0.f) best = ops / (ms * 1e-3) > best ? ops / (ms * 1e-3) : best;
     }
     cudaEventDestroy(e0);
@@ -60,3 +83,10 @@ extern "C" double aw_int32_peak_ops(void) {
     cudaFree(sink);
     return best;
 }
+
+}  // namespace
+
+// Field operations per second of the packed 16x2 chains (2 per instruction).
+extern "C" double aw_int16x2_peak_ops(void) { return probe<decltype(&int16x2_peak_kernel), uint32_t>(int16x2_peak_kernel, 8.0); }
+
+extern "C" double aw_int32_peak_ops(void) { return probe<decltype(&int_peak_kernel), int32_t>(int_peak_kernel, 4.0); }

@@ -248,6 +248,10 @@ int aw_device_count(void);
 /* Integer-ALU peak probe: IADD3/IMNMX-class 32-bit ops per second measured on
  * the current device (used as the roofline denominator for the DP kernels). */
 double aw_int32_peak_ops(void);
+/* The same probe on two 16-bit fields per register (32-bit add of a per-field constant,
+ * SIMD max/min, xor): field operations per second, the denominator of the full-matrix
+ * strip kernel, which computes two cells per instruction.  No counterpart in the reference. */
+double aw_int16x2_peak_ops(void);
 
 #define AW_OK            0
 #define AW_E_INVAL     (-1)
