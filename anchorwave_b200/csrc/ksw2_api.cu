@@ -202,8 +202,7 @@ static KswScore make_score(const Params &P) {
 // intermediate of the recurrence (a, b, a2, b2 before and after the z
 // adjustment, u, v, x, y, x2, y2) inside int8 for the invariant ranges x,y in
 // [-(q+e),-e], x2,y2 in [-(q2+e2),-e2], u,v in [-(q+e), mch+(q+e)], and inside
-// the kernel's field biases.  Its score rows keep byte 7 free (zero), so the
-// alphabet is at most 7 codes; m = 8 goes to the banded kernel at full width.
+// the kernel's field biases.
 static bool full_path_ok(const Params &P, int qlen, int tlen, int w) {
     if (exact_stop_enabled()) return false;
     const int allowed = AW_EZ_SCORE_ONLY | AW_EZ_RIGHT | AW_EZ_GENERIC_SC | AW_EZ_REV_CIGAR |
@@ -216,7 +215,6 @@ static bool full_path_ok(const Params &P, int qlen, int tlen, int w) {
     if (P.e2 > P.e || P.q2 < P.q) return false;
     const int mag = (P.q2 + P.e2) + (P.q + P.e) + std::abs(P.min_sc) + std::abs((int)P.mat[0]);
     if (mag > 100) return false;
-    if (P.m > 7) return false;
     const int64_t nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
     if (nstrip * ((int64_t)qlen + 2) + qlen > INT_MAX / 2) return false;
     return true;

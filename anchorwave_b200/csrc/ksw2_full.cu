@@ -163,34 +163,45 @@ __device__ __forceinline__ void best_merge(int &v, int &p, int ov, int op) {
     if (ov > v || (ov == v && op > p)) v = ov, p = op;
 }
 
+// Score profile of a lane: for each query code q (0..7) the 16 tagged score fields of the
+// lane's columns, 256 B per lane in shared memory, read back by the same lane only.  The
+// low columns (0..7) and the high columns (8..15) are 16 B each; lanes with bit 2 set store
+// them swapped, so the 8 lanes of a quarter-warp load 16 B each from distinct banks.
+constexpr int PROF_LANE = 32;                 // bytes per lane and code
+constexpr int PROF_CODE = 32 * PROF_LANE;     // bytes per code (one warp)
+constexpr int PROF_WARP = 8 * PROF_CODE;      // bytes per warp
+
 // State of one warp's sweep over one strip.
 struct Sweep {
-    uint32_t rlo[16], rhi[16];  // score rows of the 16 columns: bytes s+128 for query codes 0..6, byte 7 = 0
     uint32_t U[8], Y[8], Y2[8];  // column state, column pair c = (col0 + c, col0 + 8 + c)
     uint32_t X, V, X2;           // values flowing right; after a step: the outputs of column pair 7
     uint32_t qlo, qhi;           // query codes of the rows of the low / high fields at the last step
     uint32_t vcap;               // last strip: v of the pair's last column at the last step
 };
 
+__device__ __forceinline__ uint32_t u4w(const uint4 &v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+
 // One step of a warp: rows jlo = k - 2*lane (low fields) and jlo - 1 (high fields).
-// MASKED: some field of the warp is outside [0, qlen): those fields start from safe
-// left values and keep their column state.  LAST: capture v of column pair cc.
+// r0/r1: the left values of the low fields ([x, v] and [x2, query code]); the high fields
+// take the low fields' column 7 of the previous step.  MASKED: some field of the warp is
+// outside [0, qlen): those fields start from safe left values and keep their column
+// state.  LAST: capture v of column pair cc.
 template <bool CIGAR, bool RIGHT, bool MASKED, bool LAST>
-__device__ __forceinline__ void sweep_step(Sweep &w, uint32_t r0, uint32_t r1, uint32_t qlo, uint32_t M, int cc,
-                                           const CellK &K, uint8_t *tbdst) {
+__device__ __forceinline__ void sweep_step(Sweep &w, uint32_t r0, uint32_t r1, uint32_t M, int cc, const CellK &K,
+                                           const uint8_t *prof_lo, const uint8_t *prof_hi, uint8_t *tbdst) {
     uint32_t X = prmt(r0, w.X, 0x5410), V = prmt(r0, w.V, 0x5432), X2 = prmt(r1, w.X2, 0x5410);
     if (MASKED) {
         X = (X & M) | (rep2(FBX) & ~M);
         V = (V & M) | (rep2(FB) & ~M);
         X2 = (X2 & M) | (rep2(FBX) & ~M);
     }
-    const uint32_t qhi = w.qlo;
-    const uint32_t sel_lo = 0x7770u | qlo, sel_hi = 0x7077u | (qhi << 8);
+    const uint32_t qlo = r1 >> 16, qhi = w.qlo;
+    const uint4 slo = *reinterpret_cast<const uint4 *>(prof_lo + qlo * PROF_CODE);
+    const uint4 shi = *reinterpret_cast<const uint4 *>(prof_hi + qhi * PROF_CODE);
     uint32_t D[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const uint32_t plo = prmt(w.rlo[c], w.rhi[c], sel_lo), phi = prmt(w.rlo[8 + c], w.rhi[8 + c], sel_hi);
-        const uint32_t sc = (plo + phi) * 16u + K.cS;
+        const uint32_t sc = prmt(u4w(slo, c >> 1), u4w(shi, c >> 1), (c & 1) ? 0x7632 : 0x5410);
         uint32_t u = w.U[c], y = w.Y[c], y2 = w.Y2[c];
         cell2<CIGAR, RIGHT>(sc, X, V, X2, u, y, y2, D[c], K);
         if (MASKED) {
@@ -213,15 +224,79 @@ __device__ __forceinline__ void sweep_step(Sweep &w, uint32_t r0, uint32_t r1, u
     }
 }
 
+// Per-strip context shared by the steps.
+struct StripCtx {
+    int qlen, lane, s, nstrip, c_lane, c_fld, c_cc;
+    uint2 *bnd;                 // this pair's boundary columns
+    int64_t bstride;            // entries per strip
+    int *prog;                  // this warp's published progress (shared memory)
+    int pstride;
+    const uint8_t *prof_lo, *prof_hi;
+    uint8_t *tb;                // this lane's traceback word of step 0 of the strip
+    bool bnd_writer;            // lane 31 of a strip with a right neighbour
+};
+
+// Steps [k0, k1) of a strip; bx/by: lane i holds the left values of lane 0 for row k0 + i.
+template <bool CIGAR, bool RIGHT, bool MASKED, bool LAST>
+__device__ __forceinline__ void sweep_chunk(Sweep &w, const StripCtx &C, int k0, int k1, uint32_t bx, uint32_t by,
+                                            const CellK &K, int &hm16, int &mte16, int &mte_q) {
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+        const uint32_t w0 = prmt(w.X, w.V, 0x7632), w1 = prmt(w.X2, w.qhi, 0x5432);
+        uint32_t r0 = __shfl_up_sync(FULLMASK, w0, 1), r1 = __shfl_up_sync(FULLMASK, w1, 1);
+        const uint32_t b0 = __shfl_sync(FULLMASK, bx, k - k0), b1 = __shfl_sync(FULLMASK, by, k - k0);
+        if (C.lane == 0) r0 = b0, r1 = b1;
+        const int jlo = k - 2 * C.lane;
+        uint32_t M = 0xffffffffu;
+        if (MASKED)
+            M = ((unsigned)jlo < (unsigned)C.qlen ? 0x0000ffffu : 0u) |
+                ((unsigned)(jlo - 1) < (unsigned)C.qlen ? 0xffff0000u : 0u);
+        uint8_t *tbdst = CIGAR ? C.tb + (int64_t)k * (32 * 16) : nullptr;
+        sweep_step<CIGAR, RIGHT, MASKED, LAST>(w, r0, r1, M, C.c_cc, K, C.prof_lo, C.prof_hi, tbdst);
+        if (LAST && C.lane == C.c_lane) {
+            const int row = jlo - C.c_fld;
+            if ((unsigned)row < (unsigned)C.qlen) {
+                hm16 += fld(w.vcap, C.c_fld) - FB;
+                if (hm16 >= mte16) mte16 = hm16, mte_q = row;
+            }
+        }
+        if (C.bnd_writer) {
+            const int jj = k - KSW_LAG;  // row of the high fields of lane 31
+            if ((unsigned)jj < (unsigned)C.qlen) {
+                C.bnd[(int64_t)C.s * C.bstride + jj] = make_uint2(prmt(w.X, w.V, 0x7632), w.X2 >> 16);
+                if ((jj & 31) == 31 || jj == C.qlen - 1) {
+                    // the consumer reads these rows from L2 (ld.cg), so they must be
+                    // visible at device scope before the row count is published
+                    __threadfence();
+                    cuda::atomic_ref<int, cuda::thread_scope_block> pw(*C.prog);
+                    pw.store(C.s * C.pstride + jj + 1, cuda::memory_order_release);
+                }
+            }
+        }
+    }
+}
+
 template <bool CIGAR, bool RIGHT, bool LAST>
-__device__ __forceinline__ void sweep_dispatch(bool masked, Sweep &w, uint32_t r0, uint32_t r1, uint32_t qlo,
-                                               uint32_t M, int cc, const CellK &K, uint8_t *tbdst) {
-    if (masked) sweep_step<CIGAR, RIGHT, true, LAST>(w, r0, r1, qlo, M, cc, K, tbdst);
-    else sweep_step<CIGAR, RIGHT, false, LAST>(w, r0, r1, qlo, M, cc, K, tbdst);
+__device__ __forceinline__ void sweep_range(Sweep &w, const StripCtx &C, int k0, int k1, uint32_t bx, uint32_t by,
+                                            const CellK &K, int &hm16, int &mte16, int &mte_q) {
+    // every field of every lane is inside [0, qlen) for k in [KSW_LAG, qlen)
+    const int f0 = max(k0, KSW_LAG), f1 = min(k1, C.qlen);
+    if (f0 >= f1) {
+        sweep_chunk<CIGAR, RIGHT, true, LAST>(w, C, k0, k1, bx, by, K, hm16, mte16, mte_q);
+        return;
+    }
+    // the chunk's sub-ranges keep the lane-0 words of row k0 + i in lane i
+    if (k0 < f0) sweep_chunk<CIGAR, RIGHT, true, LAST>(w, C, k0, f0, bx, by, K, hm16, mte16, mte_q);
+    sweep_chunk<CIGAR, RIGHT, false, LAST>(w, C, f0, f1, __shfl_down_sync(FULLMASK, bx, f0 - k0),
+                                           __shfl_down_sync(FULLMASK, by, f0 - k0), K, hm16, mte16, mte_q);
+    if (f1 < k1)
+        sweep_chunk<CIGAR, RIGHT, true, LAST>(w, C, f1, k1, __shfl_down_sync(FULLMASK, bx, f1 - k0),
+                                              __shfl_down_sync(FULLMASK, by, f1 - k0), K, hm16, mte16, mte_q);
 }
 
 template <bool CIGAR, bool RIGHT, int W>
 __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
+    extern __shared__ __align__(16) uint8_t prof_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int g = warp / W;
@@ -234,6 +309,9 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
     __shared__ int s_stop[MAX_GROUP_WARPS];  // the group's pair passed the deadline
     int *prog = s_prog + g * W;
     volatile int *stop_flag = s_stop + g;
+    uint8_t *prof = prof_smem + warp * PROF_WARP + lane * PROF_LANE;
+    const int sw = (lane >> 2) & 1;
+    using T = Tags<CIGAR, RIGHT>;
 
     for (;;) {
         group_sync(g, W * 32);
@@ -250,31 +328,54 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
         const int qlen = P.qlen, tlen = P.tlen;
         const uint8_t *qs = A.qcodes + P.qoff;
         const uint8_t *ts = A.tcodes + P.toff;
-        // boundary column of strip s: rows at [s * (qlen + 1), +qlen), its last-row H after them
-        uint2 *bnd = reinterpret_cast<uint2 *>(A.bnd + P.bnd_off);
-        const int64_t bstride = qlen + 1;
-        uint8_t *tb = CIGAR ? A.tb + P.tb_off : nullptr;
         const int nstrip = (tlen + KSW_STRIP - 1) / KSW_STRIP;
-        const int64_t stride_k = qlen + KSW_LAG;
-        // progress of a warp: strip * pstride + (rows published, then +1 for the last-row H)
-        const int pstride = qlen + 2;
-        // the pair's last column: owning strip, lane, field and column pair
         const int tl1 = tlen - 1;
-        const int c_lane = (tl1 % KSW_STRIP) >> 4, c_fld = (tl1 >> 3) & 1, c_cc = tl1 & 7;
+        StripCtx C;
+        C.qlen = qlen, C.lane = lane, C.nstrip = nstrip;
+        // boundary column of strip s: rows at [s * (qlen + 1), +qlen), its last-row H after them
+        C.bnd = reinterpret_cast<uint2 *>(A.bnd + P.bnd_off);
+        C.bstride = qlen + 1;
+        C.prog = prog + wg;
+        // progress of a warp: strip * pstride + (rows published, then +1 for the last-row H)
+        C.pstride = qlen + 2;
+        C.prof_lo = prof + 16 * sw, C.prof_hi = prof + 16 * (1 - sw);
+        // the pair's last column: owning lane, field and column pair (in the last strip)
+        C.c_lane = (tl1 % KSW_STRIP) >> 4, C.c_fld = (tl1 >> 3) & 1, C.c_cc = tl1 & 7;
+        const int64_t stride_k = qlen + KSW_LAG;
         int mqe16 = INT_MIN, mqe_t = -1, mte16 = INT_MIN, mte_q = -1, score16 = INT_MIN;
         bool stopped = false;
 
         for (int s = wg; s < nstrip && !stopped; s += W) {
             const int col0 = s * KSW_STRIP + lane * 16;
             const bool last = s == nstrip - 1;
-            Sweep w;
+            C.s = s;
+            C.bnd_writer = lane == 31 && s + 1 < nstrip;
+            C.tb = CIGAR ? A.tb + P.tb_off + ((int64_t)s * stride_k * 32 + lane) * 16 : nullptr;
+            // score profile of the lane's 16 columns for query codes 0..7
+            {
+                uint32_t tlo[16], thi[16];
 #pragma unroll
-            for (int c = 0; c < 16; ++c) {
-                const int col = col0 + c;
-                const int tc = col < tlen ? (ts[col] & 7) : 0;
-                w.rlo[c] = S.tab_lo[tc] ^ 0x80808080u;
-                w.rhi[c] = (S.tab_hi[tc] ^ 0x80808080u) & 0x00ffffffu;
+                for (int c = 0; c < 16; ++c) {
+                    const int col = col0 + c;
+                    const int tc = col < tlen ? (ts[col] & 7) : 0;
+                    tlo[c] = S.tab_lo[tc], thi[c] = S.tab_hi[tc];
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    uint32_t wd[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int sa = (int)(int8_t)(uint8_t)(((q < 4 ? tlo[2 * i] : thi[2 * i]) >> (8 * (q & 3))) & 0xff);
+                        const int sb =
+                            (int)(int8_t)(uint8_t)(((q < 4 ? tlo[2 * i + 1] : thi[2 * i + 1]) >> (8 * (q & 3))) & 0xff);
+                        wd[i] = (uint32_t)(16 * sa + T::s + FB) | ((uint32_t)(16 * sb + T::s + FB) << 16);
+                    }
+                    *reinterpret_cast<uint4 *>(prof + q * PROF_CODE + 16 * sw) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+                    *reinterpret_cast<uint4 *>(prof + q * PROF_CODE + 16 * (1 - sw)) =
+                        make_uint4(wd[4], wd[5], wd[6], wd[7]);
+                }
             }
+            Sweep w;
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
                 w.U[c] = (uint32_t)(16 * edge_diff(col0 + c, S) + FB) |
@@ -286,12 +387,10 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
             w.qlo = 0, w.qhi = 0, w.vcap = rep2(FB);
             int hm16 = 16 * htop(tl1, S);  // H(-1, tlen-1), then down the last column
             const int src_prog_warp = (wg + W - 1) % W;
-            uint32_t qchunk = 0;
-            uint2 bchunk = make_uint2(0, 0);
             const uint32_t edge_x = (uint32_t)(FBX - 16 * S.qe), edge_x2 = (uint32_t)(FBX - 16 * S.qe2);
             const int last_k = qlen + KSW_LAG;
-            for (int k = 0; k < last_k; ++k) {
-                if ((k & 31) == 0 && A.deadline) {
+            for (int k0 = 0; k0 < last_k; k0 += 32) {
+                if (A.deadline) {
                     // cooperative stop, polled every 32 rows (ksw2_progress.c:30-38 polls
                     // every 256 anti-diagonals); any warp of the group stops the pair
                     int st = 0;
@@ -303,86 +402,47 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
                         break;
                     }
                 }
-                if ((k & 31) == 0 && k < qlen) {
-                    const int J = k;
-                    qchunk = (J + lane < qlen) ? (qs[J + lane] & 7u) : 0u;
-                    if (s > 0) {
-                        const int need = min(J + 32, qlen);
-                        int spins = 0;
-                        cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[src_prog_warp]);
-                        const int target = (s - 1) * pstride + need;
-                        while (pr.load(cuda::memory_order_acquire) < target) {
-                            if (*stop_flag) break;  // the producer stopped at the deadline
-                            if (++spins > (1 << 26)) {
-                                atomicExch(A.error, 1);
-                                break;
+                // lane 0's left values for rows k0 .. k0+31, one row per lane, with the
+                // row's query code in the top half of the second word
+                const int row = k0 + lane;
+                uint32_t bx = 0, by = 0;
+                if (k0 < qlen) {
+                    const uint32_t qc = row < qlen ? (qs[row] & 7u) : 0u;
+                    if (s == 0) {
+                        bx = edge_x | ((uint32_t)(16 * edge_diff(row, S) + FB) << 16);
+                        by = edge_x2 | (qc << 16);
+                    } else {
+                        const int need = min(k0 + 32, qlen);
+                        if (lane == 0) {
+                            int spins = 0;
+                            cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[src_prog_warp]);
+                            const int target = (s - 1) * C.pstride + need;
+                            while (pr.load(cuda::memory_order_acquire) < target) {
+                                if (*stop_flag) break;  // the producer stopped at the deadline
+                                if (++spins > (1 << 26)) {
+                                    atomicExch(A.error, 1);
+                                    break;
+                                }
+                                __nanosleep(32);
                             }
-                            __nanosleep(32);
                         }
+                        __syncwarp();
                         if (A.deadline) {
                             int st = lane == 0 ? *stop_flag : 0;
-                            st = __shfl_sync(FULLMASK, st, 0);
-                            if (st) {
+                            if (__shfl_sync(FULLMASK, st, 0)) {
                                 stopped = true;
                                 break;
                             }
                         }
-                        bchunk = (J + lane < qlen) ? __ldcg(bnd + (int64_t)(s - 1) * bstride + J + lane)
-                                                   : make_uint2(0, 0);
-                    }
-                }
-                // left values of the low fields: lane L-1's high column 15 (row k-2L), or the
-                // strip's left edge for lane 0 (row k)
-                const uint32_t w0 = prmt(w.X, w.V, 0x7632), w1 = prmt(w.X2, w.qhi, 0x5432);
-                uint32_t r0 = __shfl_up_sync(FULLMASK, w0, 1), r1 = __shfl_up_sync(FULLMASK, w1, 1);
-                const uint32_t qv = __shfl_sync(FULLMASK, qchunk, k & 31);
-                uint32_t bx = 0, by = 0;
-                if (s > 0) {
-                    bx = __shfl_sync(FULLMASK, bchunk.x, k & 31);
-                    by = __shfl_sync(FULLMASK, bchunk.y, k & 31);
-                }
-                uint32_t qlo = r1 >> 16;
-                if (lane == 0) {
-                    qlo = qv;
-                    if (s == 0) {
-                        r0 = edge_x | ((uint32_t)(16 * edge_diff(k, S) + FB) << 16);
-                        r1 = edge_x2;
-                    } else {
-                        r0 = bx, r1 = by;
-                    }
-                }
-                const int jlo = k - 2 * lane;
-                const bool masked = k < KSW_LAG || k >= qlen;  // warp-uniform
-                uint32_t M = 0xffffffffu;
-                if (masked)
-                    M = ((unsigned)jlo < (unsigned)qlen ? 0x0000ffffu : 0u) |
-                        ((unsigned)(jlo - 1) < (unsigned)qlen ? 0xffff0000u : 0u);
-                uint8_t *tbdst = CIGAR ? tb + (((int64_t)s * stride_k + k) * 32 + lane) * 16 : nullptr;
-                if (last) {
-                    sweep_dispatch<CIGAR, RIGHT, true>(masked, w, r0, r1, qlo, M, c_cc, K, tbdst);
-                    if (lane == c_lane) {
-                        const int row = jlo - c_fld;
-                        if ((unsigned)row < (unsigned)qlen) {
-                            hm16 += fld(w.vcap, c_fld) - FB;
-                            if (hm16 >= mte16) mte16 = hm16, mte_q = row;
-                        }
-                    }
-                } else {
-                    sweep_dispatch<CIGAR, RIGHT, false>(masked, w, r0, r1, qlo, M, c_cc, K, tbdst);
-                }
-                if (lane == 31 && s + 1 < nstrip) {
-                    const int jj = k - KSW_LAG;  // row of the high fields of lane 31
-                    if (jj >= 0 && jj < qlen) {
-                        bnd[(int64_t)s * bstride + jj] = make_uint2(prmt(w.X, w.V, 0x7632), w.X2 >> 16);
-                        if ((jj & 31) == 31 || jj == qlen - 1) {
-                            // the consumer reads these rows from L2 (ld.cg), so they must be
-                            // visible at device scope before the row count is published
-                            __threadfence();
-                            cuda::atomic_ref<int, cuda::thread_scope_block> pw(prog[wg]);
-                            pw.store(s * pstride + jj + 1, cuda::memory_order_release);
+                        if (row < qlen) {
+                            const uint2 e = __ldcg(C.bnd + (int64_t)(s - 1) * C.bstride + row);
+                            bx = e.x, by = (e.y & 0xffffu) | (qc << 16);
                         }
                     }
                 }
+                const int k1 = min(k0 + 32, last_k);
+                if (last) sweep_range<CIGAR, RIGHT, true>(w, C, k0, k1, bx, by, K, hm16, mte16, mte_q);
+                else sweep_range<CIGAR, RIGHT, false>(w, C, k0, k1, bx, by, K, hm16, mte16, mte_q);
             }
             __syncwarp();
             if (stopped) break;
@@ -404,7 +464,7 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
                 if (lane == 0) {
                     int spins = 0;
                     cuda::atomic_ref<int, cuda::thread_scope_block> pr(prog[src_prog_warp]);
-                    const int target = (s - 1) * pstride + qlen + 1;
+                    const int target = (s - 1) * C.pstride + qlen + 1;
                     while (pr.load(cuda::memory_order_acquire) < target) {
                         if (*stop_flag) break;
                         if (++spins > (1 << 26)) {
@@ -413,7 +473,7 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
                         }
                         __nanosleep(32);
                     }
-                    base16 = (int)__ldcg(bnd + (int64_t)(s - 1) * bstride + qlen).x;
+                    base16 = (int)__ldcg(C.bnd + (int64_t)(s - 1) * C.bstride + qlen).x;
                 }
                 base16 = __shfl_sync(FULLMASK, base16, 0);
                 if (A.deadline) {
@@ -437,16 +497,11 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
                     }
                 }
             }
-            if (lane == 31 && s + 1 < nstrip) {
-                bnd[(int64_t)s * bstride + qlen] = make_uint2((uint32_t)h, 0u);
+            if (C.bnd_writer) {
+                C.bnd[(int64_t)s * C.bstride + qlen] = make_uint2((uint32_t)h, 0u);
                 __threadfence();
                 cuda::atomic_ref<int, cuda::thread_scope_block> pw(prog[wg]);
-                pw.store(s * pstride + qlen + 1, cuda::memory_order_release);
-            }
-            if (last) {
-                // mte over the last column, tracked by its lane
-                mte16 = __shfl_sync(FULLMASK, mte16, c_lane);
-                mte_q = __shfl_sync(FULLMASK, mte_q, c_lane);
+                pw.store(s * C.pstride + qlen + 1, cuda::memory_order_release);
             }
         }
         int mqe = mqe_t >= 0 ? mqe16 >> 4 : AW_NEG_INF;
@@ -583,9 +638,16 @@ __global__ void ksw_pack_cigar_kernel(const KswPair *pairs, int n, const KswOut 
     for (int i = lane; i < nc; i += 32) dst[i] = src[i];
 }
 
+// Dynamic shared memory of a CTA: the score profiles of its warps.
+inline int prof_bytes(int warps) { return warps * PROF_WARP; }
+
 template <bool CIGAR, bool RIGHT, int W>
 cudaError_t launch_t(const KswFullArgs &a, int groups, int ctas, cudaStream_t st) {
-    ksw_full_kernel<CIGAR, RIGHT, W><<<ctas, groups * W * 32, 0, st>>>(a);
+    const int smem = prof_bytes(groups * W);
+    cudaError_t e = cudaFuncSetAttribute(ksw_full_kernel<CIGAR, RIGHT, W>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, prof_bytes(8));
+    if (e != cudaSuccess) return e;
+    ksw_full_kernel<CIGAR, RIGHT, W><<<ctas, groups * W * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -607,7 +669,10 @@ int ksw_full_occupancy(int flag, int warps_per_pair, int groups_per_cta) {
     const int threads = warps_per_pair * groups_per_cta * 32;
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY), right = !!(flag & AW_EZ_RIGHT);
     cudaError_t e = cudaErrorInvalidValue;
-#define AW_OCC(CG, RT, WW) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ksw_full_kernel<CG, RT, WW>, threads, 0)
+#define AW_OCC(CG, RT, WW)                                                                                   \
+    cudaFuncSetAttribute(ksw_full_kernel<CG, RT, WW>, cudaFuncAttributeMaxDynamicSharedMemorySize, prof_bytes(8)); \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ksw_full_kernel<CG, RT, WW>, threads,                   \
+                                                      prof_bytes(warps_per_pair * groups_per_cta))
 #define AW_OCC_W(CG, RT)                                                 \
     switch (warps_per_pair) {                                            \
     case 1: AW_OCC(CG, RT, 1); break;                                    \
