@@ -62,6 +62,9 @@ struct KswFullArgs {
     // the calling thread's deadline (globaltimer ns) or null: pairs still running when it
     // passes stop with ez->stopped = 1 (the cooperative stop of minimap2/ksw2_progress.c)
     const unsigned long long *deadline = nullptr;
+    // 1, passed at run time: the strip kernel's 2-input adds are multiply-adds by it, which
+    // the compiler keeps on the FMA pipe
+    uint32_t one = 1;
 };
 
 #ifdef __CUDACC__

@@ -77,11 +77,14 @@ __device__ __forceinline__ void group_sync(int g, int nthreads) {
 }
 
 // ---- packed cell fields ------------------------------------------------------------
-// Field biases.  With the magnitude bound of full_path_ok (every |u|, |v|, |x|, ... <= 300
-// even for the bounded excursions of masked-off fields) every 32-bit add below keeps each
-// field inside [0, 65536) and every value a DPX op compares inside [0, 32768).
-constexpr int FB = 8192;    // u, v, z, the score and the max candidates
-constexpr int FBX = 16384;  // x, y, x2, y2
+// Every field holds 16*value + FB; x, y, x2, y2 carry their candidate's priority tag on
+// top (so x + v is already the tagged candidate a), and the score carries 2*FB + its tag.
+// With the magnitude bound of full_path_ok (|u|, |v|, |x|, ... <= 300, and the bounded
+// excursions of masked-off fields within one step) every 32-bit add below keeps each field
+// inside [0, 65536) and every value a DPX op compares for a live field inside [0, 32768).
+// The adds are 2-input multiply-adds by a runtime one (or minus one), so they issue on the
+// FMA pipe and leave the ALU pipe to the max/min/permute work.
+constexpr int FB = 12288;
 // A constant in both fields: for 32-bit adds (c * 65537, so that a negative c borrows
 // exactly what the field sum carries back) and for SIMD operands (each field = c).
 __host__ __device__ constexpr uint32_t add2(int c) { return (uint32_t)c * 0x10001u; }
@@ -102,26 +105,28 @@ struct Tags {
 
 // Per-launch packed constants of the cell.
 struct CellK {
-    uint32_t cA, cB, cA2, cB2;      // candidate = left/up values + c (rebias + tag)
-    uint32_t cS;                    // score field = 16 * (s + 128) + cS
-    uint32_t nzA, nzB, nzA2, nzB2;  // W = candidate + nz - Z = 16 (cand - z - e) + FBX
-    uint32_t kqe, kqe2;             // x' = max(W, kqe)                       (SIMD)
-    uint32_t cq, cq2;               // continuation bit = relu(min(W + cq, 1)) (SIMD)
-    uint32_t mch;                   // z = min(z, mch)                        (SIMD)
+    uint32_t ke, ke2;               // Ze = Z + ke: W = candidate - Ze = 16 (cand - z - e) + FB + tag
+    uint32_t kxa, kxb, kxa2, kxb2;  // x' = max(W, kx): the field of -(q+e) (-(q2+e2)) with the tag (SIMD)
+    uint32_t ca, cb, ca2, cb2;      // continuation: relu(min(W + c, 8 or 16))       (SIMD)
+    uint32_t mch;                   // z = min(z, mch)                                (SIMD)
+    uint32_t one, neg1;             // runtime 1 and -1 of the multiply-adds
 };
 
 template <bool CIGAR, bool RIGHT>
-__device__ __forceinline__ CellK make_cellk(const KswScore &S) {
+__device__ __forceinline__ CellK make_cellk(const KswScore &S, uint32_t one) {
     using T = Tags<CIGAR, RIGHT>;
     CellK K;
-    K.cA = add2(T::a - FBX), K.cB = add2(T::b - FBX), K.cA2 = add2(T::a2 - FBX), K.cB2 = add2(T::b2 - FBX);
-    K.cS = add2(T::s + FB - 16 * 128);
-    K.nzA = add2(FBX - 16 * S.e - T::a), K.nzB = add2(FBX - 16 * S.e - T::b);
-    K.nzA2 = add2(FBX - 16 * S.e2 - T::a2), K.nzB2 = add2(FBX - 16 * S.e2 - T::b2);
-    K.kqe = rep2(FBX - 16 * S.qe), K.kqe2 = rep2(FBX - 16 * S.qe2);
-    // left-aligned: a - z + q > 0 (ksw2_extd2_sse.c:268-271); right-aligned: >= 0 (:315-318)
-    K.cq = rep2(16 * S.qe - FBX + (RIGHT ? 1 : 0)), K.cq2 = rep2(16 * S.qe2 - FBX + (RIGHT ? 1 : 0));
-    K.mch = rep2(16 * S.mch + FB);
+    K.ke = add2(16 * S.e - FB), K.ke2 = add2(16 * S.e2 - FB);
+    const int xa = FB - 16 * S.qe + T::a, xb = FB - 16 * S.qe + T::b;
+    const int xa2 = FB - 16 * S.qe2 + T::a2, xb2 = FB - 16 * S.qe2 + T::b2;
+    K.kxa = rep2(xa), K.kxb = rep2(xb), K.kxa2 = rep2(xa2), K.kxb2 = rep2(xb2);
+    // left-aligned: a - z + q > 0 (ksw2_extd2_sse.c:268-271) <=> W - kx >= 16;
+    // right-aligned: >= 0 (:315-318) <=> W - kx >= 0.  The a bit is 8, the others 16
+    // (scaled to 32 and 64 when they are added to the state byte).
+    K.ca = rep2((RIGHT ? 8 : -8) - xa), K.cb = rep2((RIGHT ? 16 : 0) - xb);
+    K.ca2 = rep2((RIGHT ? 16 : 0) - xa2), K.cb2 = rep2((RIGHT ? 16 : 0) - xb2);
+    K.mch = rep2(16 * S.mch + 2 * FB);
+    K.one = one, K.neg1 = 0u - one;
     return K;
 }
 
@@ -132,24 +137,25 @@ template <bool CIGAR, bool RIGHT>
 __device__ __forceinline__ void cell2(uint32_t sc, uint32_t &X, uint32_t &V, uint32_t &X2, uint32_t &U,
                                       uint32_t &Y, uint32_t &Y2, uint32_t &D, const CellK &K) {
     // a = x + v, b = y + u, a2 = x2 + v, b2 = y2 + u (ksw2_extd2_sse.c:240-243), tagged
-    const uint32_t A = X + V + K.cA, Bv = Y + U + K.cB, A2 = X2 + V + K.cA2, B2 = Y2 + U + K.cB2;
-    uint32_t Z = __vimax3_s16x2(__vimax3_s16x2(sc, A, Bv), A2, B2);
+    const uint32_t A = X * K.one + V, Bv = Y * K.one + U, A2 = X2 * K.one + V, B2 = Y2 * K.one + U;
+    uint32_t Z = __vimax3_s16x2(__vimax3_s16x2(sc, Bv, B2), A, A2);
     if (CIGAR) {
         D = (Z & 0x000f000fu) ^ Tags<CIGAR, RIGHT>::dx;
         Z &= 0xfff0fff0u;
     }
     Z = __vmins2(Z, K.mch);  // ksw2_extd2_sse.c:252
-    const uint32_t Un = Z - V + add2(FB), Vn = Z - U + add2(FB);
-    const uint32_t Wa = A + K.nzA - Z, Wb = Bv + K.nzB - Z, Wa2 = A2 + K.nzA2 - Z, Wb2 = B2 + K.nzB2 - Z;
-    X = __vmaxs2(Wa, K.kqe);
-    Y = __vmaxs2(Wb, K.kqe);
-    X2 = __vmaxs2(Wa2, K.kqe2);
-    Y2 = __vmaxs2(Wb2, K.kqe2);
+    const uint32_t Un = V * K.neg1 + Z, Vn = U * K.neg1 + Z;
+    const uint32_t Ze = Z * K.one + K.ke, Ze2 = Z * K.one + K.ke2;
+    const uint32_t Wa = Ze * K.neg1 + A, Wb = Ze * K.neg1 + Bv, Wa2 = Ze2 * K.neg1 + A2, Wb2 = Ze2 * K.neg1 + B2;
+    X = __vmaxs2(Wa, K.kxa);
+    Y = __vmaxs2(Wb, K.kxb);
+    X2 = __vmaxs2(Wa2, K.kxa2);
+    Y2 = __vmaxs2(Wb2, K.kxb2);
     if (CIGAR) {
-        D += 0x08u * __viaddmin_s16x2_relu(Wa, K.cq, 0x00010001u);
-        D += 0x10u * __viaddmin_s16x2_relu(Wb, K.cq, 0x00010001u);
-        D += 0x20u * __viaddmin_s16x2_relu(Wa2, K.cq2, 0x00010001u);
-        D += 0x40u * __viaddmin_s16x2_relu(Wb2, K.cq2, 0x00010001u);
+        D = __viaddmin_s16x2_relu(Wa, K.ca, 0x00080008u) * K.one + D;
+        D = __viaddmin_s16x2_relu(Wb, K.cb, 0x00100010u) * K.one + D;
+        D = __viaddmin_s16x2_relu(Wa2, K.ca2, 0x00100010u) * 2u + D;
+        D = __viaddmin_s16x2_relu(Wb2, K.cb2, 0x00100010u) * 4u + D;
     }
     U = Un;
     V = Vn;
@@ -191,9 +197,9 @@ __device__ __forceinline__ void sweep_step(Sweep &w, uint32_t r0, uint32_t r1, u
                                            const uint8_t *prof_lo, const uint8_t *prof_hi, uint8_t *tbdst) {
     uint32_t X = prmt(r0, w.X, 0x5410), V = prmt(r0, w.V, 0x5432), X2 = prmt(r1, w.X2, 0x5410);
     if (MASKED) {
-        X = (X & M) | (rep2(FBX) & ~M);
+        X = (X & M) | (K.kxa & ~M);
         V = (V & M) | (rep2(FB) & ~M);
-        X2 = (X2 & M) | (rep2(FBX) & ~M);
+        X2 = (X2 & M) | (K.kxa2 & ~M);
     }
     const uint32_t qlo = r1 >> 16, qhi = w.qlo;
     const uint4 slo = *reinterpret_cast<const uint4 *>(prof_lo + qlo * PROF_CODE);
@@ -302,7 +308,7 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
     const int g = warp / W;
     const int wg = warp % W;
     const KswScore &S = A.sc;
-    const CellK K = make_cellk<CIGAR, RIGHT>(S);
+    const CellK K = make_cellk<CIGAR, RIGHT>(S, A.one);
     __shared__ int s_pair[MAX_GROUP_WARPS];
     __shared__ int s_prog[MAX_GROUP_WARPS];  // progress published, per warp (monotone per pair)
     __shared__ int s_red[MAX_GROUP_WARPS][5];
@@ -368,7 +374,7 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
                         const int sa = (int)(int8_t)(uint8_t)(((q < 4 ? tlo[2 * i] : thi[2 * i]) >> (8 * (q & 3))) & 0xff);
                         const int sb =
                             (int)(int8_t)(uint8_t)(((q < 4 ? tlo[2 * i + 1] : thi[2 * i + 1]) >> (8 * (q & 3))) & 0xff);
-                        wd[i] = (uint32_t)(16 * sa + T::s + FB) | ((uint32_t)(16 * sb + T::s + FB) << 16);
+                        wd[i] = (uint32_t)(16 * sa + T::s + 2 * FB) | ((uint32_t)(16 * sb + T::s + 2 * FB) << 16);
                     }
                     *reinterpret_cast<uint4 *>(prof + q * PROF_CODE + 16 * sw) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
                     *reinterpret_cast<uint4 *>(prof + q * PROF_CODE + 16 * (1 - sw)) =
@@ -380,14 +386,14 @@ __global__ void __launch_bounds__(256, 2) ksw_full_kernel(KswFullArgs A) {
             for (int c = 0; c < 8; ++c) {
                 w.U[c] = (uint32_t)(16 * edge_diff(col0 + c, S) + FB) |
                          ((uint32_t)(16 * edge_diff(col0 + 8 + c, S) + FB) << 16);
-                w.Y[c] = rep2(FBX - 16 * S.qe);
-                w.Y2[c] = rep2(FBX - 16 * S.qe2);
+                w.Y[c] = K.kxb;
+                w.Y2[c] = K.kxb2;
             }
-            w.X = rep2(FBX), w.V = rep2(FB), w.X2 = rep2(FBX);
+            w.X = K.kxa, w.V = rep2(FB), w.X2 = K.kxa2;
             w.qlo = 0, w.qhi = 0, w.vcap = rep2(FB);
             int hm16 = 16 * htop(tl1, S);  // H(-1, tlen-1), then down the last column
             const int src_prog_warp = (wg + W - 1) % W;
-            const uint32_t edge_x = (uint32_t)(FBX - 16 * S.qe), edge_x2 = (uint32_t)(FBX - 16 * S.qe2);
+            const uint32_t edge_x = K.kxa & 0xffffu, edge_x2 = K.kxa2 & 0xffffu;
             const int last_k = qlen + KSW_LAG;
             for (int k0 = 0; k0 < last_k; k0 += 32) {
                 if (A.deadline) {
