@@ -33,21 +33,25 @@ __global__ void __launch_bounds__(256) int_peak_kernel(int32_t *sink, int seed) 
 }
 
 // The same chains on two 16-bit fields per register (the packed cells of the KSW2 strip
-// kernel): a 32-bit add of a per-field constant (the clamps keep every field far from a
-// carry), SIMD max / min of the fields, xor.  Each instruction is two field operations.
+// kernel), using both integer pipes as that kernel does: an add of a per-field constant
+// as a multiply-add by a runtime one (FMA pipe), SIMD max (ALU pipe), a second add,
+// SIMD min.  The clamps keep every field far from a carry.  Each instruction is two field
+// operations.
 __global__ void __launch_bounds__(256) int16x2_peak_kernel(uint32_t *sink, int seed) {
     uint32_t v[CHAINS];
 #pragma unroll
     for (int c = 0; c < CHAINS; ++c) v[c] = ((threadIdx.x * 7u + c * 13u + seed) & 0x0fffu) * 0x10001u + 0x10001000u;
-    const uint32_t a = 0x00030003u, lo = 0x08000800u + (uint32_t)(seed & 7), hi = 0x60006000u, x = 0x00050005u;
+    const uint32_t one = seed > 0 ? 1u : 3u;  // 1 at run time, unknown to the compiler
+    const uint32_t a = 0x00030003u, b = 0xfffdfffeu /* -2 in both fields, as a 32-bit add */;
+    const uint32_t lo = 0x08000800u + (uint32_t)(seed & 7), hi = 0x60006000u;
 #pragma unroll 1
     for (int it = 0; it < ITERS; ++it) {
 #pragma unroll
         for (int c = 0; c < CHAINS; ++c) {
-            uint32_t t = v[c] + a;
+            uint32_t t = v[c] * one + a;
             t = __vmaxs2(t, lo);
-            t = __vmins2(t, hi);
-            v[c] = t ^ x;
+            t = t * one + b;
+            v[c] = __vmins2(t, hi);
         }
     }
     uint32_t acc = 0;

@@ -505,8 +505,9 @@ def main():
         "phase_ms": {"dp": dp_mean, "traceback": float(np.mean(bt_ms))},
         "roofline": {"bound": "int16x2", "achieved": achieved_ops / 1e12, "peak": simd_peak / 1e12, "unit": "TOPS",
                      "frac": achieved_ops / simd_peak if simd_peak else None, "traffic": None,
-                     "peak_source": "aw_int16x2_peak_ops() live microbenchmark (add/max/min/xor chains on two "
-                                    "16-bit fields per register, 2 field-ops per instruction)",
+                     "peak_source": "aw_int16x2_peak_ops() live microbenchmark (chains of FMA-pipe adds and "
+                                    "ALU-pipe SIMD max/min on two 16-bit fields per register, "
+                                    "2 field-ops per instruction)",
                      "int32_peak": int_peak / 1e12,
                      "ops_per_cell": OPS_PER_CELL_CIGAR,
                      "hbm_store": {"achieved": tb_gbs, "peak": hbm_peak, "unit": "GB/s", "frac": tb_gbs / hbm_peak,

@@ -248,9 +248,10 @@ int aw_device_count(void);
 /* Integer-ALU peak probe: IADD3/IMNMX-class 32-bit ops per second measured on
  * the current device (used as the roofline denominator for the DP kernels). */
 double aw_int32_peak_ops(void);
-/* The same probe on two 16-bit fields per register (32-bit add of a per-field constant,
- * SIMD max/min, xor): field operations per second, the denominator of the full-matrix
- * strip kernel, which computes two cells per instruction.  No counterpart in the reference. */
+/* The same probe on two 16-bit fields per register, on both integer pipes (per-field adds
+ * as multiply-adds on the FMA pipe, SIMD max/min on the ALU pipe): field operations per
+ * second, the denominator of the full-matrix strip kernel, which computes two cells per
+ * instruction on the same two pipes.  No counterpart in the reference. */
 double aw_int16x2_peak_ops(void);
 
 #define AW_OK            0
