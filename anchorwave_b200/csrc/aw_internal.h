@@ -2,6 +2,7 @@
 #pragma once
 #include <stdint.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 
 #define AW_NEG_INF (-0x40000000)
 #define AW_E_CUDA_INTERNAL (-2)
@@ -99,12 +100,23 @@ inline int64_t ksw_full_bnd_words(int qlen, int tlen) {
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
+    // Grows by half the current capacity, at most 256 MiB more than that (pooled buffers
+    // see batches of varying size, and every cudaFree synchronises the device), falling
+    // back to exactly n when the larger request does not fit.
     cudaError_t ensure(size_t n) {
         if (n <= cap) return cudaSuccess;
+        const size_t grown = cap + std::min(cap / 2, (size_t)256 << 20);
         if (p) cudaFree(p);
         p = nullptr;
-        cap = 0;
         size_t want = n < 4096 ? 4096 : n;
+        if (grown > want && cap > 0) {
+            if (cudaMalloc(&p, grown) == cudaSuccess) {
+                cap = grown;
+                return cudaSuccess;
+            }
+            cudaGetLastError();
+        }
+        cap = 0;
         cudaError_t e = cudaMalloc(&p, want);
         if (e == cudaSuccess) cap = want;
         return e;
@@ -120,6 +132,8 @@ void set_error(const char *msg);
 
 // Traceback budget of the calling thread's batches, 0 = process-wide (ksw2_api.cu).
 void set_thread_tb_budget(int64_t bytes);
+// Allocates the calling thread's pooled traceback arena (ksw2_api.cu).
+int reserve_thread_tb(int64_t bytes);
 
 // Strip-path parameter check + score table (ksw2_api.cu).
 int full_path_params(int qlen, int tlen, int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2,

@@ -590,9 +590,17 @@ static int plan_launch(aw_ksw_plan_t *pl) {
             a.order = B->order.as<int32_t>() + W.begin_small;
             a.n = W.n_small;
             a.queue = B->queue.as<int32_t>() + 64 * (2 * k + 1);
-            const int occ = std::max(1, ksw_full_occupancy(P.flag, 1, 8));
-            const int ctas = std::min((W.n_small + 7) / 8, occ * B->sms);
-            AW_CUDA(launch_ksw_full(a, P.flag, 1, 8, ctas, B->st));
+            // warps per small pair: one when the pairs alone fill the resident warps, else
+            // up to 8 so that a small batch still runs on the whole GPU (a pair's strips
+            // then pipeline over its warps instead of running one after another)
+            const int resident = 16 * B->sms;  // 2 CTAs x 8 warps per SM
+            const int64_t used = std::min<int64_t>((int64_t)W.n_large * large_warps, resident);
+            int ws = 1;
+            while (ws < 8 && (int64_t)W.n_small * (2 * ws) <= resident - used) ws *= 2;
+            const int groups = 8 / ws;
+            const int occ = std::max(1, ksw_full_occupancy(P.flag, ws, groups));
+            const int ctas = std::min((W.n_small + groups - 1) / groups, occ * B->sms);
+            AW_CUDA(launch_ksw_full(a, P.flag, ws, groups, ctas, B->st));
             ++launches;
         }
         AW_CUDA(cudaEventRecord(B->ev_b, B->st2));
@@ -880,6 +888,14 @@ void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tle
 namespace aw {
 // Traceback budget of the calling thread's batches (0 = the process-wide setting).
 void set_thread_tb_budget(int64_t bytes) { tls_tb_budget = bytes; }
+
+// Allocates the calling thread's traceback arena up front (serving workers), so that
+// batches do not grow it (a device-wide synchronisation) while other workers run.
+int reserve_thread_tb(int64_t bytes) {
+    Buffers *B = thread_buffers();
+    if (B->init()) return AW_E_CUDA;
+    return B->tb.ensure((size_t)bytes + 256) == cudaSuccess ? AW_OK : AW_E_CUDA;
+}
 
 // Parameter checks and score table of the full-matrix strip path, for callers
 // outside this file.  Returns AW_OK when (qlen, tlen, parameters, flag) can run

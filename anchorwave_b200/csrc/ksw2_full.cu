@@ -41,6 +41,7 @@
 #include "aw_internal.h"
 #include "tb_walk.cuh"
 #include <cuda/atomic>
+#include <atomic>
 
 namespace aw {
 
@@ -671,6 +672,15 @@ cudaError_t launch_w(const KswFullArgs &a, int W, int groups, int ctas, cudaStre
 }  // namespace
 
 int ksw_full_occupancy(int flag, int warps_per_pair, int groups_per_cta) {
+    // CTAs per SM depend only on the instantiation and the CTA shape: cached per device
+    static std::atomic<int> cache[16][3][4][4];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int mode = (flag & AW_EZ_SCORE_ONLY) ? 0 : (flag & AW_EZ_RIGHT) ? 2 : 1;
+    const int wi = warps_per_pair == 1 ? 0 : warps_per_pair == 2 ? 1 : warps_per_pair == 4 ? 2 : 3;
+    const int gi = groups_per_cta == 1 ? 0 : groups_per_cta == 2 ? 1 : groups_per_cta == 4 ? 2 : 3;
+    std::atomic<int> *slot = dev >= 0 && dev < 16 ? &cache[dev][mode][wi][gi] : nullptr;
+    if (slot && slot->load() > 0) return slot->load();
     int nb = 0;
     const int threads = warps_per_pair * groups_per_cta * 32;
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY), right = !!(flag & AW_EZ_RIGHT);
@@ -691,7 +701,9 @@ int ksw_full_occupancy(int flag, int warps_per_pair, int groups_per_cta) {
     else { AW_OCC_W(false, false) }
 #undef AW_OCC_W
 #undef AW_OCC
-    return e == cudaSuccess ? nb : 0;
+    if (e != cudaSuccess) return 0;
+    if (slot) slot->store(nb);
+    return nb;
 }
 
 cudaError_t launch_ksw_full(const KswFullArgs &a, int flag, int warps_per_pair, int groups_per_cta,

@@ -6,9 +6,10 @@
 //     the engine the caller's selector chose for it (KSW2 full/banded, KSW2
 //     Singletrack, WFA, WFA Singletrack);
 //   * `slots` worker threads each own their CUDA streams and pooled device
-//     buffers (the thread-local pools of the batch entries); an idle worker takes
-//     the oldest queued requests of one engine/parameter class, up to max_batch,
-//     as one micro-batch, so requests that arrive while others run on the GPU
+//     buffers (the thread-local pools of the batch entries); requests wait in one
+//     FIFO per engine/parameter class, and an idle worker takes the class whose
+//     head waited longest, up to max_batch of its requests, as one micro-batch,
+//     so requests that arrive while others run on the GPU
 //     are admitted as soon as a worker and memory are free, and the micro-batches
 //     of different workers overlap on the device;
 //   * admission: each request carries its predicted device bytes (traceback or
@@ -34,6 +35,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 using namespace aw;
@@ -99,7 +101,10 @@ struct aw_server {
     aw_serve_config_t cfg;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Req> queue;
+    // one FIFO per class (engine, KSW2 scoring flag, length class); popping the front of
+    // a class keeps a take O(batch) however long the backlog is
+    std::map<std::tuple<int, int, int>, std::deque<Req>> queues;
+    size_t queued = 0;
     std::map<uint64_t, Res> done;
     uint64_t next_release = 0;
     int64_t inflight_bytes = 0;
@@ -114,32 +119,35 @@ struct aw_server {
 
 namespace {
 
-// Pops one micro-batch: the oldest request plus later ones of the same class
-// (engine, scoring flag, length class) while they fit the batch size and the budget.
+// Pops one micro-batch: the requests of the class whose head waited longest, oldest
+// first, while they fit the batch size and the budget.
 bool take_batch(aw_server *S, std::vector<Req> &batch) {
     batch.clear();
-    if (S->queue.empty()) return false;
-    const Req &head = S->queue.front();
+    if (S->queued == 0) return false;
+    std::deque<Req> *q = nullptr;
+    for (auto &kv : S->queues)
+        if (!kv.second.empty() && (!q || kv.second.front().id < q->front().id)) q = &kv.second;
     const int64_t budget = S->cfg.hbm_budget;
-    if (S->inflight_bytes > 0 && S->inflight_bytes + head.pred > budget) return false;
-    // requests of one class share a launch: same engine, KSW2 scoring flag and length class
-    // (bands may differ)
-    auto klass = [](const Req &r) { return std::make_tuple(r.method, r.generic, r.bucket); };
-    const auto k0 = klass(head);
+    if (S->inflight_bytes > 0 && S->inflight_bytes + q->front().pred > budget) return false;
     int64_t bytes = 0;
-    for (auto it = S->queue.begin(); it != S->queue.end() && (int)batch.size() < S->cfg.max_batch;) {
-        if (klass(*it) != k0) {
-            ++it;
-            continue;
-        }
-        if (!batch.empty() && S->inflight_bytes + bytes + it->pred > budget) break;
-        bytes += it->pred;
-        batch.push_back(std::move(*it));
-        it = S->queue.erase(it);
+    while (!q->empty() && (int)batch.size() < S->cfg.max_batch) {
+        if (!batch.empty() && S->inflight_bytes + bytes + q->front().pred > budget) break;
+        bytes += q->front().pred;
+        batch.push_back(std::move(q->front()));
+        q->pop_front();
     }
+    S->queued -= batch.size();
     S->inflight_bytes += bytes;
     return true;
 }
+
+// Device memory of one worker: its share of the budget, split between the KSW2 traceback
+// arena (reserved when the worker starts) and the wavefront pools of the two WFA engines
+// (allocated when an engine first runs), so that the pooled allocations of all workers
+// stay inside the budget whatever mix of engines each worker sees.
+int64_t worker_share(const aw_server *S) { return S->cfg.hbm_budget / std::max(1, S->cfg.slots); }
+int64_t ksw_tb_share(const aw_server *S) { return worker_share(S) * 6 / 10; }
+int64_t wfa_pool_share(const aw_server *S) { return worker_share(S) * 2 / 10; }
 
 void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wavefront_aligner_gpu_t **al) {
     const aw_serve_config_t &C = S->cfg;
@@ -165,8 +173,17 @@ void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wav
         memset(ez.data(), 0, sizeof(ksw_extz_t) * n);
         int flag = generic ? AW_EZ_GENERIC_SC : 0;
         if (method == AW_ROUTE_KSW2_SINGLETRACK) flag |= AW_EZ_SINGLETRACK;
-        const int rc = aw_ksw_extd2_batch(n, ql.data(), qp.data(), tl.data(), tp.data(), w.data(), C.m, C.mat, C.q,
-                                          C.e, C.q2, C.e2, -1, 0, flag, ez.data());
+        int rc = aw_ksw_extd2_batch(n, ql.data(), qp.data(), tl.data(), tp.data(), w.data(), C.m, C.mat, C.q, C.e,
+                                    C.q2, C.e2, -1, 0, flag, ez.data());
+        if (rc == AW_E_CUDA || rc == AW_E_NOMEM) {
+            // device memory taken meanwhile (fragmentation, another process): give back the
+            // pooled buffers and run the batch once more
+            for (int i = 0; i < n; ++i) free(ez[i].cigar);
+            memset(ez.data(), 0, sizeof(ksw_extz_t) * n);
+            aw_release_thread_buffers();
+            rc = aw_ksw_extd2_batch(n, ql.data(), qp.data(), tl.data(), tp.data(), w.data(), C.m, C.mat, C.q, C.e,
+                                    C.q2, C.e2, -1, 0, flag, ez.data());
+        }
         for (int i = 0; i < n; ++i) {
             out[i].r.status = rc;
             out[i].r.ez = ez[i];
@@ -176,8 +193,8 @@ void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wav
         a.mismatch = C.wfa_x, a.gap_opening1 = C.wfa_o1, a.gap_extension1 = C.wfa_e1;
         a.gap_opening2 = C.wfa_o2, a.gap_extension2 = C.wfa_e2;
         a.singletrack = method == AW_ROUTE_WFA_SINGLETRACK;
-        // wavefront pool of this worker: its share of the device budget
-        a.max_memory_abort = std::max<int64_t>(S->cfg.hbm_budget / std::max(1, S->cfg.slots), (int64_t)1 << 26);
+        // wavefront pool of this engine in this worker: its part of the worker's share
+        a.max_memory_abort = std::max<int64_t>(wfa_pool_share(S), (int64_t)1 << 26);
         // one aligner per worker and engine, kept for the worker's lifetime
         wavefront_aligner_gpu_t *&A = al[a.singletrack ? 1 : 0];
         if (!A) A = wavefront_aligner_new_gpu(&a);
@@ -210,14 +227,16 @@ void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wav
 void worker_main(aw_server *S, int slot) {
     cudaSetDevice(S->device);
     // each worker's batches get an equal share of the device budget
-    set_thread_tb_budget(std::max<int64_t>(S->cfg.hbm_budget / std::max(1, S->cfg.slots), (int64_t)1 << 26));
+    const int64_t tb = std::max<int64_t>(ksw_tb_share(S), (int64_t)1 << 26);
+    set_thread_tb_budget(tb);
+    reserve_thread_tb(tb);
     std::vector<Req> batch;
     std::vector<Res> res;
     wavefront_aligner_gpu_t *al[2] = {nullptr, nullptr};
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] { return S->stopping || (!S->queue.empty() && take_batch(S, batch)); });
+            S->cv_work.wait(lk, [&] { return S->stopping || (S->queued > 0 && take_batch(S, batch)); });
             if (batch.empty() && S->stopping) {
                 lk.unlock();
                 wavefront_aligner_delete_gpu(al[0]);
@@ -270,7 +289,7 @@ aw_server_t *aw_serve_open(const aw_serve_config_t *cfg) {
     if (S->cfg.hbm_budget <= 0) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
-        S->cfg.hbm_budget = (int64_t)(fr * 0.5);
+        S->cfg.hbm_budget = (int64_t)(fr * 0.7);
     }
     for (int i = 0; i < cfg->slots; ++i) S->workers.emplace_back(worker_main, S, i);
     return S;
@@ -294,7 +313,9 @@ int aw_serve_submit(aw_server_t *S, uint64_t id, int method, int band, const cha
     {
         std::lock_guard<std::mutex> lk(S->mu);
         if (S->t_first_submit < 0) S->t_first_submit = r.t_submit;
-        S->queue.push_back(std::move(r));
+        const auto key = std::make_tuple(r.method, r.generic, r.bucket);
+        S->queues[key].push_back(std::move(r));
+        ++S->queued;
         ++S->submitted;
     }
     S->cv_work.notify_one();
@@ -324,7 +345,7 @@ int aw_serve_stats(aw_server_t *S, aw_serve_stats_t *st) {
     st->submitted = S->submitted;
     st->completed = S->completed;
     st->micro_batches = S->batches;
-    st->queued = (uint64_t)S->queue.size();
+    st->queued = (uint64_t)S->queued;
     st->inflight_bytes = S->inflight_bytes;
     std::vector<double> l = S->latencies;
     std::sort(l.begin(), l.end());

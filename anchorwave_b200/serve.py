@@ -10,6 +10,8 @@ import ctypes as C
 from dataclasses import dataclass, field
 from typing import List, Optional
 
+import numpy as np
+
 from ._lib import AwError, ServeConfig, ServeResult, ServeStats, last_error, lib
 
 ROUTE_KSW2 = 0
@@ -56,7 +58,10 @@ class AlignmentServer:
             item = ServedAlignment(int(r.id), int(r.method), int(r.status), float(r.latency_s))
             if r.method in (ROUTE_KSW2, ROUTE_KSW2_SINGLETRACK):
                 ez = r.ez
-                cig = tuple(ez.cigar[j] for j in range(ez.n_cigar)) if ez.n_cigar > 0 and ez.cigar else ()
+                # one copy of the CIGAR words (indexing a ctypes pointer word by word costs
+                # more than the alignment itself for long intervals)
+                cig = (tuple(np.frombuffer(C.string_at(ez.cigar, 4 * ez.n_cigar), dtype=np.uint32).tolist())
+                       if ez.n_cigar > 0 and ez.cigar else ())
                 item.ksw = (ez.max, ez.zdropped, ez.max_q, ez.max_t, ez.mqe, ez.mqe_t, ez.mte, ez.mte_q, ez.score,
                             ez.n_cigar, ez.reach_end, ez.stopped, cig)
             else:

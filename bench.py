@@ -262,7 +262,9 @@ def serving_measurement(nreq: int, rank: int):
     sat = len(reqs) / dt_sat
     dt, st = run(0.7 * sat)
     return {"requests": len(reqs), "cells": cells, "saturated_requests_per_s": sat,
-            "saturated_gcups": cells / dt_sat / 1e9, "offered_requests_per_s": 0.7 * sat,
+            "saturated_gcups": cells / dt_sat / 1e9,
+            "saturated_server_requests_per_s": len(reqs) / st_sat["elapsed_s"] if st_sat["elapsed_s"] else None,
+            "offered_requests_per_s": 0.7 * sat,
             "requests_per_s": len(reqs) / dt, "gcups": cells / dt / 1e9,
             "latency_ms_p50": 1e3 * st["latency_p50_s"], "latency_ms_p99": 1e3 * st["latency_p99_s"],
             "micro_batches": st["micro_batches"], "slots": 4, "max_batch": 512,

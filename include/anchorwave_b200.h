@@ -138,7 +138,8 @@ int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const cha
 typedef struct {
     int slots;            /* concurrent micro-batches (workers with their own streams) */
     int max_batch;        /* requests per micro-batch */
-    int64_t hbm_budget;   /* predicted device bytes admitted at once (0 = half of free) */
+    int64_t hbm_budget;   /* device bytes of the server: admission of predicted bytes, and the
+                             pooled buffers of its workers (0 = 70% of free memory) */
     int8_t m;             /* KSW2 scoring: alphabet size, m*m matrix, q, e, q2, e2 */
     int8_t mat[64];
     int8_t q, e, q2, e2;
