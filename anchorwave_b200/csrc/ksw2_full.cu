@@ -651,9 +651,17 @@ inline int prof_bytes(int warps) { return warps * PROF_WARP; }
 template <bool CIGAR, bool RIGHT, int W>
 cudaError_t launch_t(const KswFullArgs &a, int groups, int ctas, cudaStream_t st) {
     const int smem = prof_bytes(groups * W);
-    cudaError_t e = cudaFuncSetAttribute(ksw_full_kernel<CIGAR, RIGHT, W>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, prof_bytes(8));
-    if (e != cudaSuccess) return e;
+    // the dynamic shared memory limit is an attribute of the kernel on a device: set once
+    static std::atomic<uint32_t> set_on(0);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint32_t bit = 1u << (dev & 31);
+    if (!(set_on.load() & bit)) {
+        cudaError_t e = cudaFuncSetAttribute(ksw_full_kernel<CIGAR, RIGHT, W>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, prof_bytes(8));
+        if (e != cudaSuccess) return e;
+        set_on.fetch_or(bit);
+    }
     ksw_full_kernel<CIGAR, RIGHT, W><<<ctas, groups * W * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
