@@ -25,7 +25,7 @@ class KswExtz(C.Structure):
 EXPORTS = [
     "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "aw_ksw_extd2_batch",
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
-    "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_free",
+    "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_graph", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_release_thread_buffers",
     "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc",
@@ -105,6 +105,8 @@ def _load(path: str = LIB_PATH):
     lib.aw_last_error.restype = C.c_char_p
     lib.aw_device_count.argtypes = []
     lib.aw_device_count.restype = i32
+    lib.aw_ksw_plan_graph.argtypes = [vp]
+    lib.aw_ksw_plan_graph.restype = i32
     lib.aw_int32_peak_ops.argtypes = []
     lib.aw_int32_peak_ops.restype = C.c_double
     lib.aw_int16x2_peak_ops.argtypes = []

@@ -44,6 +44,13 @@ static void set_error(const std::string &s) { set_error(s.c_str()); }
 // probe (alignSlidingWindow.cpp:593-640).
 static thread_local bool tls_has_deadline = false;
 static thread_local std::chrono::steady_clock::time_point tls_deadline;
+
+// Set while this thread captures a plan into a CUDA graph: the timing events then become
+// event-record nodes of the graph, so they still time every replay.
+static thread_local bool tls_capturing = false;
+static cudaError_t record_timing(cudaEvent_t e, cudaStream_t st) {
+    return tls_capturing ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
+}
 #define AW_CUDA(call)                                                                   \
     do {                                                                                \
         cudaError_t _e = (call);                                                        \
@@ -316,6 +323,20 @@ struct aw_ksw_plan {
     int launches = 0;
     bool uploaded = false, executed = false;
     float dp_ms = 0.f, bt_ms = 0.f;
+    // re-execution through a CUDA graph (aw_ksw_plan_execute): the first execute runs
+    // eagerly (lazy set-up of the kernels), the second captures the launch sequence, later
+    // ones replay it
+    int eager_runs = 0;
+    bool graph_off = false, graph_used = false;
+    int graph_warps = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    void drop_graph() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        gexec = nullptr, graph = nullptr;
+    }
+    ~aw_ksw_plan() { drop_graph(); }
 };
 
 // Columns per lane of the banded kernel for this plan: 4 halves the pipeline lag between
@@ -538,7 +559,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
     AW_CUDA(cudaMemsetAsync(B->queue.p, 0, sizeof(int32_t) * nq, B->st));
     AW_CUDA(cudaMemsetAsync(B->error.p, 0, sizeof(int32_t) * 4, B->st));
     AW_CUDA(cudaMemsetAsync(B->out.p, 0, sizeof(KswOut) * (size_t)std::max(pl->n, 1), B->st));
-    AW_CUDA(cudaEventRecord(B->ev_t0, B->st));
+    AW_CUDA(record_timing(B->ev_t0, B->st));
     // the deadline word: globaltimer at the start of this work + the time left
     const unsigned long long *deadline = nullptr;
     if (tls_has_deadline) {
@@ -572,7 +593,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         a.error = B->error.as<int32_t>();
         a.sc = pl->S;
         a.deadline = deadline;
-        AW_CUDA(cudaEventRecord(B->ev_k[3 * k], B->st));
+        AW_CUDA(record_timing(B->ev_k[3 * k], B->st));
         // fork: large pairs on st2 (groups of large_warps warps), small on st (single warps)
         AW_CUDA(cudaEventRecord(B->ev_a, B->st));
         AW_CUDA(cudaStreamWaitEvent(B->st2, B->ev_a, 0));
@@ -605,14 +626,14 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         }
         AW_CUDA(cudaEventRecord(B->ev_b, B->st2));
         AW_CUDA(cudaStreamWaitEvent(B->st, B->ev_b, 0));
-        AW_CUDA(cudaEventRecord(B->ev_k[3 * k + 1], B->st));
+        AW_CUDA(record_timing(B->ev_k[3 * k + 1], B->st));
         if (!(P.flag & AW_EZ_SCORE_ONLY) && W.n_large + W.n_small > 0) {
             AW_CUDA(launch_ksw_backtrack_full(B->pairs.as<KswPair>(), B->order.as<int32_t>() + W.begin_large,
                                               W.n_large + W.n_small, B->tb.as<uint8_t>(), B->out.as<KswOut>(),
                                               B->cig.as<uint32_t>(), P.flag, B->st));
             ++launches;
         }
-        AW_CUDA(cudaEventRecord(B->ev_k[3 * k + 2], B->st));
+        AW_CUDA(record_timing(B->ev_k[3 * k + 2], B->st));
     }
     const int nbw = pl->band_ids.empty() ? 0 : (int)pl->band.waves.size();
     if (nbw > 0) {
@@ -626,10 +647,10 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         const int ctas = band_occupancy(P.flag) * B->sms;
         for (int k = 0; k < nbw; ++k) {
             cudaEvent_t *ev = &B->ev_k[3 * (nw + k)];
-            AW_CUDA(cudaEventRecord(ev[0], B->st));
+            AW_CUDA(record_timing(ev[0], B->st));
             AW_CUDA(band_launch_dp(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S, P.flag,
                                    ctas, B->st));
-            AW_CUDA(cudaEventRecord(ev[1], B->st));
+            AW_CUDA(record_timing(ev[1], B->st));
             AW_CUDA(band_launch_finish(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S,
                                        P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), P.mat, P.m, B->st));
             launches += 2;
@@ -642,7 +663,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
                 for (int gi = BW.group0; gi < BW.group0 + BW.ngroup; ++gi) lasts += pl->band.groups[gi].last;
                 launches += 3 * BW.ngroup + lasts;  // counters, strips, walk per group; tail per pair
             }
-            AW_CUDA(cudaEventRecord(ev[2], B->st));
+            AW_CUDA(record_timing(ev[2], B->st));
         }
     }
     if (!pl->exact_ids.empty()) {
@@ -653,7 +674,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
                                B->st, &launches, deadline);
         if (rc) return rc;
     }
-    AW_CUDA(cudaEventRecord(B->ev_t1, B->st));
+    AW_CUDA(record_timing(B->ev_t1, B->st));
     pl->launches = launches;
     return AW_OK;
 }
@@ -793,10 +814,53 @@ int aw_ksw_plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uin
     return plan_upload(pl, query, target);
 }
 
+// Plans above this many DP cells (about 20 ms of device work) always launch eagerly.
+static constexpr int64_t kGraphMaxCells = 20000000000LL;
+
 int aw_ksw_plan_execute(aw_ksw_plan_t *pl, float *ms) {
     if (!pl) return AW_E_INVAL;
-    return plan_execute(pl, ms);
+    pl->graph_used = false;
+    // graphs for the strip and banded kernels of plans small enough that launch overhead
+    // matters (on the 4,096-pair bench plan, 1.7e11 cells, replaying the graph measured 5-8%
+    // slower than launching eagerly); the anti-diagonal kernel synchronises on the host
+    // between workspace groups, and a deadline is re-armed per call
+    if (pl->graph_off || !pl->uploaded || !pl->exact_ids.empty() || tls_has_deadline ||
+        pl->cells > kGraphMaxCells)
+        return plan_execute(pl, ms);
+    int lw;
+    {
+        std::lock_guard<std::mutex> lk(g_cfg_mu);
+        lw = g_large_warps;
+    }
+    if (pl->gexec && pl->graph_warps != lw) pl->drop_graph();  // tuning changed: capture again
+    if (!pl->gexec) {
+        if (pl->eager_runs < 1) {
+            ++pl->eager_runs;
+            return plan_execute(pl, ms);
+        }
+        Buffers *B = pl->B;
+        AW_CUDA(cudaStreamBeginCapture(B->st, cudaStreamCaptureModeThreadLocal));
+        tls_capturing = true;
+        const int rc = plan_launch(pl);
+        tls_capturing = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(B->st, &g);
+        cudaGraphExec_t ge = nullptr;
+        if (rc || ec != cudaSuccess || !g || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
+            // a step of this plan cannot be captured here: keep running it eagerly
+            cudaGetLastError();
+            if (g) cudaGraphDestroy(g);
+            pl->graph_off = true;
+            return plan_execute(pl, ms);
+        }
+        pl->graph = g, pl->gexec = ge, pl->graph_warps = lw;
+    }
+    AW_CUDA(cudaGraphLaunch(pl->gexec, pl->B->st));
+    pl->graph_used = true;
+    return plan_finish(pl, ms);
 }
+
+int aw_ksw_plan_graph(const aw_ksw_plan_t *pl) { return pl && pl->graph_used ? 1 : 0; }
 
 int aw_ksw_plan_download(aw_ksw_plan_t *pl, ksw_extz_t *ez) {
     if (!pl || !ez) return AW_E_INVAL;

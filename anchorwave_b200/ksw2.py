@@ -193,6 +193,10 @@ class KswPlan:
         check(lib.aw_ksw_plan_execute(self.h, C.byref(ms)), "aw_ksw_plan_execute")
         return ms.value
 
+    def uses_graph(self) -> bool:
+        """True when the last execute replayed the plan's CUDA graph."""
+        return bool(lib.aw_ksw_plan_graph(self.h))
+
     def timing(self):
         """(dp_ms, backtrack_ms) of the last execute, CUDA events on the plan's stream."""
         dp, bt = C.c_float(0.0), C.c_float(0.0)

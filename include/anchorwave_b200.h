@@ -85,6 +85,14 @@ int aw_ksw_plan_upload(aw_ksw_plan_t *plan, const uint8_t *const *query,
 /* Runs every wave of the plan on its stream; ms (optional) receives the CUDA-event
  * time of the device work between the first and the last launch. */
 int aw_ksw_plan_execute(aw_ksw_plan_t *plan, float *ms);
+/* 1 when the last aw_ksw_plan_execute replayed the plan as a CUDA graph.  For plans of
+ * up to 2e10 DP cells (where launch overhead is a visible part of an execute) the first
+ * execute runs eagerly, the second captures the launch sequence into a graph, later ones
+ * replay it (one launch call per execute).  Larger plans, plans with pairs on the
+ * anti-diagonal kernel (z-drop, approximate max, extension-only, positive match scores)
+ * and executes under a deadline (aw_ksw_set_deadline) always launch eagerly.  No
+ * counterpart in the reference (its calls are one-shot). */
+int aw_ksw_plan_graph(const aw_ksw_plan_t *plan);
 int aw_ksw_plan_download(aw_ksw_plan_t *plan, ksw_extz_t *ez);
 /* Device-side statistics of the plan: cells, traceback bytes, waves, launches. */
 int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_bytes, int *waves,
