@@ -76,28 +76,20 @@ __device__ __forceinline__ void cell(int s, int &xs, int &vs, int &x2s, int &ut,
                                      const KswScore &S) {
     const int a = xs + vs, b = yt + ut, a2 = x2s + vs, b2 = y2t + ut;
     int z = s;
-    bool p;
     if (!ARGMAX) {
         z = __vimax3_s32(z, a, b);
         z = __vimax3_s32(z, a2, b2);
-    } else if (!RIGHT) {
-        z = __vibmax_s32(z, a, &p);
-        d = p ? 0 : 1;
-        z = __vibmax_s32(z, b, &p);
-        d = p ? d : 2;
-        z = __vibmax_s32(z, a2, &p);
-        d = p ? d : 3;
-        z = __vibmax_s32(z, b2, &p);
-        d = p ? d : 4;
     } else {
-        z = __vibmax_s32(a, z, &p);
-        d = p ? 1 : 0;
-        z = __vibmax_s32(b, z, &p);
-        d = p ? 2 : d;
-        z = __vibmax_s32(a2, z, &p);
-        d = p ? 3 : d;
-        z = __vibmax_s32(b2, z, &p);
-        d = p ? 4 : d;
+        // arg-max by priority tags in the low 4 bits of 16 * candidate: the larger tag wins a
+        // tie of values, so the max gives z and the state code at once.  Left-aligned: the
+        // first candidate wins a tie (ksw2_extd2_sse.c:244-251), tags s=7 > a=6 > ... > b2=3,
+        // code = tag ^ 7; right-aligned: the last (:291-298), tags = codes 0..4.
+        constexpr int Ts = RIGHT ? 0 : 7, Ta = RIGHT ? 1 : 6, Tb = RIGHT ? 2 : 5, Ta2 = RIGHT ? 3 : 4,
+                      Tb2 = RIGHT ? 4 : 3;
+        int zt = __vimax3_s32(s * 16 + Ts, b * 16 + Tb, b2 * 16 + Tb2);
+        zt = __vimax3_s32(zt, a * 16 + Ta, a2 * 16 + Ta2);
+        d = RIGHT ? (zt & 15) : ((zt & 15) ^ 7);
+        z = zt >> 4;
     }
     z = min(z, S.mch);
     const int un = z - vs, vn = z - ut;
