@@ -151,16 +151,18 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     const int scope = std::max(A.gap_opening1 + A.gap_extension1, A.gap_opening2 + A.gap_extension2);
     W.max_score_scope = std::max(scope, A.mismatch) + 1;
     const int occ = std::max(1, wfa_occupancy());
-    // Rounds: every round restarts the pool; pairs that found it exhausted run again.
-    // If a round completes nothing, the remaining pairs run one at a time, and a pair
-    // that cannot finish with the whole pool to itself reports WF_STATUS_OOM (the
-    // reference's max-memory abort).
+    // Rounds: every round restarts the pool and runs up to `chunk` pending pairs, largest
+    // first; pairs that found the pool exhausted stay pending.  A round that completes
+    // nothing halves the chunk (the pairs in flight together share the pool), one that
+    // completes all of its pairs doubles it again; a pair that cannot finish with the whole
+    // pool to itself reports WF_STATUS_OOM (the reference's max-memory abort).
     std::vector<int32_t> pending = order;
+    size_t chunk = pending.size();
     float total_ms = 0.f;
     int launches = 0;
-    bool serial = false;
     while (!pending.empty()) {
-        std::vector<int32_t> batch = serial ? std::vector<int32_t>{pending[0]} : pending;
+        const size_t take = std::min(chunk, pending.size());
+        std::vector<int32_t> batch(pending.begin(), pending.begin() + (std::ptrdiff_t)take);
         WCUDA(cudaMemcpyAsync(al->d_order.p, batch.data(), sizeof(int32_t) * batch.size(), cudaMemcpyHostToDevice,
                               al->st));
         WCUDA(cudaMemsetAsync(al->d_queue.p, 0, 4, al->st));
@@ -184,14 +186,18 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
         if (getenv("AW_VERBOSE"))
             fprintf(stderr, "[aw_b200] WFA round %d: %zu pairs, %zu to retry, %.1f ms\n", launches, batch.size(),
                     again.size(), ms);
-        if (serial) {
-            if (!again.empty()) al->outs[pending[0]].status = WFA_OOM;
-            pending.erase(pending.begin());
-        } else if (again.size() == batch.size()) {
-            serial = true;
-        } else {
-            pending.swap(again);
+        const size_t done = batch.size() - again.size();
+        if (done == 0 && take == 1) {
+            al->outs[batch[0]].status = WFA_OOM;
+            again.clear();
+        } else if (done == 0) {
+            chunk = std::max<size_t>(1, take / 2);
+        } else if (again.empty() && take == chunk) {
+            chunk *= 2;
         }
+        // the retried pairs first (still largest first), then those not yet run
+        again.insert(again.end(), pending.begin() + (std::ptrdiff_t)take, pending.end());
+        pending.swap(again);
     }
     al->last_ms = total_ms;
     al->last_launches = launches;

@@ -73,7 +73,7 @@ def test_wfa_batched_workload_subset_vs_reference(gpu):
 
 
 def test_wfa_pool_retry_rounds(gpu, restatement):
-    """A tiny pool forces retry rounds and the one-at-a-time fallback; results unchanged."""
+    """A tiny pool forces retry rounds down to one pair at a time; results unchanged."""
     wfa = _wfa()
     rng = np.random.default_rng(99)
     ps, ts = [], []
@@ -86,6 +86,31 @@ def test_wfa_pool_retry_rounds(gpu, restatement):
     for p, t, r in zip(ps, ts, res):
         exp = restatement.wfa_align(p, t, 4, 4, 2, 24, 1, False)
         assert r == exp or r[0] == -200
+
+
+def test_wfa_pool_pressure_keeps_batches(gpu):
+    """Many long pairs sharing a pool too small for all of them at once: the rounds halve
+    the pairs in flight instead of running them one by one, so the batch ends quickly with
+    the results of a run that had the pool to spare."""
+    import time
+    wfa = _wfa()
+    rng = np.random.default_rng(7)
+    ps, ts = [], []
+    for _ in range(256):
+        q, t = W.divergent_pair(rng, 3000, 0.02, 0.03, 4.0)
+        ps.append(W.to_ascii(t))
+        ts.append(W.to_ascii(q))
+    big = wfa.WfaAligner(4, 4, 2, 24, 1, max_memory_abort=8 << 30)
+    exp, _ = big.align_batch(ps, ts)
+    big.close()
+    small = wfa.WfaAligner(4, 4, 2, 24, 1, max_memory_abort=256 << 20)
+    t0 = time.perf_counter()
+    res, _ = small.align_batch(ps, ts)
+    secs = time.perf_counter() - t0
+    small.close()
+    assert res == exp
+    assert all(r[0] == 0 for r in res)
+    assert secs < 20.0, secs
 
 
 def test_align_with_wfa_mirror(gpu, restatement):
