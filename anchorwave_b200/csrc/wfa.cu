@@ -3,9 +3,11 @@
 //
 // One warp per pair; the lanes cover the diagonals of a wavefront.  Per score s:
 //   * extend M[s] (wavefront/wavefront_extend.c:86-121): each lane advances its
-//     diagonal by comparing 8 bytes of pattern and text at a time (one XOR and
-//     __ffsll per 8 bases); sentinels after each sequence ('!' pattern, '?' text,
-//     wavefront/wavefront_sequences.c:37-39) stop the run;
+//     diagonal by comparing 32 bases of pattern and text at a time in 2-bit copies of
+//     the sequences (one XOR and __ffsll per 32 bases; the run also ends at the end of
+//     either sequence); pairs with any byte other than A, C, G, T (the reference compares
+//     raw characters) compare 8 bytes at a time instead, where the sentinels after each
+//     sequence ('!' pattern, '?' text, wavefront/wavefront_sequences.c:37-39) stop the run;
 //   * end-to-end check on diagonal tlen-plen (wavefront/wavefront_termination.c:37-60);
 //   * compute s+1 from M[s-x], M[s-o1-e1], I1/D1[s-e1], M[s-o2-e2], I2/D2[s-e2]
 //     (wavefront/wavefront_compute_affine2p.c:45-106) over the limits of
@@ -106,6 +108,16 @@ __device__ __forceinline__ uint64_t load8(const uint8_t *base, int64_t pos) {
     return (lo >> sh) | (p[1] << (64 - sh));
 }
 
+// 32 bases from base g of a 2-bit arena (base i at bits 2*(i%32) of word i/32); the arena
+// ends with a spare word.
+__device__ __forceinline__ uint64_t load32b(const uint64_t *p, int64_t g) {
+    const int64_t w = g >> 5;
+    const int sh = (int)(g & 31) * 2;
+    const uint64_t lo = __ldg(p + w);
+    if (!sh) return lo;
+    return (lo >> sh) | (__ldg(p + w + 1) << (64 - sh));
+}
+
 __device__ __forceinline__ bool in_matrix(int32_t o, int k, int plen, int tlen) {
     return (uint32_t)o <= (uint32_t)tlen && (uint32_t)(o - k) <= (uint32_t)plen;
 }
@@ -196,6 +208,34 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                             v[u] = (int64_t)o[u] - k, h[u] = o[u];
                         }
                         bool any = run[0] || run[1] || run[2] || run[3];
+                        if (PR.packed) {
+                            // 32 bases per XOR; the run ends at the first differing base or
+                            // at the end of either sequence (the sentinels of the byte path)
+                            int64_t rem[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                rem[u] = run[u] ? min((int64_t)plen - v[u], (int64_t)tlen - h[u]) : 0;
+                                if (rem[u] <= 0) run[u] = false;
+                            }
+                            any = run[0] || run[1] || run[2] || run[3];
+                            while (any) {
+                                uint64_t x[4];
+#pragma unroll
+                                for (int u = 0; u < 4; ++u)
+                                    x[u] = run[u] ? (load32b(A.ppat, PR.poff + v[u]) ^ load32b(A.ptxt, PR.toff + h[u])) : 0;
+                                any = false;
+#pragma unroll
+                                for (int u = 0; u < 4; ++u) {
+                                    if (!run[u]) continue;
+                                    int64_t nb = x[u] ? (int64_t)((__ffsll((long long)x[u]) - 1) >> 1) : 32;
+                                    const bool stop = x[u] != 0 || nb >= rem[u];
+                                    if (nb > rem[u]) nb = rem[u];
+                                    v[u] += nb, h[u] += nb, rem[u] -= nb;
+                                    if (stop || rem[u] == 0) run[u] = false;
+                                    else any = true;
+                                }
+                            }
+                        }
                         while (any) {
                             uint64_t x[4];
 #pragma unroll
@@ -526,6 +566,59 @@ cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st) {
         if (e != cudaSuccess) return e;
     }
     wfa_kernel<<<ctas, 128, smem, st>>>(a, rs);
+    return cudaGetLastError();
+}
+
+namespace {
+
+__device__ __forceinline__ uint64_t code2(uint8_t c) {
+    return c == 'C' ? 1u : c == 'G' ? 2u : c == 'T' ? 3u : 0u;
+}
+
+// One thread per word of 32 bases.
+__global__ void wfa_pack_kernel(const uint8_t *src, int64_t nbytes, uint64_t *dst, int64_t nwords) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nwords) return;
+    uint64_t r = 0;
+    const int64_t b0 = w * 32;
+    if (b0 + 32 <= nbytes) {
+        const uint4 a = *reinterpret_cast<const uint4 *>(src + b0), b = *reinterpret_cast<const uint4 *>(src + b0 + 16);
+        const uint32_t wd[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 32; ++i) r |= code2((uint8_t)(wd[i >> 2] >> (8 * (i & 3)))) << (2 * i);
+    } else {
+        for (int i = 0; i < 32 && b0 + i < nbytes; ++i) r |= code2(src[b0 + i]) << (2 * i);
+    }
+    dst[w] = r;
+}
+
+// One warp per pair: packed = no byte other than A, C, G, T in the pattern and the text.
+__global__ void wfa_classify_kernel(const uint8_t *pat, const uint8_t *txt, WfaPairDev *pairs, int n) {
+    const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const WfaPairDev P = pairs[i];
+    bool bad = false;
+    for (int j = lane; j < P.plen && !bad; j += 32) {
+        const uint8_t c = pat[P.poff + j];
+        bad = !(c == 'A' || c == 'C' || c == 'G' || c == 'T');
+    }
+    for (int j = lane; j < P.tlen && !bad; j += 32) {
+        const uint8_t c = txt[P.toff + j];
+        bad = !(c == 'A' || c == 'C' || c == 'G' || c == 'T');
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) pairs[i].packed = bad ? 0 : 1;
+}
+
+}  // namespace
+
+cudaError_t launch_wfa_pack(const uint8_t *pat, int64_t pbytes, uint64_t *ppat, const uint8_t *txt, int64_t tbytes,
+                            uint64_t *ptxt, WfaPairDev *pairs, int n, cudaStream_t st) {
+    const int64_t pw = (pbytes + 31) / 32 + 2, tw = (tbytes + 31) / 32 + 2;
+    wfa_pack_kernel<<<(unsigned)((pw + 255) / 256), 256, 0, st>>>(pat, pbytes, ppat, pw);
+    wfa_pack_kernel<<<(unsigned)((tw + 255) / 256), 256, 0, st>>>(txt, tbytes, ptxt, tw);
+    if (n > 0) wfa_classify_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(pat, txt, pairs, n);
     return cudaGetLastError();
 }
 

@@ -48,6 +48,7 @@ struct wavefront_aligner_gpu {
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     DevBuf d_pat, d_txt, d_pairs, d_order, d_pool, d_head, d_ctab, d_ops, d_out, d_queue;
+    DevBuf d_ppat, d_ptxt;  // 2-bit copies of the sequence arenas
     PinBuf h_pat, h_txt, h_ops;
     std::vector<WfaPairDev> pairs;
     std::vector<WfaOutDev> outs;
@@ -61,6 +62,7 @@ struct wavefront_aligner_gpu {
     ~wavefront_aligner_gpu() {
         d_pat.release(), d_txt.release(), d_pairs.release(), d_order.release(), d_pool.release();
         d_head.release(), d_ctab.release(), d_ops.release(), d_out.release(), d_queue.release();
+        d_ppat.release(), d_ptxt.release();
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
         if (st) cudaStreamDestroy(st);
@@ -117,6 +119,8 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     });
     WCUDA(al->d_pat.ensure((size_t)pb + 64));
     WCUDA(al->d_txt.ensure((size_t)tb + 64));
+    WCUDA(al->d_ppat.ensure(8 * (size_t)((pb + 31) / 32 + 2)));
+    WCUDA(al->d_ptxt.ensure(8 * (size_t)((tb + 31) / 32 + 2)));
     WCUDA(al->d_pairs.ensure(sizeof(WfaPairDev) * (size_t)n));
     WCUDA(al->d_order.ensure(sizeof(int32_t) * (size_t)n));
     WCUDA(al->d_ctab.ensure(8 * (size_t)cb + 64));
@@ -137,8 +141,12 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     WCUDA(cudaMemcpyAsync(al->d_txt.p, ht, (size_t)tb, cudaMemcpyHostToDevice, al->st));
     WCUDA(cudaMemcpyAsync(al->d_pairs.p, al->pairs.data(), sizeof(WfaPairDev) * (size_t)n, cudaMemcpyHostToDevice,
                           al->st));
+    // 2-bit arenas for the extend step, and which pairs may use them
+    WCUDA(launch_wfa_pack(al->d_pat.as<uint8_t>(), pb, al->d_ppat.as<uint64_t>(), al->d_txt.as<uint8_t>(), tb,
+                          al->d_ptxt.as<uint64_t>(), al->d_pairs.as<WfaPairDev>(), n, al->st));
     WfaArgs W;
     W.pat = al->d_pat.as<uint8_t>(), W.txt = al->d_txt.as<uint8_t>();
+    W.ppat = al->d_ppat.as<uint64_t>(), W.ptxt = al->d_ptxt.as<uint64_t>();
     W.pairs = al->d_pairs.as<WfaPairDev>();
     W.pool = al->d_pool.as<uint8_t>(), W.pool_bytes = (int64_t)al->d_pool.cap;
     W.pool_head = al->d_head.as<unsigned long long>();

@@ -21,7 +21,8 @@ struct WfaPairDev {
     int32_t plen, tlen;
     int64_t ops_off;       // CIGAR operation slot (plen + tlen + 8 chars)
     int64_t ctab_off;      // header-chunk table (int64 pool offsets), ctab_cap entries
-    int32_t ctab_cap, pad;
+    int32_t ctab_cap;
+    int32_t packed;        // 1: pattern and text are uppercase ACGT only (set on the device)
 };
 
 struct WfaOutDev {
@@ -31,6 +32,7 @@ struct WfaOutDev {
 
 struct WfaArgs {
     const uint8_t *pat, *txt;
+    const uint64_t *ppat, *ptxt;  // the same arenas at 2 bits per base (32 bases per word)
     const WfaPairDev *pairs;
     const int32_t *order;
     int32_t n;
@@ -47,6 +49,10 @@ struct WfaArgs {
 };
 
 cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st);
+// 2-bit copies of the pattern and text arenas (A=0, C=1, G=2, T=3, any other byte 0), and
+// the per-pair flag that the pair's sequences are uppercase ACGT only.
+cudaError_t launch_wfa_pack(const uint8_t *pat, int64_t pbytes, uint64_t *ppat, const uint8_t *txt, int64_t tbytes,
+                            uint64_t *ptxt, WfaPairDev *pairs, int n, cudaStream_t st);
 int wfa_occupancy();
 
 }  // namespace aw

@@ -88,6 +88,31 @@ def test_wfa_pool_retry_rounds(gpu, restatement):
         assert r == exp or r[0] == -200
 
 
+def test_wfa_non_acgt_pairs(gpu, restatement):
+    """Pairs with N or lowercase bases (the reference compares raw characters, so 'a' and
+    'A' differ) extend byte by byte; pure uppercase ACGT pairs use the 2-bit arenas; one
+    batch mixes both, and both match the oracle."""
+    wfa = _wfa()
+    rng = np.random.default_rng(17)
+    ps, ts = [], []
+    for i in range(48):
+        q, t = W.divergent_pair(rng, int(rng.integers(20, 3000)), 0.0, 0.05, 4.0)
+        p_, t_ = bytearray(W.to_ascii(t)), bytearray(W.to_ascii(q))
+        if i % 3 == 1:
+            for j in rng.integers(0, len(p_), 3):
+                p_[j] = ord("N")
+        elif i % 3 == 2:
+            for j in rng.integers(0, len(t_), 5):
+                t_[j] = t_[j] + 32  # lowercase
+        ps.append(bytes(p_))
+        ts.append(bytes(t_))
+    al = wfa.WfaAligner(4, 4, 2, 24, 1)
+    res, _ = al.align_batch(ps, ts)
+    al.close()
+    for p, t, r in zip(ps, ts, res):
+        assert r == restatement.wfa_align(p, t, 4, 4, 2, 24, 1, False), (len(p), len(t))
+
+
 def test_wfa_pool_pressure_keeps_batches(gpu):
     """Many long pairs sharing a pool too small for all of them at once: the rounds halve
     the pairs in flight instead of running them one by one, so the batch ends quickly with
