@@ -28,7 +28,7 @@ EXPORTS = [
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_graph", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_release_thread_buffers",
     "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
-    "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc",
+    "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc", "aw_cigar_rows_batch",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
     "wavefront_align_batch_gpu", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
     "aw_serve_result_free", "aw_serve_close",
@@ -107,6 +107,8 @@ def _load(path: str = LIB_PATH):
     lib.aw_device_count.restype = i32
     lib.aw_ksw_plan_graph.argtypes = [vp]
     lib.aw_ksw_plan_graph.restype = i32
+    lib.aw_cigar_rows_batch.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64]
+    lib.aw_cigar_rows_batch.restype = i32
     lib.aw_int32_peak_ops.argtypes = []
     lib.aw_int32_peak_ops.restype = C.c_double
     lib.aw_int16x2_peak_ops.argtypes = []

@@ -703,3 +703,30 @@ def align_sliding_window(dna_q: str, dna_d: str, sliding_window_size: int, match
     """alignSlidingWindow (alignSlidingWindow.cpp:457-590) for one interval."""
     return align_sliding_window_batch([(dna_q, dna_d)], sliding_window_size, matching_score, mismatching_penalty,
                                       open1, extend1, open2, extend2)[0]
+
+
+def cigar_rows_batch(cigars, queries, targets) -> List[Tuple[str, str]]:
+    """aw_cigar_rows_batch: the gapped rows (aligned query, aligned reference) of many CIGARs,
+    decoded on the device (alignSlidingWindow.cpp:307-324).  queries / targets: str or bytes."""
+    n = len(cigars)
+    if n == 0:
+        return []
+    cw = [np.ascontiguousarray(np.asarray(c, dtype=np.uint32)) for c in cigars]
+    qb = [q.encode() if isinstance(q, str) else bytes(q) for q in queries]
+    tb = [t.encode() if isinstance(t, str) else bytes(t) for t in targets]
+    qbufs = [C.create_string_buffer(b, len(b) + 1) for b in qb]
+    tbufs = [C.create_string_buffer(b, len(b) + 1) for b in tb]
+    cp = (C.c_void_p * n)(*[c.ctypes.data for c in cw])
+    qp = (C.c_void_p * n)(*[C.addressof(b) for b in qbufs])
+    tp = (C.c_void_p * n)(*[C.addressof(b) for b in tbufs])
+    nc = np.array([len(c) for c in cw], dtype=np.int32)
+    ql = np.array([len(b) for b in qb], dtype=np.int32)
+    tl = np.array([len(b) for b in tb], dtype=np.int32)
+    cap = int(ql.sum() + tl.sum()) + 1
+    rq, rd = C.create_string_buffer(cap), C.create_string_buffer(cap)
+    off = np.zeros(n, dtype=np.int64)
+    ln = np.zeros(n, dtype=np.int32)
+    check(lib.aw_cigar_rows_batch(n, cp, nc.ctypes.data, qp, ql.ctypes.data, tp, tl.ctypes.data, rq, rd,
+                                  off.ctypes.data, ln.ctypes.data, cap), "aw_cigar_rows_batch")
+    bq, bd = rq.raw, rd.raw
+    return [(bq[o:o + l].decode(), bd[o:o + l].decode()) for o, l in zip(off.tolist(), ln.tolist())]

@@ -102,6 +102,18 @@ int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_byt
 int aw_ksw_plan_timing(const aw_ksw_plan_t *plan, float *dp_ms, float *bt_ms);
 void aw_ksw_plan_free(aw_ksw_plan_t *plan);
 
+/* Gapped alignment rows from KSW2 CIGARs, decoded on the device: the rows AnchorWave's
+ * callers build on the host before the MAF writer (src/myImportandFunction/
+ * alignSlidingWindow.cpp:307-324).  Pair i: CIGAR cigar[i][0..n_cigar[i]) over query[i]
+ * (qlen[i] characters) and target[i] (tlen[i]); row_q / row_d receive the aligned query and
+ * reference back to back, pair i at row_off[i] with row_len[i] characters (capacity: room
+ * in each row buffer).  M, = and X copy both sequences, I copies the query against '-', D
+ * puts '-' against the reference.  Returns 0, or AW_E_INVAL for another operation, a CIGAR
+ * that runs past the end of a sequence, or rows beyond the capacity. */
+int aw_cigar_rows_batch(int n, const uint32_t *const *cigar, const int *n_cigar, const char *const *query,
+                        const int *qlen, const char *const *target, const int *tlen, char *row_q, char *row_d,
+                        int64_t *row_off, int *row_len, int64_t capacity);
+
 /* ---- WFA (gap-affine-2p, end to end) ------------------------------------------ */
 
 /* Attributes of WfaAlignment.cpp:143-170: match 0, these penalties (positive), high
