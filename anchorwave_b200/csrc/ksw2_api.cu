@@ -26,6 +26,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace aw {
@@ -519,9 +520,32 @@ static int plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uin
     const int n = pl->n;
     AW_CUDA(B->h_codes.ensure((size_t)(pl->qbytes + pl->tbytes) + 32));
     uint8_t *hq = B->h_codes.as<uint8_t>(), *ht = hq + pl->qbytes + 16;
-    for (int i = 0; i < n; ++i) {
-        if (pl->qlen[i] > 0) memcpy(hq + pl->qoff[i], query[i], (size_t)pl->qlen[i]);
-        if (pl->tlen[i] > 0) memcpy(ht + pl->toff[i], target[i], (size_t)pl->tlen[i]);
+    auto stage = [&](int lo, int hi) {
+        for (int i = lo; i < hi; ++i) {
+            if (pl->qlen[i] > 0) memcpy(hq + pl->qoff[i], query[i], (size_t)pl->qlen[i]);
+            if (pl->tlen[i] > 0) memcpy(ht + pl->toff[i], target[i], (size_t)pl->tlen[i]);
+        }
+    };
+    // large batches: the staging copy (pageable -> pinned) is split over a few host threads
+    const int64_t bytes = pl->qbytes + pl->tbytes;
+    const int nt = bytes < ((int64_t)8 << 20) ? 1
+                   : (int)std::min<int64_t>({8, (int64_t)std::max(1u, std::thread::hardware_concurrency()), bytes >> 22});
+    if (nt <= 1) {
+        stage(0, n);
+    } else {
+        // pairs split by bytes, so every thread copies about the same amount
+        std::vector<int> cut(nt + 1, n);
+        cut[0] = 0;
+        int64_t acc = 0;
+        int t = 1;
+        for (int i = 0; i < n && t < nt; ++i) {
+            acc += std::max(pl->qlen[i], 0) + std::max(pl->tlen[i], 0);
+            if (acc >= bytes * t / nt) cut[t++] = i + 1;
+        }
+        std::vector<std::thread> th;
+        for (int k = 1; k < nt; ++k) th.emplace_back(stage, cut[k], cut[k + 1]);
+        stage(cut[0], cut[1]);
+        for (auto &x : th) x.join();
     }
     memcpy(B->h_pairs.p, pl->pairs.data(), sizeof(KswPair) * (size_t)n);
     int32_t *ho = B->h_order.as<int32_t>();
