@@ -30,7 +30,7 @@ EXPORTS = [
     "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc", "aw_cigar_rows_batch",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
-    "wavefront_align_batch_gpu", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
+    "wavefront_align_batch_gpu", "wavefront_gpu_memory", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
     "aw_serve_result_free", "aw_serve_close",
 ]
 
@@ -60,7 +60,7 @@ class WfaAttr(C.Structure):
     """wavefront_gpu_attr_t (include/anchorwave_b200.h)."""
     _fields_ = [("mismatch", C.c_int), ("gap_opening1", C.c_int), ("gap_extension1", C.c_int),
                 ("gap_opening2", C.c_int), ("gap_extension2", C.c_int), ("singletrack", C.c_int),
-                ("max_memory_abort", C.c_int64)]
+                ("memory_mode", C.c_int), ("max_memory_abort", C.c_int64)]
 
 
 def _load(path: str = LIB_PATH):
@@ -125,6 +125,8 @@ def _load(path: str = LIB_PATH):
     lib.wavefront_gpu_cigar.restype = i32
     lib.wavefront_align_batch_gpu.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, C.POINTER(C.c_float)]
     lib.wavefront_align_batch_gpu.restype = i32
+    lib.wavefront_gpu_memory.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
+    lib.wavefront_gpu_memory.restype = i32
     lib.aw_serve_open.argtypes = [C.POINTER(ServeConfig)]
     lib.aw_serve_open.restype = vp
     lib.aw_serve_submit.argtypes = [vp, C.c_uint64, i32, i32, C.c_char_p, i32, C.c_char_p, i32]

@@ -67,10 +67,11 @@ struct Res {
 
 int64_t predict_bytes(const Req &rq) {
     const int64_t ql = (int64_t)rq.q.size(), tl = (int64_t)rq.t.size();
-    if (rq.method == AW_ROUTE_WFA || rq.method == AW_ROUTE_WFA_SINGLETRACK) {
-        // wavefront retention grows with the alignment score; a length-based proxy
+    if (rq.method >= AW_ROUTE_WFA) {
+        // wavefront retention grows with the alignment score; a length-based proxy (the
+        // piggyback modes keep a ring of recent scores and about 1.6 bytes of blocks per cell)
         const int64_t L = ql + tl;
-        return 64 * L + L * L / (rq.method == AW_ROUTE_WFA ? 16 : 64);
+        return 64 * L + L * L / (rq.method == AW_ROUTE_WFA ? 16 : rq.method == AW_ROUTE_WFA_SINGLETRACK ? 64 : 128);
     }
     if (rq.band >= 0 && rq.band < std::max(ql, tl)) {
         const int64_t n = std::min(std::min(ql, tl), (int64_t)rq.band + 1);
@@ -142,12 +143,17 @@ bool take_batch(aw_server *S, std::vector<Req> &batch) {
 }
 
 // Device memory of one worker: its share of the budget, split between the KSW2 traceback
-// arena (reserved when the worker starts) and the wavefront pools of the two WFA engines
-// (allocated when an engine first runs), so that the pooled allocations of all workers
-// stay inside the budget whatever mix of engines each worker sees.
+// arena (60%, reserved when the worker starts) and the wavefront pools of the four WFA
+// engines (allocated when an engine first runs; high memory 20%, Singletrack 12% as it
+// keeps M only, medium and low 4% each as they keep a ring and packed-CIGAR blocks), so
+// that the pooled allocations of all workers stay inside the budget whatever mix of
+// engines each worker sees.
 int64_t worker_share(const aw_server *S) { return S->cfg.hbm_budget / std::max(1, S->cfg.slots); }
 int64_t ksw_tb_share(const aw_server *S) { return worker_share(S) * 6 / 10; }
-int64_t wfa_pool_share(const aw_server *S) { return worker_share(S) * 2 / 10; }
+int64_t wfa_pool_share(const aw_server *S, int method) {
+    const int pct = method == AW_ROUTE_WFA ? 20 : method == AW_ROUTE_WFA_SINGLETRACK ? 12 : 4;
+    return worker_share(S) * pct / 100;
+}
 
 void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wavefront_aligner_gpu_t **al) {
     const aw_serve_config_t &C = S->cfg;
@@ -193,10 +199,11 @@ void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wav
         a.mismatch = C.wfa_x, a.gap_opening1 = C.wfa_o1, a.gap_extension1 = C.wfa_e1;
         a.gap_opening2 = C.wfa_o2, a.gap_extension2 = C.wfa_e2;
         a.singletrack = method == AW_ROUTE_WFA_SINGLETRACK;
+        a.memory_mode = method == AW_ROUTE_WFA_MEDIUM ? 1 : method == AW_ROUTE_WFA_LOW ? 2 : 0;
         // wavefront pool of this engine in this worker: its part of the worker's share
-        a.max_memory_abort = std::max<int64_t>(wfa_pool_share(S), (int64_t)1 << 26);
+        a.max_memory_abort = std::max<int64_t>(wfa_pool_share(S, method), (int64_t)1 << 26);
         // one aligner per worker and engine, kept for the worker's lifetime
-        wavefront_aligner_gpu_t *&A = al[a.singletrack ? 1 : 0];
+        wavefront_aligner_gpu_t *&A = al[method - AW_ROUTE_WFA];
         if (!A) A = wavefront_aligner_new_gpu(&a);
         std::vector<const char *> pp(n), tp(n);
         std::vector<int> pl(n), tl(n), st(n), sc(n), no(n);
@@ -232,15 +239,14 @@ void worker_main(aw_server *S, int slot) {
     reserve_thread_tb(tb);
     std::vector<Req> batch;
     std::vector<Res> res;
-    wavefront_aligner_gpu_t *al[2] = {nullptr, nullptr};
+    wavefront_aligner_gpu_t *al[4] = {nullptr, nullptr, nullptr, nullptr};
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
             S->cv_work.wait(lk, [&] { return S->stopping || (S->queued > 0 && take_batch(S, batch)); });
             if (batch.empty() && S->stopping) {
                 lk.unlock();
-                wavefront_aligner_delete_gpu(al[0]);
-                wavefront_aligner_delete_gpu(al[1]);
+                for (wavefront_aligner_gpu_t *a : al) wavefront_aligner_delete_gpu(a);
                 return;
             }
             ++S->busy;
@@ -297,7 +303,7 @@ aw_server_t *aw_serve_open(const aw_serve_config_t *cfg) {
 
 int aw_serve_submit(aw_server_t *S, uint64_t id, int method, int band, const char *query, int qlen,
                     const char *target, int tlen) {
-    if (!S || qlen < 0 || tlen < 0 || method < AW_ROUTE_KSW2 || method > AW_ROUTE_WFA_SINGLETRACK) return AW_E_INVAL;
+    if (!S || qlen < 0 || tlen < 0 || method < AW_ROUTE_KSW2 || method > AW_ROUTE_WFA_LOW) return AW_E_INVAL;
     Req r;
     r.id = id, r.method = method, r.band = band;
     r.q.assign(query ? query : "", (size_t)qlen);

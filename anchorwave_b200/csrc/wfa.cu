@@ -19,6 +19,13 @@
 // every score for the piggyback backtrace (wavefront/wavefront_backtrace.c:321-530);
 // Singletrack keeps only M and recycles I/D through a ring of max(e1,e2)+1 slots,
 // then reconstructs the path from M (:587-762).
+// Medium and low memory (the piggyback modes, wavefront/wavefront_compute_affine2p.c:110-282)
+// keep only the last max_score_scope scores in a ring of slots; every cell carries the
+// packed CIGAR of its latest operations and a link to the block that holds the earlier
+// ones, and a cell whose packed CIGAR reaches 15 operations moves it into a new block
+// (wavefront/wavefront_backtrace_offload.c); the traceback follows the links from the end
+// cell and unpacks the blocks oldest first, re-extending the matches
+// (wavefront/wavefront_backtrace.c:767-799, wavefront/wavefront_pcigar.c:222-278).
 //
 // Memory: per-score headers and wavefront arrays come from one device pool by a
 // bump allocator (atomicAdd, 256 KiB chunks).  A pair that finds the pool empty
@@ -45,7 +52,14 @@ enum { CM = 0, CI1 = 1, CD1 = 2, CI2 = 3, CD2 = 4 };
 struct Alloc {
     int64_t cur, end;
     bool ok;
+    int64_t used;  // bytes taken from the pool (lane 0's copy)
 };
+
+// Packed CIGAR of the piggyback modes (wavefront/wavefront_pcigar.h:44-71): 2 bits per
+// operation, newest lowest (1 deletion, 2 mismatch or gap close, 3 insertion).
+constexpr uint32_t PC_ALMOST_FULL = 0x10000000u;  // 15 operations or more
+constexpr uint32_t BT_NULL = 0xFFFFFFFFu;          // no earlier block
+constexpr int PIG_ARRAYS = 15;                     // 5 components x (offsets, pcigar, link)
 
 __device__ __forceinline__ int64_t pool_grab(const WfaArgs &A, int64_t bytes) {
     const unsigned long long b = atomicAdd(A.pool_head, (unsigned long long)bytes);
@@ -63,7 +77,7 @@ __device__ int64_t warp_alloc(const WfaArgs &A, Alloc &al, int64_t bytes, int la
                 const int64_t sz = bytes > DATA_CHUNK ? bytes : DATA_CHUNK;
                 const int64_t b = pool_grab(A, sz);
                 if (b < 0) al.ok = false;
-                else al.cur = b, al.end = b + sz;
+                else al.cur = b, al.end = b + sz, al.used += sz;
             }
             if (al.ok) {
                 r = al.cur;
@@ -99,6 +113,18 @@ __device__ __forceinline__ int32_t getv(const WfaArgs &A, const CompHdr &h, int 
     return ((const int32_t *)(A.pool + h.off))[k - h.base];
 }
 
+// A piggyback cell: offset, packed CIGAR, link.  In a ring slot the three arrays of a
+// component lie h.pad elements apart.
+struct Cell {
+    int32_t o;
+    uint32_t pc, pv;
+};
+__device__ __forceinline__ Cell getc(const WfaArgs &A, const CompHdr &h, int k) {
+    if (k < h.lo || k > h.hi) return Cell{WF_NULL, 0u, BT_NULL};
+    const int32_t *d = (const int32_t *)(A.pool + h.off) + (k - h.base);
+    return Cell{d[0], (uint32_t)d[h.pad], (uint32_t)d[2 * h.pad]};
+}
+
 __device__ __forceinline__ uint64_t load8(const uint8_t *base, int64_t pos) {
     const uintptr_t a = (uintptr_t)(base + pos);
     const uint64_t *p = (const uint64_t *)(a & ~(uintptr_t)7);
@@ -122,6 +148,27 @@ __device__ __forceinline__ bool in_matrix(int32_t o, int k, int plen, int tlen) 
     return (uint32_t)o <= (uint32_t)tlen && (uint32_t)(o - k) <= (uint32_t)plen;
 }
 
+// Length of the run of equal bases from pattern[v] / text[h], by the extend step's rules
+// (2-bit words for ACGT-only pairs, else 8 bytes at a time up to the sentinels).
+__device__ int64_t lcp1(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat, const uint8_t *txt, int64_t v,
+                        int64_t h) {
+    const int64_t rem = min((int64_t)PR.plen - v, (int64_t)PR.tlen - h);
+    if (rem <= 0) return 0;
+    int64_t n = 0;
+    if (PR.packed) {
+        for (;;) {
+            const uint64_t x = load32b(A.ppat, PR.poff + v + n) ^ load32b(A.ptxt, PR.toff + h + n);
+            n += x ? (int64_t)((__ffsll((long long)x) - 1) >> 1) : 32;
+            if (x || n >= rem) return min(n, rem);
+        }
+    }
+    for (;;) {
+        const uint64_t x = load8(pat, v + n) ^ load8(txt, h + n);
+        if (x) return n + ((__ffsll((long long)x) - 1) >> 3);
+        n += 8;
+    }
+}
+
 __device__ __forceinline__ int64_t pb(int32_t o, int t) {
     return (int64_t)((((uint64_t)(int64_t)o) << 4) | (uint64_t)t);
 }
@@ -138,6 +185,7 @@ struct OpsWriter {
     }
 };
 
+template <bool PIG>
 __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
     const int lane = threadIdx.x & 31;
     const WfaPen P = A.pen;
@@ -153,10 +201,17 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         const int plen = PR.plen, tlen = PR.tlen;
         const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
         int64_t *ctab = A.ctab + PR.ctab_off;
-        Alloc al{0, 0, true};
-        const int64_t pool_start = -1;
-        (void)pool_start;
+        Alloc al{0, 0, true, 0};
         int status = 0, end_score = -1;
+        // piggyback ring: SR slots x 15 arrays x rcap elements; grows by reallocation
+        const int SR = A.max_score_scope;
+        int rcap = 0;
+        int64_t rbase = -1;
+        if constexpr (PIG) {
+            rcap = 32;
+            rbase = warp_alloc(A, al, (int64_t)SR * PIG_ARRAYS * rcap * 4, lane);
+            if (rbase < 0) status = WFA_RETRY;
+        }
         // Singletrack ring for I/D: R slots x 4 components x cap offsets
         const int R = (P.e1 > P.e2 ? P.e1 : P.e2) + 1;
         const int ring_cap = plen + tlen + 8;
@@ -173,15 +228,20 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         }
         int64_t d0 = -1;
         if (status == 0) {
-            d0 = warp_alloc(A, al, 16, lane);
+            if constexpr (PIG) d0 = rbase;  // slot 0, component M
+            else d0 = warp_alloc(A, al, 16, lane);
             if (d0 < 0) status = WFA_RETRY;
         }
         if (status == 0 && lane == 0) {
             ctab[0] = h0;
             ScoreHdr *H = (ScoreHdr *)(A.pool + h0);
             for (int c = 0; c < 5; ++c) H->c[c] = CompHdr{1, -1, 0, 0, 0};
-            H->c[CM] = CompHdr{0, 0, 0, 0, d0};
+            H->c[CM] = CompHdr{0, 0, 0, PIG ? rcap : 0, d0};
             *(int32_t *)(A.pool + d0) = 0;
+            if constexpr (PIG) {
+                ((uint32_t *)(A.pool + d0))[rcap] = 0u;
+                ((uint32_t *)(A.pool + d0))[2 * rcap] = BT_NULL;  // the start (0, 0)
+            }
             if (HR.rs) HR.ring[0] = *H;
         }
         __syncwarp();
@@ -323,19 +383,32 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
             CompHdr out[5];
             for (int c = 0; c < 5; ++c) out[c] = NUL;
             const bool alloc_c[5] = {true, a_i1, a_d1, a_i2, a_d2};
-            const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
-            int nstore = 1;
-            if (!A.singletrack) nstore += (int)a_i1 + (int)a_d1 + (int)a_i2 + (int)a_d2;
-            if (A.singletrack && width > ring_cap) {
-                status = WFA_OVERFLOW;
-                break;
-            }
-            const int64_t blk = warp_alloc(A, al, wb * nstore, lane);
-            if (blk < 0) {
-                status = WFA_RETRY;
-                break;
-            }
-            {
+            if constexpr (PIG) {
+                if (width > rcap) {
+                    const int nc = max(2 * rcap, (width + 3) & ~3);
+                    const int64_t nb = warp_alloc(A, al, (int64_t)SR * PIG_ARRAYS * nc * 4, lane);
+                    if (nb < 0) {
+                        status = WFA_RETRY;
+                        break;
+                    }
+                    rcap = nc, rbase = nb;
+                }
+                for (int c = 0; c < 5; ++c)
+                    if (alloc_c[c])
+                        out[c] = CompHdr{lo, hi, lo, rcap, rbase + ((int64_t)(s % SR) * PIG_ARRAYS + c * 3) * rcap * 4};
+            } else {
+                const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
+                int nstore = 1;
+                if (!A.singletrack) nstore += (int)a_i1 + (int)a_d1 + (int)a_i2 + (int)a_d2;
+                if (A.singletrack && width > ring_cap) {
+                    status = WFA_OVERFLOW;
+                    break;
+                }
+                const int64_t blk = warp_alloc(A, al, wb * nstore, lane);
+                if (blk < 0) {
+                    status = WFA_RETRY;
+                    break;
+                }
                 int64_t o = blk;
                 for (int c = 0; c < 5; ++c) {
                     if (!alloc_c[c]) continue;
@@ -355,33 +428,117 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
             int kmin[5], kmax[5];
 #pragma unroll
             for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
-            // four diagonals per lane at a time: all input loads before any output store
-            for (int k0 = lo + lane; k0 <= hi; k0 += 128) {
-                int32_t ins1[4], ins2[4], del1[4], del2[4], misms[4];
+            if constexpr (PIG) {
+                // two diagonals per lane at a time; each gap cell takes the extension on a
+                // tie, M the mismatch, then D2, D1, I2, I1 (the kernel's assignment order).
+                // Every lane runs every trip (the block allocation below is warp-wide).
+                for (int kb = lo; kb <= hi; kb += 64) {
+                    const int k0 = kb + lane;
+                    Cell C[2][5];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int k = k0 + 32 * u;
-                    ins1[u] = max(getv(A, m_open1, k - 1), getv(A, i1, k - 1)) + 1;
-                    ins2[u] = max(getv(A, m_open2, k - 1), getv(A, i2, k - 1)) + 1;
-                    del1[u] = max(getv(A, m_open1, k + 1), getv(A, d1, k + 1));
-                    del2[u] = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
-                    misms[u] = getv(A, m_misms, k) + 1;
+                    for (int u = 0; u < 2; ++u) {
+                        const int k = k0 + 32 * u;
+                        Cell a = getc(A, m_open1, k - 1), b = getc(A, i1, k - 1);
+                        Cell g = b.o >= a.o ? b : a;
+                        C[u][CI1] = Cell{g.o + 1, (g.pc << 2) | 3u, g.pv};
+                        a = getc(A, m_open2, k - 1), b = getc(A, i2, k - 1);
+                        g = b.o >= a.o ? b : a;
+                        C[u][CI2] = Cell{g.o + 1, (g.pc << 2) | 3u, g.pv};
+                        a = getc(A, m_open1, k + 1), b = getc(A, d1, k + 1);
+                        g = b.o >= a.o ? b : a;
+                        C[u][CD1] = Cell{g.o, (g.pc << 2) | 1u, g.pv};
+                        a = getc(A, m_open2, k + 1), b = getc(A, d2, k + 1);
+                        g = b.o >= a.o ? b : a;
+                        C[u][CD2] = Cell{g.o, (g.pc << 2) | 1u, g.pv};
+                        Cell x = getc(A, m_misms, k);
+                        x.o += 1;
+                        const int32_t best = max(max(C[u][CD1].o, C[u][CD2].o), max(x.o, max(C[u][CI1].o, C[u][CI2].o)));
+                        const Cell &src = best == x.o ? x
+                                          : best == C[u][CD2].o ? C[u][CD2]
+                                          : best == C[u][CD1].o ? C[u][CD1]
+                                          : best == C[u][CI2].o ? C[u][CI2]
+                                                                : C[u][CI1];
+                        C[u][CM] = Cell{in_matrix(best, k, plen, tlen) ? best : WF_NULL, (src.pc << 2) | 2u, src.pv};
+                    }
+                    // cells whose packed CIGAR holds 15 operations move it into a block;
+                    // the warp takes its blocks in one allocation (lane order)
+                    uint32_t fl = 0;
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int k = k0 + 32 * u;
+#pragma unroll
+                        for (int c = 0; c < 5; ++c)
+                            if (k <= hi && alloc_c[c] && C[u][c].pc >= PC_ALMOST_FULL && in_matrix(C[u][c].o, k, plen, tlen))
+                                fl |= 1u << (u * 5 + c);
+                    }
+                    const int cnt = __popc(fl);
+                    int incl = cnt;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const int t = __shfl_up_sync(0xffffffffu, incl, d);
+                        if (lane >= d) incl += t;
+                    }
+                    const int total = __shfl_sync(0xffffffffu, incl, 31);
+                    if (total > 0) {
+                        const int64_t bb = warp_alloc(A, al, (int64_t)total * 8, lane);
+                        if (bb < 0) {
+                            status = WFA_RETRY;
+                            break;
+                        }
+                        uint32_t idx = (uint32_t)(bb >> 3) + (uint32_t)(incl - cnt);
+                        uint2 *blk = (uint2 *)A.pool;
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+#pragma unroll
+                            for (int c = 0; c < 5; ++c)
+                                if (fl & (1u << (u * 5 + c))) {
+                                    blk[idx] = make_uint2(C[u][c].pc, C[u][c].pv);
+                                    C[u][c].pc = 0u, C[u][c].pv = idx++;
+                                }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int k = k0 + 32 * u;
+                        if (k > hi) break;
+#pragma unroll
+                        for (int c = 0; c < 5; ++c) {
+                            if (!alloc_c[c]) continue;
+                            int32_t *d = (int32_t *)(A.pool + out[c].off) + (k - lo);
+                            d[0] = C[u][c].o, d[rcap] = (int32_t)C[u][c].pc, d[2 * rcap] = (int32_t)C[u][c].pv;
+                            if (in_matrix(C[u][c].o, k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
+                        }
+                    }
                 }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int k = k0 + 32 * u;
-                    if (k > hi) break;
-                    int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
-                    if (!in_matrix(best, k, plen, tlen)) best = WF_NULL;
-                    oM[k - lo] = best;
-                    if (oI1) oI1[k - lo] = ins1[u];
-                    if (oD1) oD1[k - lo] = del1[u];
-                    if (oI2) oI2[k - lo] = ins2[u];
-                    if (oD2) oD2[k - lo] = del2[u];
-                    const int32_t vals[5] = {best, ins1[u], del1[u], ins2[u], del2[u]};
-#pragma unroll
-                    for (int c = 0; c < 5; ++c)
-                        if (in_matrix(vals[c], k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
+                if (status != 0) break;
+            } else {
+                // four diagonals per lane at a time: all input loads before any output store
+                for (int k0 = lo + lane; k0 <= hi; k0 += 128) {
+                    int32_t ins1[4], ins2[4], del1[4], del2[4], misms[4];
+    #pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + 32 * u;
+                        ins1[u] = max(getv(A, m_open1, k - 1), getv(A, i1, k - 1)) + 1;
+                        ins2[u] = max(getv(A, m_open2, k - 1), getv(A, i2, k - 1)) + 1;
+                        del1[u] = max(getv(A, m_open1, k + 1), getv(A, d1, k + 1));
+                        del2[u] = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
+                        misms[u] = getv(A, m_misms, k) + 1;
+                    }
+    #pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + 32 * u;
+                        if (k > hi) break;
+                        int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
+                        if (!in_matrix(best, k, plen, tlen)) best = WF_NULL;
+                        oM[k - lo] = best;
+                        if (oI1) oI1[k - lo] = ins1[u];
+                        if (oD1) oD1[k - lo] = del1[u];
+                        if (oI2) oI2[k - lo] = ins2[u];
+                        if (oD2) oD2[k - lo] = del2[u];
+                        const int32_t vals[5] = {best, ins1[u], del1[u], ins2[u], del2[u]};
+    #pragma unroll
+                        for (int c = 0; c < 5; ++c)
+                            if (in_matrix(vals[c], k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
+                    }
                 }
             }
             __syncwarp();
@@ -405,10 +562,62 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         if (lane == 0) {
             WfaOutDev o;
             o.status = status, o.score = 0, o.n_ops = 0, o.final_s = s;
-            o.mem_bytes = 0;
+            o.mem_bytes = al.used;
             if (status == 0) {
                 OpsWriter w{A.ops + PR.ops_off, 0, plen + tlen + 8, true};
-                if (!A.singletrack) {
+                if constexpr (PIG) {
+                    // reverse the links from the end cell in place, then unpack the blocks
+                    // oldest first: before every operation taken in M the run of matches
+                    // is re-extended; the mismatch that closes a gap is dropped
+                    const CompHdr m = HR.get(A, ctab, end_score, end_score)->c[CM];
+                    const uint32_t *md = (const uint32_t *)(A.pool + m.off) + (k_end - m.base);
+                    const uint32_t pc_end = md[m.pad];
+                    uint32_t cur = md[2 * m.pad], prv = BT_NULL;
+                    uint2 *blk = (uint2 *)A.pool;
+                    const int64_t lim = 2 * ((int64_t)plen + tlen) + 64;
+                    int64_t steps = 0;
+                    bool ok = true;
+                    while (cur != BT_NULL) {
+                        if (++steps > lim) { ok = false; break; }
+                        const uint32_t nxt = blk[cur].y;
+                        blk[cur].y = prv;
+                        prv = cur, cur = nxt;
+                    }
+                    int64_t v = 0, h = 0;
+                    bool in_m = true;
+                    cur = prv;
+                    for (bool last = false; ok && !last;) {
+                        uint32_t pc;
+                        if (cur != BT_NULL) pc = blk[cur].x, cur = blk[cur].y;
+                        else pc = pc_end, last = true;
+                        const int len = pc ? 16 - (__clz(pc) >> 1) : 0;
+                        for (int j = len - 1; j >= 0; --j) {
+                            if (in_m) {
+                                const int64_t nm = lcp1(A, PR, pat, txt, v, h);
+                                w.put('M', (int)nm);
+                                v += nm, h += nm;
+                            }
+                            const uint32_t op = (pc >> (2 * j)) & 3u;
+                            if (!in_m && op == 2u) {
+                                in_m = true;
+                                continue;
+                            }
+                            w.put(op == 1u ? 'D' : op == 2u ? 'X' : 'I', 1);
+                            v += (op == 1u || op == 2u), h += (op == 2u || op == 3u);
+                            in_m = op == 2u;
+                            if (op == 0u || v > plen || h > tlen) { ok = false; break; }
+                        }
+                    }
+                    if (ok) {
+                        const int64_t nm = min((int64_t)plen - v, (int64_t)tlen - h);
+                        w.put('M', (int)nm);
+                        v += nm, h += nm;
+                        w.put('I', (int)(tlen - h));
+                        w.put('D', (int)(plen - v));
+                    } else {
+                        o.status = WFA_UNATTAINABLE;
+                    }
+                } else if (!A.singletrack) {
                     enum { BM = 9, BD2E = 8, BD2O = 7, BD1E = 6, BD1O = 5, BI2E = 4, BI2O = 3, BI1E = 2, BI1O = 1 };
                     int mt = CM, sc = end_score, k = k_end;
                     int32_t off = tlen;
@@ -534,7 +743,7 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                 }
                 if (!w.ok) o.status = WFA_OVERFLOW;
                 if (o.status == 0) {
-                    for (int a = 0, b = w.n - 1; a < b; ++a, --b) {
+                    for (int a = 0, b = PIG ? 0 : w.n - 1; a < b; ++a, --b) {
                         const char t = w.buf[a];
                         w.buf[a] = w.buf[b], w.buf[b] = t;
                     }
@@ -558,15 +767,21 @@ static int ring_size(int scope) {
     return rs <= 128 ? rs : 0;
 }
 
-cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st) {
+template <bool PIG>
+static cudaError_t launch_wfa_t(const WfaArgs &a, int ctas, cudaStream_t st) {
     const int rs = ring_size(a.max_score_scope);
     const size_t smem = (size_t)4 * rs * sizeof(ScoreHdr);
     if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(wfa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const cudaError_t e =
+            cudaFuncSetAttribute(wfa_kernel<PIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    wfa_kernel<<<ctas, 128, smem, st>>>(a, rs);
+    wfa_kernel<PIG><<<ctas, 128, smem, st>>>(a, rs);
     return cudaGetLastError();
+}
+
+cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st) {
+    return a.piggyback ? launch_wfa_t<true>(a, ctas, st) : launch_wfa_t<false>(a, ctas, st);
 }
 
 namespace {
@@ -622,11 +837,12 @@ cudaError_t launch_wfa_pack(const uint8_t *pat, int64_t pbytes, uint64_t *ppat, 
     return cudaGetLastError();
 }
 
-int wfa_occupancy() {
+int wfa_occupancy(bool piggyback) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_kernel, 128, 4 * 32 * sizeof(ScoreHdr)) != cudaSuccess)
-        return 1;
-    return nb;
+    const cudaError_t e =
+        piggyback ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_kernel<true>, 128, 4 * 32 * sizeof(ScoreHdr))
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wfa_kernel<false>, 128, 4 * 32 * sizeof(ScoreHdr));
+    return e == cudaSuccess ? nb : 1;
 }
 
 }  // namespace aw

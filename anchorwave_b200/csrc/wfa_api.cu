@@ -55,7 +55,7 @@ struct wavefront_aligner_gpu {
     // single-call result
     std::string ops;
     int score = 0;
-    uint64_t mem_used = 0;
+    int64_t mem_pair_max = 0, mem_total = 0;
     int sms = 0;
     float last_ms = 0.f;
     int last_launches = 0;
@@ -134,6 +134,8 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
         WCUDA(cudaMemGetInfo(&fr, &tot));
         int64_t want = (int64_t)(fr * 0.85);
         if (A.max_memory_abort > 0) want = std::min<int64_t>(want, A.max_memory_abort);
+        // piggyback blocks are addressed by 32-bit indices of 8-byte units
+        if (A.memory_mode != 0) want = std::min<int64_t>(want, ((int64_t)1 << 35) - ((int64_t)1 << 20));
         want = std::max<int64_t>(want, (int64_t)64 << 20);
         WCUDA(al->d_pool.ensure((size_t)want));
     }
@@ -155,10 +157,11 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     W.out = al->d_out.as<WfaOutDev>();
     W.queue = al->d_queue.as<int32_t>();
     W.pen = WfaPen{A.mismatch, A.gap_opening1, A.gap_extension1, A.gap_opening2, A.gap_extension2};
-    W.singletrack = A.singletrack ? 1 : 0;
+    W.piggyback = A.memory_mode != 0 ? 1 : 0;
+    W.singletrack = A.singletrack && !W.piggyback ? 1 : 0;
     const int scope = std::max(A.gap_opening1 + A.gap_extension1, A.gap_opening2 + A.gap_extension2);
     W.max_score_scope = std::max(scope, A.mismatch) + 1;
-    const int occ = std::max(1, wfa_occupancy());
+    const int occ = std::max(1, wfa_occupancy(W.piggyback != 0));
     // Rounds: every round restarts the pool and runs up to `chunk` pending pairs, largest
     // first; pairs that found the pool exhausted stay pending.  A round that completes
     // nothing halves the chunk (the pairs in flight together share the pool), one that
@@ -209,6 +212,11 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     }
     al->last_ms = total_ms;
     al->last_launches = launches;
+    al->mem_pair_max = 0, al->mem_total = 0;
+    for (int i = 0; i < n; ++i) {
+        al->mem_pair_max = std::max<int64_t>(al->mem_pair_max, al->outs[i].mem_bytes);
+        al->mem_total += al->outs[i].mem_bytes;
+    }
     return AW_OK;
 }
 
@@ -237,6 +245,10 @@ wavefront_aligner_gpu_t *wavefront_aligner_new_gpu(const wavefront_gpu_attr_t *a
     if (attr->mismatch <= 0 || attr->gap_opening1 < 0 || attr->gap_extension1 <= 0 || attr->gap_opening2 < 0 ||
         attr->gap_extension2 <= 0) {
         set_error("wavefront_aligner_new_gpu: penalties must be X>0, O1>=0, E1>0, O2>=0, E2>0");
+        return nullptr;
+    }
+    if (attr->memory_mode < 0 || attr->memory_mode > 2) {
+        set_error("wavefront_aligner_new_gpu: memory_mode must be 0 (high), 1 (medium) or 2 (low)");
         return nullptr;
     }
     wavefront_aligner_gpu *al = new wavefront_aligner_gpu();
@@ -271,6 +283,13 @@ int wavefront_align_gpu(wavefront_aligner_gpu_t *al, const char *pattern, int pa
         al->score = o.score;
     }
     return public_status(o.status);
+}
+
+int wavefront_gpu_memory(const wavefront_aligner_gpu_t *al, int64_t *pair_max, int64_t *total) {
+    if (!al) return AW_E_INVAL;
+    if (pair_max) *pair_max = al->mem_pair_max;
+    if (total) *total = al->mem_total;
+    return AW_OK;
 }
 
 int wavefront_gpu_cigar(const wavefront_aligner_gpu_t *al, const char **operations, int *num_operations,

@@ -45,6 +45,7 @@ struct WfaArgs {
     int32_t *queue;
     WfaPen pen;
     int singletrack;
+    int piggyback;        // medium / low memory: ring of recent scores + packed-CIGAR blocks
     int max_score_scope;
 };
 
@@ -53,6 +54,6 @@ cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st);
 // the per-pair flag that the pair's sequences are uppercase ACGT only.
 cudaError_t launch_wfa_pack(const uint8_t *pat, int64_t pbytes, uint64_t *ppat, const uint8_t *txt, int64_t tbytes,
                             uint64_t *ptxt, WfaPairDev *pairs, int n, cudaStream_t st);
-int wfa_occupancy();
+int wfa_occupancy(bool piggyback);
 
 }  // namespace aw

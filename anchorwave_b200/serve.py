@@ -18,6 +18,8 @@ ROUTE_KSW2 = 0
 ROUTE_KSW2_SINGLETRACK = 1
 ROUTE_WFA = 2
 ROUTE_WFA_SINGLETRACK = 3
+ROUTE_WFA_MEDIUM = 4
+ROUTE_WFA_LOW = 5
 
 
 @dataclass

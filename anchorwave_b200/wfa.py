@@ -3,8 +3,9 @@
 * :class:`WfaAligner` mirrors the WFA2-lib aligner object AnchorWave caches per thread
   (wavefront_aligner_new / wavefront_align / wavefront_aligner_delete, WFA2-lib
   wavefront/wfa.h:129-134, :210-215) with the attributes of
-  src/myImportandFunction/WfaAlignment.cpp:143-170 (match 0, positive penalties, high
-  memory, no heuristic, end to end, full CIGAR, optional Singletrack).
+  src/myImportandFunction/WfaAlignment.cpp:143-170 (match 0, positive penalties, no
+  heuristic, end to end, full CIGAR) in high memory (optionally Singletrack), medium or
+  low memory (WfaAlignment.cpp:461-543: alignWith{Singletrack,Standard,Medium,Low}Wfa).
 * :func:`align_with_wfa` mirrors alignWithWfaMode + decodeCigar
   (WfaAlignment.cpp:223-391): reference is the pattern, query the text; 'M'/'X' consume
   both, 'I' the query, 'D' the reference; score is the negated penalty.
@@ -22,6 +23,11 @@ WF_STATUS_ALG_COMPLETED = 0
 WF_STATUS_OOM = -200
 WF_STATUS_UNATTAINABLE = -300
 
+# wavefront_memory_t (WFA2-lib wavefront/wavefront_attributes.h:122-127)
+WAVEFRONT_MEMORY_HIGH = 0
+WAVEFRONT_MEMORY_MED = 1
+WAVEFRONT_MEMORY_LOW = 2
+
 
 def positive_penalty(p: int) -> int:
     """AnchorWave passes negative penalties; WFA takes their magnitude (WfaAlignment.cpp:298-302)."""
@@ -30,9 +36,10 @@ def positive_penalty(p: int) -> int:
 
 class WfaAligner:
     def __init__(self, mismatch: int, gap_opening1: int, gap_extension1: int, gap_opening2: int,
-                 gap_extension2: int, singletrack: bool = False, max_memory_abort: int = 0):
+                 gap_extension2: int, singletrack: bool = False, max_memory_abort: int = 0,
+                 memory_mode: int = WAVEFRONT_MEMORY_HIGH):
         self.attr = WfaAttr(mismatch, gap_opening1, gap_extension1, gap_opening2, gap_extension2,
-                            int(bool(singletrack)), int(max_memory_abort))
+                            int(bool(singletrack)), int(memory_mode), int(max_memory_abort))
         self.h = lib.wavefront_aligner_new_gpu(C.byref(self.attr))
         if not self.h:
             raise AwError(f"wavefront_aligner_new_gpu failed: {last_error()}")
@@ -102,6 +109,13 @@ class WfaAligner:
         out = [(int(status[i]), int(score[i]), raw[offs[i]:offs[i] + nops[i]].decode()) for i in range(n)]
         return out, ms.value
 
+    def memory(self) -> Tuple[int, int]:
+        """Device bytes the last call's alignments took: (largest single alignment, sum)."""
+        mx = C.c_int64(0)
+        tot = C.c_int64(0)
+        lib.wavefront_gpu_memory(self.h, C.byref(mx), C.byref(tot))
+        return mx.value, tot.value
+
     def close(self):
         if self.h:
             lib.wavefront_aligner_delete_gpu(self.h)
@@ -139,11 +153,12 @@ def decode_cigar(query: str, reference: str, ops: str):
 
 
 def align_with_wfa(query: str, reference: str, mismatching_penalty: int, open1: int, extend1: int, open2: int,
-                   extend2: int, singletrack: bool = False, aligner: WfaAligner = None):
+                   extend2: int, singletrack: bool = False, aligner: WfaAligner = None,
+                   memory_mode: int = WAVEFRONT_MEMORY_HIGH):
     """alignWithWfaMode (WfaAlignment.cpp:270-391) on the GPU: (status, score, aln_query, aln_reference)."""
     al = aligner or WfaAligner(positive_penalty(mismatching_penalty), positive_penalty(open1),
                                positive_penalty(extend1), positive_penalty(open2), positive_penalty(extend2),
-                               singletrack)
+                               singletrack, memory_mode=memory_mode)
     st = al.align(reference.encode(), query.encode())
     if st != WF_STATUS_ALG_COMPLETED:
         return st, 0, "", ""
@@ -152,3 +167,17 @@ def align_with_wfa(query: str, reference: str, mismatching_penalty: int, open1: 
     if dec is None:
         return WF_STATUS_UNATTAINABLE, 0, "", ""
     return st, score, dec[0], dec[1]
+
+
+def align_with_medium_wfa(query: str, reference: str, mismatching_penalty: int, open1: int, extend1: int,
+                          open2: int, extend2: int, aligner: WfaAligner = None):
+    """alignWithMediumWfa (WfaAlignment.cpp:503-522): medium memory, piggyback traceback."""
+    return align_with_wfa(query, reference, mismatching_penalty, open1, extend1, open2, extend2, aligner=aligner,
+                          memory_mode=WAVEFRONT_MEMORY_MED)
+
+
+def align_with_low_wfa(query: str, reference: str, mismatching_penalty: int, open1: int, extend1: int,
+                       open2: int, extend2: int, aligner: WfaAligner = None):
+    """alignWithLowWfa (WfaAlignment.cpp:524-543): low memory, piggyback traceback."""
+    return align_with_wfa(query, reference, mismatching_penalty, open1, extend1, open2, extend2, aligner=aligner,
+                          memory_mode=WAVEFRONT_MEMORY_LOW)

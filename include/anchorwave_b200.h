@@ -116,11 +116,16 @@ int aw_cigar_rows_batch(int n, const uint32_t *const *cigar, const int *n_cigar,
 
 /* ---- WFA (gap-affine-2p, end to end) ------------------------------------------ */
 
-/* Attributes of WfaAlignment.cpp:143-170: match 0, these penalties (positive), high
- * memory, no heuristic, full CIGAR; singletrack selects the Singletrack traceback. */
+/* Attributes of WfaAlignment.cpp:143-170: match 0, these penalties (positive), no
+ * heuristic, full CIGAR; memory_mode as WFA2-lib's wavefront_memory_t
+ * (wavefront/wavefront_attributes.h:122-127): 0 high (every wavefront kept), 1 medium and
+ * 2 low (piggyback: a ring of recent scores plus packed-CIGAR blocks; the ultralow
+ * BiWFA mode 3 is not provided).  singletrack selects the Singletrack traceback and, as in
+ * wavefront/wavefront_aligner.c:251-260, only applies in high memory. */
 typedef struct {
     int mismatch, gap_opening1, gap_extension1, gap_opening2, gap_extension2;
     int singletrack;
+    int memory_mode;
     int64_t max_memory_abort;   /* device pool cap in bytes (0 = 85% of free memory) */
 } wavefront_gpu_attr_t;
 
@@ -145,6 +150,10 @@ int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const cha
                               const int *text_length, int *status, int *score,
                               int64_t *ops_offset, int *n_ops, char *ops, int64_t ops_capacity,
                               float *device_ms);
+/* Device memory the last call's alignments took from the wavefront pool (headers,
+ * wavefronts and packed-CIGAR blocks; the reference's align_status.memory_used,
+ * WfaAlignment.cpp:353-354): the largest single alignment and the sum over the call. */
+int wavefront_gpu_memory(const wavefront_aligner_gpu_t *aligner, int64_t *pair_max, int64_t *total);
 
 /* ---- serving loop (continuous batching) --------------------------------------- */
 
@@ -154,6 +163,8 @@ int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const cha
 #define AW_ROUTE_KSW2_SINGLETRACK 1  /* ksw_extd2 with the Singletrack traceback */
 #define AW_ROUTE_WFA              2  /* gap-affine-2p WFA, high memory */
 #define AW_ROUTE_WFA_SINGLETRACK  3  /* gap-affine-2p WFA, Singletrack */
+#define AW_ROUTE_WFA_MEDIUM       4  /* gap-affine-2p WFA, medium memory (piggyback) */
+#define AW_ROUTE_WFA_LOW          5  /* gap-affine-2p WFA, low memory (piggyback) */
 
 typedef struct {
     int slots;            /* concurrent micro-batches (workers with their own streams) */

@@ -118,6 +118,9 @@ class Restatement:
             L.oracle_wfa_align.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int,
                                            C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
                                            C.c_char_p, C.c_int, C.POINTER(C.c_int)]
+            L.oracle_wfa_align_mode.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int,
+                                                C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                                C.c_char_p, C.c_int, C.POINTER(C.c_int)]
 
     def ksw_extd2(self, query: bytes, target: bytes, mat, q, e, q2, e2, w=-1, zdrop=-1, end_bonus=0,
                   flag=0, block=64, m=5, stop_interval=0, stop_at=-1) -> KswResult:
@@ -127,13 +130,15 @@ class Restatement:
                                   C.byref(ez))
         return extz_to_result(ez, self.lib.oracle_free)
 
-    def wfa_align(self, pattern: bytes, text: bytes, x, o1, e1, o2, e2, singletrack=False):
+    def wfa_align(self, pattern: bytes, text: bytes, x, o1, e1, o2, e2, singletrack=False, memory_mode=0):
+        """memory_mode as WFA2-lib's wavefront_memory_t: 0 high, 1 medium, 2 low (piggyback)."""
         score = C.c_int(0)
         nops = C.c_int(0)
         cap = len(pattern) + len(text) + 16
         ops = C.create_string_buffer(cap)
-        st = self.lib.oracle_wfa_align(pattern, len(pattern), text, len(text), x, o1, e1, o2, e2,
-                                       int(bool(singletrack)), C.byref(score), ops, cap, C.byref(nops))
+        st = self.lib.oracle_wfa_align_mode(pattern, len(pattern), text, len(text), x, o1, e1, o2, e2,
+                                            int(bool(singletrack)), int(memory_mode), C.byref(score), ops, cap,
+                                            C.byref(nops))
         return st, score.value, ops.raw[: nops.value].decode() if st == 0 else ""
 
 

@@ -17,6 +17,15 @@
  *                             wavefront/wavefront_termination.c:37-60
  *   backtrace (piggyback ties) wavefront/wavefront_backtrace.c:41-60, :321-530
  *   Singletrack backtrace     wavefront/wavefront_backtrace.c:587-762
+ *   medium / low memory       (memory_mode 1 / 2, wavefront/wavefront_attributes.h:122-127)
+ *     piggyback kernel        wavefront/wavefront_compute_affine2p.c:110-282
+ *                             (the gap-affine delegate :291-299 has the same ties)
+ *     occupancy + offload     wavefront/wavefront_backtrace_offload.c:39-71, :130-288
+ *     BT-buffer               wavefront/wavefront_backtrace_buffer.c:219-247
+ *     pcigar traceback        wavefront/wavefront_backtrace.c:767-799,
+ *                             wavefront/wavefront_backtrace_buffer.c:251-265, :323-366,
+ *                             wavefront/wavefront_pcigar.c:222-278
+ *   (Singletrack is only honoured in high memory, wavefront/wavefront_aligner.c:251-260.)
  * Every wavefront value outside its trimmed [lo, hi] reads as NULL, which is
  * what the reference's init_ends NULL padding makes it.
  */
@@ -31,7 +40,33 @@ typedef struct {
     int lo, hi;      /* trimmed range; lo > hi means null */
     int base;        /* off[k - base] */
     int32_t *off;
+    uint32_t *pc;    /* piggyback: packed CIGAR of the cell's last operations */
+    uint32_t *pv;    /* piggyback: BT-block holding the operations before them */
+    int occ;         /* piggyback: bt_occupancy_max */
 } wo_wf;
+
+/* Packed CIGAR (wavefront/wavefront_pcigar.h:44-71): 2 bits per operation, newest in the
+ * low bits: 1 deletion, 2 mismatch (or gap close), 3 insertion; 16 operations per word. */
+#define WO_PC_FULL 0x40000000u
+#define WO_PC_ALMOST_FULL 0x10000000u /* 15 operations or more */
+#define WO_PC_HALF_FULL 0x00010000u   /* 9 operations or more */
+#define WO_BT_NULL 0xFFFFFFFFu
+
+typedef struct {
+    uint32_t pc, prev;
+} wo_blk;
+typedef struct {
+    wo_blk *b;
+    size_t n, cap;
+} wo_blocks;
+static uint32_t wo_blk_push(wo_blocks *B, uint32_t pc, uint32_t prev) {
+    if (B->n == B->cap) {
+        B->cap = B->cap ? 2 * B->cap : 1024;
+        B->b = (wo_blk *)realloc(B->b, sizeof(wo_blk) * B->cap);
+    }
+    B->b[B->n].pc = pc, B->b[B->n].prev = prev;
+    return (uint32_t)B->n++;
+}
 
 typedef struct {
     wo_wf *M, *I1, *D1, *I2, *D2; /* NULL pointer: no wavefront for that score */
@@ -45,15 +80,44 @@ static int wo_isnull(const wo_wf *w) { return !w || w->lo > w->hi; }
 static __thread long long wo_ints_allocated = 0;
 /* Offsets allocated by the last oracle_wfa_align call on this thread (sizing aid). */
 long long oracle_wfa_last_ints(void) { return wo_ints_allocated; }
+static __thread int wo_bt = 0; /* the aligner runs in a piggyback memory mode */
 static wo_wf *wo_new(int lo, int hi) {
     wo_wf *w = (wo_wf *)malloc(sizeof(wo_wf));
-    wo_ints_allocated += hi - lo + 1 > 0 ? hi - lo + 1 : 1;
+    const size_t len = (size_t)(hi - lo + 1 > 0 ? hi - lo + 1 : 1);
+    wo_ints_allocated += (long long)len;
     w->lo = lo, w->hi = hi, w->base = lo;
-    w->off = (int32_t *)malloc(sizeof(int32_t) * (size_t)(hi - lo + 1 > 0 ? hi - lo + 1 : 1));
+    w->off = (int32_t *)malloc(sizeof(int32_t) * len);
+    w->pc = wo_bt ? (uint32_t *)calloc(len, sizeof(uint32_t)) : 0;
+    w->pv = wo_bt ? (uint32_t *)malloc(sizeof(uint32_t) * len) : 0;
+    w->occ = 0;
     return w;
 }
 static void wo_free(wo_wf *w) {
-    if (w) free(w->off), free(w);
+    if (w) free(w->off), free(w->pc), free(w->pv), free(w);
+}
+static uint32_t wo_getpc(const wo_wf *w, int k) {
+    if (!w || w->lo > w->hi || k < w->lo || k > w->hi) return 0;
+    return w->pc[k - w->base];
+}
+static uint32_t wo_getpv(const wo_wf *w, int k) {
+    if (!w || w->lo > w->hi || k < w->lo || k > w->hi) return WO_BT_NULL;
+    return w->pv[k - w->base];
+}
+/* wavefront_backtrace_offload_blocks_selective: every cell of [lo, hi] with an offset and
+ * at least the mask's operations moves its packed CIGAR into a new BT-block. */
+static void wo_offload(wo_wf *w, int lo, int hi, uint32_t mask, wo_blocks *B) {
+    for (int k = lo; k <= hi; ++k) {
+        if (w->off[k - w->base] >= 0 && w->pc[k - w->base] >= mask) {
+            const uint32_t idx = wo_blk_push(B, w->pc[k - w->base], w->pv[k - w->base]);
+            w->pc[k - w->base] = 0;
+            w->pv[k - w->base] = idx;
+        }
+    }
+}
+static int wo_lcp(const char *pattern, int plen, const char *text, int tlen, int v, int h) {
+    int n = 0;
+    while (v + n < plen && h + n < tlen && pattern[v + n] == text[h + n]) ++n;
+    return n;
 }
 static void wo_trim(wo_wf *w, int plen, int tlen) {
     int k;
@@ -78,16 +142,25 @@ static int32_t mx(int32_t a, int32_t b) { return a > b ? a : b; }
  * success *score is the classic score (-penalty) and ops[0..*n_ops) the CIGAR
  * operations (M match, X mismatch, I text-only, D pattern-only).
  */
-int oracle_wfa_align(const char *pattern, int plen, const char *text, int tlen, int x, int o1, int e1,
-                     int o2, int e2, int singletrack, int *score_out, char *ops, int ops_cap, int *n_ops) {
+int oracle_wfa_align_mode(const char *pattern, int plen, const char *text, int tlen, int x, int o1, int e1,
+                          int o2, int e2, int singletrack, int memory_mode, int *score_out, char *ops, int ops_cap,
+                          int *n_ops) {
     *score_out = 0, *n_ops = 0;
     wo_ints_allocated = 0;
+    const int bt = memory_mode == 1 || memory_mode == 2;
+    if (bt) singletrack = 0;
+    wo_bt = bt;
+    wo_blocks B = {0, 0, 0};
     const int scope = (o1 + e1 > o2 + e2 ? o1 + e1 : o2 + e2);
     const int max_score_scope = (scope > x ? scope : x) + 1;
     int cap = 1024, s = 0, num_null = 0;
     wo_score *W = (wo_score *)calloc((size_t)cap, sizeof(wo_score));
     W[0].M = wo_new(0, 0);
     W[0].M->off[0] = 0;
+    if (bt) { /* initial BT-block: start position (0, 0), no predecessor */
+        W[0].M->pc[0] = 0;
+        W[0].M->pv[0] = wo_blk_push(&B, 0, WO_BT_NULL);
+    }
     const int k_end = tlen - plen;
     int status = 0, end_score = -1;
     for (;;) {
@@ -170,6 +243,64 @@ int oracle_wfa_align(const char *pattern, int plen, const char *text, int tlen, 
             if (oI2) oI2->off[k - lo] = ins2;
             if (oD1) oD1->off[k - lo] = del1;
             if (oD2) oD2->off[k - lo] = del2;
+            if (bt) {
+                /* each gap cell takes the extension on a tie; M prefers the mismatch, then
+                 * D2, D1, I2, I1 (the last equal candidate assigned wins) */
+                uint32_t i1pc, i1pv, i2pc, i2pv, d1pc, d1pv, d2pc, d2pv, mpc = 0, mpv = WO_BT_NULL;
+                if (wo_get(i1, k - 1) >= wo_get(m_open1, k - 1)) i1pc = wo_getpc(i1, k - 1), i1pv = wo_getpv(i1, k - 1);
+                else i1pc = wo_getpc(m_open1, k - 1), i1pv = wo_getpv(m_open1, k - 1);
+                if (wo_get(i2, k - 1) >= wo_get(m_open2, k - 1)) i2pc = wo_getpc(i2, k - 1), i2pv = wo_getpv(i2, k - 1);
+                else i2pc = wo_getpc(m_open2, k - 1), i2pv = wo_getpv(m_open2, k - 1);
+                if (wo_get(d1, k + 1) >= wo_get(m_open1, k + 1)) d1pc = wo_getpc(d1, k + 1), d1pv = wo_getpv(d1, k + 1);
+                else d1pc = wo_getpc(m_open1, k + 1), d1pv = wo_getpv(m_open1, k + 1);
+                if (wo_get(d2, k + 1) >= wo_get(m_open2, k + 1)) d2pc = wo_getpc(d2, k + 1), d2pv = wo_getpv(d2, k + 1);
+                else d2pc = wo_getpc(m_open2, k + 1), d2pv = wo_getpv(m_open2, k + 1);
+                i1pc = (i1pc << 2) | 3u, i2pc = (i2pc << 2) | 3u;
+                d1pc = (d1pc << 2) | 1u, d2pc = (d2pc << 2) | 1u;
+                const int32_t mmax = mx(mx(del1, del2), mx(misms, mx(ins1, ins2)));
+                if (mmax == ins1) mpc = i1pc, mpv = i1pv;
+                if (mmax == ins2) mpc = i2pc, mpv = i2pv;
+                if (mmax == del1) mpc = d1pc, mpv = d1pv;
+                if (mmax == del2) mpc = d2pc, mpv = d2pv;
+                if (mmax == misms) mpc = wo_getpc(m_misms, k), mpv = wo_getpv(m_misms, k);
+                oM->pc[k - lo] = (mpc << 2) | 2u, oM->pv[k - lo] = mpv;
+                if (oI1) oI1->pc[k - lo] = i1pc, oI1->pv[k - lo] = i1pv;
+                if (oI2) oI2->pc[k - lo] = i2pc, oI2->pv[k - lo] = i2pv;
+                if (oD1) oD1->pc[k - lo] = d1pc, oD1->pv[k - lo] = d1pv;
+                if (oD2) oD2->pc[k - lo] = d2pc, oD2->pv[k - lo] = d2pv;
+            }
+        }
+        if (bt) {
+            /* occupancy bound of every output (wavefront_backtrace_offload_occupation_affine) */
+            int occ_i1 = 0, occ_d1 = 0, occ_i2 = 0, occ_d2 = 0, occ_m = 0;
+            if (m_open1) occ_i1 = occ_d1 = m_open1->occ + 1;
+            if (i1 && occ_i1 < i1->occ + 1) occ_i1 = i1->occ + 1;
+            if (d1 && occ_d1 < d1->occ + 1) occ_d1 = d1->occ + 1;
+            if (m_open2) occ_i2 = occ_d2 = m_open2->occ + 1;
+            if (i2 && occ_i2 < i2->occ + 1) occ_i2 = i2->occ + 1;
+            if (d2 && occ_d2 < d2->occ + 1) occ_d2 = d2->occ + 1;
+            if (m_misms) occ_m = m_misms->occ;
+            if (occ_m < occ_i1) occ_m = occ_i1;
+            if (occ_m < occ_i2) occ_m = occ_i2;
+            if (occ_m < occ_d1) occ_m = occ_d1;
+            if (occ_m < occ_d2) occ_m = occ_d2;
+            ++occ_m;
+            oM->occ = occ_m;
+            if (oI1) oI1->occ = occ_i1;
+            if (oD1) oD1->occ = occ_d1;
+            if (oI2) oI2->occ = occ_i2;
+            if (oD2) oD2->occ = occ_d2;
+            /* offload the outputs that may fill up: medium moves half-full words and
+             * resumes at 8, low moves words of 15 or more and resumes at 14 */
+            const uint32_t mask = memory_mode == 1 ? WO_PC_HALF_FULL : WO_PC_ALMOST_FULL;
+            const int resume = memory_mode == 1 ? 8 : 14;
+            wo_wf *outs[5] = {oM, oI1, oD1, oI2, oD2};
+            for (int c = 0; c < 5; ++c) {
+                if (outs[c] && outs[c]->occ >= 15) {
+                    wo_offload(outs[c], lo, hi, mask, &B);
+                    outs[c]->occ = resume;
+                }
+            }
         }
         wo_trim(oM, plen, tlen);
         if (oI1) wo_trim(oI1, plen, tlen);
@@ -182,7 +313,56 @@ int oracle_wfa_align(const char *pattern, int plen, const char *text, int tlen, 
     const int maxops = 2 * (plen + tlen) + 8;
     char *rev = (char *)malloc((size_t)maxops);
     int n = 0;
-    if (status == 0) {
+    int fwd = 0; /* the piggyback traceback writes the operations in order */
+    if (status == 0 && bt) {
+        /* wavefront_backtrace_pcigar: collect the packed CIGARs from the end cell back to
+         * the initial block, then unpack them oldest first, extending the matches before
+         * every operation taken in M and dropping the mismatch that closes a gap */
+        const wo_wf *mw = W[end_score].M;
+        uint32_t cur_pc = mw->pc[k_end - mw->base], cur_prev = mw->pv[k_end - mw->base];
+        size_t nb = 0, cb = 64;
+        uint32_t *chain = (uint32_t *)malloc(sizeof(uint32_t) * cb);
+        while (cur_prev != WO_BT_NULL) {
+            if (nb == cb) cb *= 2, chain = (uint32_t *)realloc(chain, sizeof(uint32_t) * cb);
+            chain[nb++] = cur_pc;
+            cur_pc = B.b[cur_prev].pc, cur_prev = B.b[cur_prev].prev;
+        }
+        /* cur_pc is now the initial block's start-position record: (0, 0) end to end */
+        int v = 0, h = 0, in_m = 1;
+        for (size_t i = nb; i-- > 0;) {
+            uint32_t pc = chain[i];
+            int len = 16;
+            if (pc < WO_PC_FULL) {
+                const int free_slots = pc ? __builtin_clz(pc) / 2 : 16;
+                len -= free_slots;
+                if (len > 0) pc <<= free_slots * 2;
+            }
+            for (int j = 0; j < len; ++j) {
+                if (in_m) {
+                    const int nm = wo_lcp(pattern, plen, text, tlen, v, h);
+                    for (int t = 0; t < nm; ++t) rev[n++] = 'M';
+                    v += nm, h += nm;
+                }
+                const uint32_t op = pc >> 30;
+                pc <<= 2;
+                if (!in_m && op == 2u) {
+                    in_m = 1;
+                    continue;
+                }
+                rev[n++] = op == 1u ? 'D' : op == 2u ? 'X' : op == 3u ? 'I' : '?';
+                v += op == 1u || op == 2u;
+                h += op == 2u || op == 3u;
+                in_m = op == 2u;
+            }
+        }
+        free(chain);
+        const int nm = (plen - v) < (tlen - h) ? (plen - v) : (tlen - h);
+        for (int t = 0; t < nm; ++t) rev[n++] = 'M';
+        v += nm, h += nm;
+        while (h < tlen) rev[n++] = 'I', ++h;
+        while (v < plen) rev[n++] = 'D', ++v;
+        fwd = 1;
+    } else if (status == 0) {
         const int plen_ = plen, tlen_ = tlen;
         if (!singletrack) {
             /* wavefront_backtrace_affine: piggyback (offset<<4 | type), M=9 > D2ext=8 > ... > I1open=1 */
@@ -311,12 +491,20 @@ int oracle_wfa_align(const char *pattern, int plen, const char *text, int tlen, 
         *score_out = -end_score;
         *n_ops = n;
         if (ops && n <= ops_cap)
-            for (int i = 0; i < n; ++i) ops[i] = rev[n - 1 - i];
+            for (int i = 0; i < n; ++i) ops[i] = fwd ? rev[i] : rev[n - 1 - i];
     }
     free(rev);
+    free(B.b);
+    wo_bt = 0;
     for (int i = 0; i <= s && i < cap; ++i) {
         wo_free(W[i].M), wo_free(W[i].I1), wo_free(W[i].D1), wo_free(W[i].I2), wo_free(W[i].D2);
     }
     free(W);
     return status;
+}
+
+int oracle_wfa_align(const char *pattern, int plen, const char *text, int tlen, int x, int o1, int e1, int o2, int e2,
+                     int singletrack, int *score_out, char *ops, int ops_cap, int *n_ops) {
+    return oracle_wfa_align_mode(pattern, plen, text, tlen, x, o1, e1, o2, e2, singletrack, 0, score_out, ops, ops_cap,
+                                 n_ops);
 }

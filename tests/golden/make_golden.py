@@ -125,12 +125,26 @@ def wfa_cases():
         for stk in (False, True):
             cases.append(dict(name=name + ("-st" if stk else ""), query=q, target=t, x=4, o1=4, e1=2, o2=24,
                               e2=1, singletrack=stk))
+    # medium / low memory (piggyback traceback): long enough pairs that packed CIGARs fill
+    # and move into blocks, tie-heavy penalties, and the edge cases
+    rng2 = np.random.default_rng(4242)
+    pens = [(4, 4, 2, 24, 1), (1, 0, 1, 0, 1), (2, 3, 1, 10, 1), (6, 8, 2, 75, 1)]
+    for i in range(24):
+        L = int(np.exp(rng2.uniform(np.log(20), np.log(4000))))
+        q, t = W.divergent_pair(rng2, L, 0.005, 0.15, 4.0)
+        x, o1, e1, o2, e2 = pens[i % len(pens)]
+        cases.append(dict(name=f"wfa-mem-{i}", query=W.to_ascii(q).decode(), target=W.to_ascii(t).decode(),
+                          x=x, o1=o1, e1=e1, o2=o2, e2=e2, singletrack=False, memory_mode=1 + i % 2))
+    for name, q, t in edge:
+        for mode in (1, 2):
+            cases.append(dict(name=f"{name}-mem{mode}", query=q, target=t, x=4, o1=4, e1=2, o2=24, e2=1,
+                              singletrack=bool(mode == 2), memory_mode=mode))
     return cases
 
 
 def run_wfa(ref: oracle.Reference, c):
     st, score, ops = ref.wfa_align(c["target"].encode(), c["query"].encode(), c["x"], c["o1"], c["e1"], c["o2"],
-                                   c["e2"], singletrack=c["singletrack"])
+                                   c["e2"], singletrack=c["singletrack"], memory_mode=c.get("memory_mode", 0))
     return {"status": st, "score": score, "ops": ops}
 
 

@@ -111,3 +111,40 @@ def test_simd_variants_agree_in_full_mode(reference):
         a = reference.ksw_extd2(q.tobytes(), t.tobytes(), oracle.anchorwave_matrix(-4), 4, 2, 24, 1, variant=0)
         b = reference.ksw_extd2(q.tobytes(), t.tobytes(), oracle.anchorwave_matrix(-4), 4, 2, 24, 1, variant=1)
         assert a.key() == b.key()
+
+
+WFA_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "wfa_golden.json")
+
+
+def test_wfa_restatement_matches_golden(restatement):
+    """The WFA restatement (high memory, Singletrack, medium and low memory) against the
+    golden vectors of the compiled WFA2-lib."""
+    with open(WFA_GOLDEN) as f:
+        g = json.load(f)
+    bad = []
+    for c in g["cases"]:
+        r = restatement.wfa_align(c["target"].encode(), c["query"].encode(), c["x"], c["o1"], c["e1"], c["o2"],
+                                  c["e2"], c["singletrack"], memory_mode=c.get("memory_mode", 0))
+        if r != (c["result"]["status"], c["result"]["score"], c["result"]["ops"]):
+            bad.append(c["name"])
+    assert not bad, f"WFA restatement differs from golden on {bad}"
+    assert sum(1 for c in g["cases"] if c.get("memory_mode")) >= 24
+
+
+@pytest.mark.parametrize("memory_mode", [1, 2])
+def test_wfa_piggyback_restatement_matches_reference(restatement, reference, memory_mode):
+    """Medium / low memory (piggyback traceback) against the compiled WFA2-lib on fresh
+    seeded pairs, including tie-heavy penalties and low-complexity sequences."""
+    rng = np.random.default_rng(300 + memory_mode)
+    pens = [(4, 4, 2, 24, 1), (1, 0, 1, 0, 1), (2, 2, 1, 4, 1), (3, 0, 1, 3, 1)]
+    for i in range(120):
+        L = int(np.exp(rng.uniform(np.log(1), np.log(2500))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.3, 4.0)
+        if i % 5 == 4:  # two-letter alphabet: many equal-score paths
+            q, t = q % 2, t % 2
+        p, tx = W.to_ascii(t), W.to_ascii(q)
+        pen = pens[i % len(pens)]
+        exp = reference.wfa_align(p, tx, *pen, memory_mode=memory_mode)
+        assert restatement.wfa_align(p, tx, *pen, memory_mode=memory_mode) == exp, (i, len(p), len(tx), pen)
+        # the piggyback traceback and the high-memory traceback break ties alike
+        assert reference.wfa_align(p, tx, *pen, memory_mode=0) == exp, (i, pen)

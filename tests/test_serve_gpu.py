@@ -25,8 +25,8 @@ def _mix(seed, n):
         if rng.random() < 0.1:
             q = q.copy()
             q[rng.integers(0, len(q), 2)] = 4
-        kind = i % 5
-        method = [0, 0, 1, 2, 3][kind]
+        kind = i % 7
+        method = [0, 0, 1, 2, 3, 4, 5][kind]
         band = int(0.3 * min(len(q), len(t))) if kind == 1 else -1
         reqs.append((i, method, W.to_ascii(q), W.to_ascii(t), band))
     return reqs
@@ -39,7 +39,8 @@ def _standalone(gpu, wfa, method, q, t, band):
         tc, f2 = ksw2.encode(t)
         fn = gpu.ksw_extd2_singletrack if method == 1 else gpu.ksw_extd2
         return fn(qc, tc, oracle.anchorwave_matrix(-4), *PEN, w=band, flag=f1 | f2).key()
-    al = wfa.WfaAligner(*WPEN, singletrack=(method == 3))
+    # routes 4 / 5: medium / low memory
+    al = wfa.WfaAligner(*WPEN, singletrack=(method == 3), memory_mode=max(0, method - 3))
     st = al.align(t, q)
     ops, score = al.cigar() if st == 0 else ("", 0)
     al.close()

@@ -21,17 +21,20 @@ def _wfa():
 def test_wfa_golden_single_calls(gpu):
     wfa = _wfa()
     g = json.load(open(GOLDEN))
-    als = {}
-    bad = []
+    groups = {}
     for c in g["cases"]:
-        key = (c["x"], c["o1"], c["e1"], c["o2"], c["e2"], c["singletrack"])
-        if key not in als:
-            als[key] = wfa.WfaAligner(*key)
-        al = als[key]
-        st = al.align(c["target"].encode(), c["query"].encode())
-        ops, score = al.cigar() if st == 0 else ("", 0)
-        if (st, score, ops) != (c["result"]["status"], c["result"]["score"], c["result"]["ops"]):
-            bad.append(c["name"])
+        key = (c["x"], c["o1"], c["e1"], c["o2"], c["e2"], c["singletrack"], c.get("memory_mode", 0))
+        groups.setdefault(key, []).append(c)
+    bad = []
+    # one aligner at a time: each takes its wavefront pool from the free device memory
+    for key, cases in groups.items():
+        al = wfa.WfaAligner(*key[:6], memory_mode=key[6])
+        for c in cases:
+            st = al.align(c["target"].encode(), c["query"].encode())
+            ops, score = al.cigar() if st == 0 else ("", 0)
+            if (st, score, ops) != (c["result"]["status"], c["result"]["score"], c["result"]["ops"]):
+                bad.append(c["name"])
+        al.close()
     assert not bad, bad
 
 
@@ -147,3 +150,108 @@ def test_align_with_wfa_mirror(gpu, restatement):
     o = restatement.wfa_align(ts.encode(), qs.encode(), 4, 4, 2, 24, 1, False)
     assert st == 0 and score == o[1]
     assert aq.replace("-", "") == qs and ar.replace("-", "") == ts
+
+
+@pytest.mark.parametrize("memory_mode", [1, 2])
+@pytest.mark.parametrize("pen", [(4, 4, 2, 24, 1), (1, 0, 1, 0, 1), (2, 3, 1, 10, 1)])
+def test_wfa_piggyback_batch_vs_oracle(gpu, restatement, pen, memory_mode):
+    """Medium / low memory: ring of recent scores plus packed-CIGAR blocks on the device,
+    bit-exact with the piggyback restatement (which follows the reference's offload rules;
+    the device moves a cell's packed CIGAR into a block at 15 operations instead)."""
+    wfa = _wfa()
+    rng = np.random.default_rng(500 + sum(pen) + memory_mode)
+    ps, ts = [], []
+    for i in range(120):
+        L = int(np.exp(rng.uniform(np.log(1), np.log(4000))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.15, 4.0)
+        if i % 6 == 5:
+            q, t = q % 2, t % 2  # two-letter alphabet: many equal-score paths
+        if rng.random() < 0.1:
+            q = q.copy()
+            q[rng.integers(0, len(q), 3)] = 4
+        ps.append(W.to_ascii(t))
+        ts.append(W.to_ascii(q))
+    ps.append(b""), ts.append(b"ACGT")
+    ps.append(b"ACGTA"), ts.append(b"")
+    al = wfa.WfaAligner(*pen, memory_mode=memory_mode)
+    res, _ = al.align_batch(ps, ts)
+    al.close()
+    for p, t, r in zip(ps, ts, res):
+        assert r == restatement.wfa_align(p, t, *pen, memory_mode=memory_mode), (len(p), len(t))
+
+
+def test_wfa_piggyback_workload_subset_vs_reference(gpu):
+    """512 pairs of the 100 bp-10 kb workload in medium and low memory against the compiled
+    WFA2-lib in the same modes, and against the device's high-memory results."""
+    wfa = _wfa()
+    try:
+        ref = oracle.Reference()
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    ps = W.batched_wfa_set(512, seed=3)
+    pats = [W.to_ascii(t) for t in ps.targets]
+    txts = [W.to_ascii(q) for q in ps.queries]
+    hi = wfa.WfaAligner(4, 4, 2, 24, 1)
+    exp, _ = hi.align_batch(pats, txts)
+    hi.close()
+    for mode in (1, 2):
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, memory_mode=mode)
+        res, _ = al.align_batch(pats, txts)
+        al.close()
+        assert res == exp
+        for i in range(0, 512, 11):
+            assert res[i] == ref.wfa_align(pats[i], txts[i], 4, 4, 2, 24, 1, memory_mode=mode), (mode, i)
+
+
+def test_wfa_piggyback_uses_less_memory(gpu):
+    """Long pairs: the piggyback modes take a fraction of the high-memory mode's device
+    memory per alignment (ring of the last scores plus blocks, instead of every wavefront)."""
+    wfa = _wfa()
+    rng = np.random.default_rng(77)
+    ps, ts = [], []
+    for _ in range(32):
+        q, t = W.divergent_pair(rng, 8000, 0.04, 0.05, 4.0)
+        ps.append(W.to_ascii(t))
+        ts.append(W.to_ascii(q))
+    use = {}
+    out = {}
+    for mode in (0, 1):
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, memory_mode=mode)
+        out[mode], _ = al.align_batch(ps, ts)
+        use[mode] = al.memory()
+        al.close()
+    assert out[0] == out[1]
+    assert all(r[0] == 0 for r in out[1])
+    # 8 kb pairs at 4-5%: about 2.7x less (the ring and the blocks each take about an
+    # eighth of what keeping every wavefront takes, plus allocation granularity)
+    assert use[1][0] * 2 < use[0][0], use
+    assert use[1][1] * 2 < use[0][1], use
+
+
+def test_wfa_piggyback_pool_retry_rounds(gpu, restatement):
+    """A small pool forces retry rounds in the piggyback mode too; results unchanged."""
+    wfa = _wfa()
+    rng = np.random.default_rng(98)
+    ps, ts = [], []
+    for _ in range(40):
+        q, t = W.divergent_pair(rng, int(rng.integers(500, 4000)), 0.02, 0.08, 4.0)
+        ps.append(W.to_ascii(t))
+        ts.append(W.to_ascii(q))
+    al = wfa.WfaAligner(4, 4, 2, 24, 1, max_memory_abort=8 << 20, memory_mode=2)
+    res, _ = al.align_batch(ps, ts)
+    al.close()
+    for p, t, r in zip(ps, ts, res):
+        exp = restatement.wfa_align(p, t, 4, 4, 2, 24, 1, False, memory_mode=2)
+        assert r == exp or r[0] == -200
+
+
+def test_align_with_medium_and_low_wfa(gpu, restatement):
+    wfa = _wfa()
+    rng = np.random.default_rng(2)
+    q, t = W.divergent_pair(rng, 1500, 0.05, 0.05, 4.0)
+    qs, ts = W.to_ascii(q).decode(), W.to_ascii(t).decode()
+    for fn, mode in ((wfa.align_with_medium_wfa, 1), (wfa.align_with_low_wfa, 2)):
+        st, score, aq, ar = fn(qs, ts, -4, -4, -2, -24, -1)
+        o = restatement.wfa_align(ts.encode(), qs.encode(), 4, 4, 2, 24, 1, False, memory_mode=mode)
+        assert st == 0 and score == o[1]
+        assert aq.replace("-", "") == qs and ar.replace("-", "") == ts
