@@ -60,6 +60,8 @@ struct Alloc {
 constexpr uint32_t PC_ALMOST_FULL = 0x10000000u;  // 15 operations or more
 constexpr uint32_t BT_NULL = 0xFFFFFFFFu;          // no earlier block
 constexpr int PIG_ARRAYS = 15;                     // 5 components x (offsets, pcigar, link)
+constexpr int PIG_U = 2;                           // diagonals per lane in flight
+constexpr uint32_t LANE_BLOCKS = 32;               // blocks a lane reserves at a time
 
 __device__ __forceinline__ int64_t pool_grab(const WfaArgs &A, int64_t bytes) {
     const unsigned long long b = atomicAdd(A.pool_head, (unsigned long long)bytes);
@@ -202,6 +204,7 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
         int64_t *ctab = A.ctab + PR.ctab_off;
         Alloc al{0, 0, true, 0};
+        uint32_t bnext = 0, bend = 0;  // this lane's reserved piggyback blocks
         int status = 0, end_score = -1;
         // piggyback ring: SR slots x 15 arrays x rcap elements; grows by reallocation
         const int SR = A.max_score_scope;
@@ -429,14 +432,14 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
 #pragma unroll
             for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
             if constexpr (PIG) {
-                // two diagonals per lane at a time; each gap cell takes the extension on a
-                // tie, M the mismatch, then D2, D1, I2, I1 (the kernel's assignment order).
-                // Every lane runs every trip (the block allocation below is warp-wide).
-                for (int kb = lo; kb <= hi; kb += 64) {
+                // PIG_U diagonals per lane at a time; each gap cell takes the extension on
+                // a tie, M the mismatch, then D2, D1, I2, I1 (the kernel's assignment order).
+                // Every lane runs every trip (the block reservation below is warp-wide).
+                for (int kb = lo; kb <= hi; kb += 32 * PIG_U) {
                     const int k0 = kb + lane;
-                    Cell C[2][5];
+                    Cell C[PIG_U][5];
 #pragma unroll
-                    for (int u = 0; u < 2; ++u) {
+                    for (int u = 0; u < PIG_U; ++u) {
                         const int k = k0 + 32 * u;
                         Cell a = getc(A, m_open1, k - 1), b = getc(A, i1, k - 1);
                         Cell g = b.o >= a.o ? b : a;
@@ -460,44 +463,44 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                                                                 : C[u][CI1];
                         C[u][CM] = Cell{in_matrix(best, k, plen, tlen) ? best : WF_NULL, (src.pc << 2) | 2u, src.pv};
                     }
-                    // cells whose packed CIGAR holds 15 operations move it into a block;
-                    // the warp takes its blocks in one allocation (lane order)
+                    // cells whose packed CIGAR holds 15 operations move it into a block,
+                    // taken from the lane's reserved run; lanes whose run is short reserve
+                    // LANE_BLOCKS more in one warp allocation
                     uint32_t fl = 0;
 #pragma unroll
-                    for (int u = 0; u < 2; ++u) {
+                    for (int u = 0; u < PIG_U; ++u) {
                         const int k = k0 + 32 * u;
 #pragma unroll
                         for (int c = 0; c < 5; ++c)
                             if (k <= hi && alloc_c[c] && C[u][c].pc >= PC_ALMOST_FULL && in_matrix(C[u][c].o, k, plen, tlen))
                                 fl |= 1u << (u * 5 + c);
                     }
-                    const int cnt = __popc(fl);
-                    int incl = cnt;
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const int t = __shfl_up_sync(0xffffffffu, incl, d);
-                        if (lane >= d) incl += t;
-                    }
-                    const int total = __shfl_sync(0xffffffffu, incl, 31);
-                    if (total > 0) {
-                        const int64_t bb = warp_alloc(A, al, (int64_t)total * 8, lane);
+                    const bool refill = bend - bnext < (uint32_t)__popc(fl);
+                    const unsigned rb = __ballot_sync(0xffffffffu, refill);
+                    if (rb) {
+                        const int64_t bb = warp_alloc(A, al, (int64_t)__popc(rb) * LANE_BLOCKS * 8, lane);
                         if (bb < 0) {
                             status = WFA_RETRY;
                             break;
                         }
-                        uint32_t idx = (uint32_t)(bb >> 3) + (uint32_t)(incl - cnt);
+                        if (refill) {
+                            bnext = (uint32_t)(bb >> 3) + (uint32_t)__popc(rb & ((1u << lane) - 1u)) * LANE_BLOCKS;
+                            bend = bnext + LANE_BLOCKS;
+                        }
+                    }
+                    if (fl) {
                         uint2 *blk = (uint2 *)A.pool;
 #pragma unroll
-                        for (int u = 0; u < 2; ++u)
+                        for (int u = 0; u < PIG_U; ++u)
 #pragma unroll
                             for (int c = 0; c < 5; ++c)
                                 if (fl & (1u << (u * 5 + c))) {
-                                    blk[idx] = make_uint2(C[u][c].pc, C[u][c].pv);
-                                    C[u][c].pc = 0u, C[u][c].pv = idx++;
+                                    blk[bnext] = make_uint2(C[u][c].pc, C[u][c].pv);
+                                    C[u][c].pc = 0u, C[u][c].pv = bnext++;
                                 }
                     }
 #pragma unroll
-                    for (int u = 0; u < 2; ++u) {
+                    for (int u = 0; u < PIG_U; ++u) {
                         const int k = k0 + 32 * u;
                         if (k > hi) break;
 #pragma unroll

@@ -283,9 +283,10 @@ def serving_measurement(nreq: int, rank: int):
 
 def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
     """The batched gap-affine-2p WFA workload (lengths log-uniform 100 bp-10 kb, divergence
-    0.5-5%, penalties x=4, o1=4, e1=2, o2=24, e2=1), standard and Singletrack: pairs/s on the
-    device and through the C call with host buffers, and the reference's WFA2 code on the host
-    cores on the same pairs (scores and CIGAR lengths compared)."""
+    0.5-5%, penalties x=4, o1=4, e1=2, o2=24, e2=1), standard and Singletrack in high memory
+    and the medium-memory (piggyback) mode: pairs/s on the device and through the C call with
+    host buffers, device memory per alignment, and the reference's WFA2 code in the same mode
+    on the host cores on the same pairs (scores and CIGAR lengths compared)."""
     import numpy as np
 
     from anchorwave_b200 import wfa
@@ -295,17 +296,21 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
     txts = [W.to_ascii(q) for q in ps.queries]
     out = {"workload": ps.name, "pairs": len(ps), "matrix_cells": ps.cells()}
     dev = {}
-    for name, stk in (("standard", False), ("singletrack", True)):
-        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=stk, max_memory_abort=int(pool_gb * 2**30))
+    modes = (("standard", False, 0), ("singletrack", True, 0), ("medium", False, 1))
+    for name, stk, mem in modes:
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=stk, max_memory_abort=int(pool_gb * 2**30),
+                            memory_mode=mem)
         al.align_batch_raw(pats[:64], txts[:64])
         runs = [al.align_batch_raw(pats, txts) for _ in range(2)]
+        pair_max, total = al.memory()
         al.close()
         st, sc, offs, nops, ops, ms, secs = min(runs, key=lambda r: r[5])
         dev[name] = (st, sc, nops)
         out[name] = {"device_ms": ms, "pairs_per_s": len(ps) / (ms * 1e-3),
                      "e2e_pairs_per_s": len(ps) / min(r[6] for r in runs),
                      "gcups_equivalent": ps.cells() / (ms * 1e-3) / 1e9,
-                     "completed": int(np.sum(st == 0))}
+                     "completed": int(np.sum(st == 0)),
+                     "device_bytes_per_pair_mean": total / len(ps), "device_bytes_pair_max": pair_max}
     if cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
@@ -314,9 +319,9 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
         except FileNotFoundError as e:
             out["cpu_reference"] = {"unavailable": str(e)}
             return out
-        for name, stk in (("standard", False), ("singletrack", True)):
+        for name, stk, mem in modes:
             # the helper takes (queries, targets) and aligns pattern = target, text = query
-            r = ref.wfa_batch(txts, pats, 4, 4, 2, 24, 1, singletrack=stk, time_budget_s=10.0)
+            r = ref.wfa_batch(txts, pats, 4, 4, 2, 24, 1, singletrack=stk, time_budget_s=10.0, memory_mode=mem)
             done = [i for i in range(len(ps)) if r["n_ops"][i] > 0]
             st, sc, nops = dev[name]
             same = all(st[i] == 0 and sc[i] == r["score"][i] and nops[i] == r["n_ops"][i] for i in done)

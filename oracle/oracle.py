@@ -170,7 +170,7 @@ class Reference:
         L.awref_wfa_batch.restype = C.c_double
         L.awref_wfa_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                      C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+                                      C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
         assert L.awref_sizeof_extz() == C.sizeof(KswExtz)
 
     def ksw_extd2(self, query: bytes, target: bytes, mat, q, e, q2, e2, w=-1, zdrop=-1, end_bonus=0,
@@ -218,7 +218,7 @@ class Reference:
                 "threads": nthreads}
 
     def wfa_batch(self, queries, targets, x, o1, e1, o2, e2, singletrack=False, nthreads=None,
-                  time_budget_s=0.0):
+                  time_budget_s=0.0, memory_mode=0):
         """Threaded batch over the reference wavefront_align (ASCII sequences)."""
         import numpy as np
         nthreads = nthreads or os.cpu_count() or 1
@@ -237,7 +237,8 @@ class Reference:
         done = C.c_int(0)
         secs = self.lib.awref_wfa_batch(n, ql.ctypes.data, qoff.ctypes.data, qbuf.ctypes.data, tl.ctypes.data,
                                         toff.ctypes.data, tbuf.ctypes.data, x, o1, e1, o2, e2,
-                                        int(bool(singletrack)), nthreads, time_budget_s, score.ctypes.data,
+                                        int(bool(singletrack)), int(memory_mode), nthreads, time_budget_s,
+                                        score.ctypes.data,
                                         nops.ctypes.data, C.byref(done))
         return {"score": score[:n], "n_ops": nops[:n], "seconds": secs, "done": done.value, "threads": nthreads}
 

@@ -163,7 +163,7 @@ typedef struct {
     const uint8_t *qbuf, *tbuf;
     const int8_t *mat;
     int q, e, q2, e2, w, flag, variant;
-    int wfa_x, wfa_o1, wfa_e1, wfa_o2, wfa_e2, wfa_singletrack;
+    int wfa_x, wfa_o1, wfa_e1, wfa_o2, wfa_e2, wfa_singletrack, wfa_memory_mode;
     int32_t *score_out, *ncig_out;
     uint64_t *hash_out;
     double deadline;          /* CLOCK_MONOTONIC seconds; <= 0 disables */
@@ -200,7 +200,7 @@ static void *awref_batch_worker(void *arg) {
             free(ez.cigar);
         } else {
             if (!al) al = awref_wfa_new(b->wfa_x, b->wfa_o1, b->wfa_e1, b->wfa_o2,
-                                        b->wfa_e2, b->wfa_singletrack, 0);
+                                        b->wfa_e2, b->wfa_singletrack, b->wfa_memory_mode);
             int need = b->qlen[i] + b->tlen[i] + 8;
             if (need > ops_cap) { free(ops); ops_cap = need; ops = (char *)malloc((size_t)ops_cap); }
             int sc = 0, nops = 0;
@@ -248,17 +248,18 @@ double awref_ksw_batch(int n, const int *qlen, const int64_t *qoff, const uint8_
 }
 
 /* WFA over a pair list (ASCII sequences; pattern = target/reference, text =
- * query), one thread-local standard or Singletrack aligner per worker. */
+ * query), one thread-local aligner per worker (standard or Singletrack in high
+ * memory, or the medium / low piggyback modes). */
 double awref_wfa_batch(int n, const int *qlen, const int64_t *qoff, const uint8_t *qbuf,
                        const int *tlen, const int64_t *toff, const uint8_t *tbuf,
-                       int x, int o1, int e1, int o2, int e2, int singletrack,
+                       int x, int o1, int e1, int o2, int e2, int singletrack, int memory_mode,
                        int nthreads, double time_budget_s,
                        int32_t *score_out, int32_t *nops_out, int *n_done) {
     awref_batch_t b;
     memset(&b, 0, sizeof(b));
     b.kind = 1; b.n = n; b.qlen = qlen; b.tlen = tlen; b.qoff = qoff; b.toff = toff;
     b.qbuf = qbuf; b.tbuf = tbuf; b.wfa_x = x; b.wfa_o1 = o1; b.wfa_e1 = e1;
-    b.wfa_o2 = o2; b.wfa_e2 = e2; b.wfa_singletrack = singletrack;
+    b.wfa_o2 = o2; b.wfa_e2 = e2; b.wfa_singletrack = singletrack; b.wfa_memory_mode = memory_mode;
     b.score_out = score_out; b.ncig_out = nops_out;
     b.deadline = time_budget_s > 0 ? awref_now() + time_budget_s : 0;
     return awref_run_batch(&b, nthreads, n_done);
