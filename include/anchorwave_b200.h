@@ -155,6 +155,32 @@ int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const cha
  * WfaAlignment.cpp:353-354): the largest single alignment and the sum over the call. */
 int wavefront_gpu_memory(const wavefront_aligner_gpu_t *aligner, int64_t *pair_max, int64_t *total);
 
+/* ---- selector sequence summary ------------------------------------------------- */
+
+/* One sequence of summarizeSequencePair (src/myImportandFunction/
+ * AlignmentAlgorithmSelector.cpp:180-191, :730-757): FNV-1a fingerprint, the fraction of
+ * bases other than A/C/G/T, the mean normalized entropy of 64-base blocks, the fraction
+ * of bases at run length >= 4, and the k = 9, 15, 21 sketches (hash, start position;
+ * position order, at most 4 entries per hash) at sketch_offset[s], sketch_count[s]
+ * entries, in the arrays of aw_sequence_summary_sketches. */
+typedef struct {
+    uint64_t fingerprint;
+    double ambiguous_fraction, normalized_entropy, low_complexity_fraction;
+    int64_t sketch_offset[3];
+    int64_t sketch_count[3];
+} aw_sequence_summary_t;
+
+/* Replaces summarizeSequencePair for n interval pairs on the device: out[2i] = query i,
+ * out[2i+1] = reference i, identical[i] = the two are equal.  modulos: n x 3 sampling
+ * modulos, or NULL for those of makeAlignmentSelectionPlan (:1752-1760).  The sketches
+ * stay with the calling thread until its next call.  Returns 0 or a negative AW_E_*. */
+int aw_sequence_summary_batch(int n, const char *const *query, const int64_t *qlen,
+                              const char *const *reference, const int64_t *rlen,
+                              const uint64_t *modulos, aw_sequence_summary_t *out, int *identical);
+/* Copies the calling thread's last sketches (capacity entries at least; hash and position
+ * both NULL: returns the number of entries only).  Returns the number of entries. */
+int64_t aw_sequence_summary_sketches(uint64_t *hash, uint32_t *position, int64_t capacity);
+
 /* ---- serving loop (continuous batching) --------------------------------------- */
 
 /* Engine of a request, as chosen by AnchorWave's exact-tier / fallback-tier selector

@@ -1,7 +1,8 @@
 """TEST INFRASTRUCTURE (oracle) -- ctypes front end of the two CPU oracles.
 
-* ``Restatement``: ``liboracle.so`` built from ``ksw2_oracle.c`` / ``wfa_oracle.c``,
-  the plain-C restatement of the reference algorithms (always available).
+* ``Restatement``: ``liboracle.so`` built from ``ksw2_oracle.c`` / ``wfa_oracle.c`` /
+  ``summary_oracle.c``, the plain-C restatement of the reference algorithms (always
+  available).
 * ``Reference``: ``_ref/libawref_<isa>.so``, AnchorWave's own KSW2 / WFA2 sources
   compiled from the reference tree by ``oracle/Makefile`` (present wherever it was
   built; it travels with the repository snapshot).
@@ -37,6 +38,43 @@ class KswExtz(C.Structure):
                 ("mte", C.c_int), ("mte_q", C.c_int), ("score", C.c_int),
                 ("m_cigar", C.c_int), ("n_cigar", C.c_int), ("reach_end", C.c_int),
                 ("stopped", C.c_int), ("cigar", C.POINTER(C.c_uint32))]
+
+
+class SummaryOut(C.Structure):
+    """One sequence of summarizeSequencePair (AlignmentAlgorithmSelector.cpp:180-191)."""
+    _fields_ = [("fingerprint", C.c_uint64), ("ambiguous_fraction", C.c_double),
+                ("normalized_entropy", C.c_double), ("low_complexity_fraction", C.c_double),
+                ("count", C.c_int64 * 3)]
+
+
+def _summary_call(fn, query: bytes, reference: bytes, modulos=None):
+    """Runs a summarizeSequencePair front end: returns (identical, [query, reference]) with
+    each side {fingerprint, fractions, sketches: [[(hash, pos)...] per k=9, 15, 21]}."""
+    import numpy as np
+    out = (SummaryOut * 2)()
+    ident = C.c_int(0)
+    mod = (C.c_uint64 * 3)(*modulos) if modulos is not None else None
+    n = fn(query, len(query), reference, len(reference), mod, out, C.byref(ident), None, None, 0)
+    h = np.zeros(max(n, 1), dtype=np.uint64)
+    p = np.zeros(max(n, 1), dtype=np.uint32)
+    fn(query, len(query), reference, len(reference), mod, out, C.byref(ident), h.ctypes.data, p.ctypes.data, n)
+    sides, w = [], 0
+    for t in range(2):
+        sk = []
+        for sc in range(3):
+            c = int(out[t].count[sc])
+            sk.append(list(zip(h[w:w + c].tolist(), p[w:w + c].tolist())))
+            w += c
+        sides.append({"fingerprint": int(out[t].fingerprint), "ambiguous_fraction": out[t].ambiguous_fraction,
+                      "normalized_entropy": out[t].normalized_entropy,
+                      "low_complexity_fraction": out[t].low_complexity_fraction, "sketches": sk})
+    return bool(ident.value), sides
+
+
+def _summary_argtypes(fn):
+    fn.argtypes = [C.c_char_p, C.c_int64, C.c_char_p, C.c_int64, C.c_void_p, C.c_void_p, C.POINTER(C.c_int),
+                   C.c_void_p, C.c_void_p, C.c_int64]
+    fn.restype = C.c_int64
 
 
 @dataclass
@@ -118,6 +156,8 @@ class Restatement:
             L.oracle_wfa_align.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int,
                                            C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
                                            C.c_char_p, C.c_int, C.POINTER(C.c_int)]
+            _summary_argtypes(L.oracle_sequence_summary)
+            assert L.oracle_sizeof_summary() == C.sizeof(SummaryOut)
             L.oracle_wfa_align_mode.argtypes = [C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int,
                                                 C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
                                                 C.c_char_p, C.c_int, C.POINTER(C.c_int)]
@@ -129,6 +169,10 @@ class Restatement:
                                   q, e, q2, e2, w, zdrop, end_bonus, flag, stop_interval, stop_at,
                                   C.byref(ez))
         return extz_to_result(ez, self.lib.oracle_free)
+
+    def sequence_summary(self, query: bytes, reference: bytes, modulos=None):
+        """summarizeSequencePair restated (summary_oracle.c)."""
+        return _summary_call(self.lib.oracle_sequence_summary, query, reference, modulos)
 
     def wfa_align(self, pattern: bytes, text: bytes, x, o1, e1, o2, e2, singletrack=False, memory_mode=0):
         """memory_mode as WFA2-lib's wavefront_memory_t: 0 high, 1 medium, 2 low (piggyback)."""
@@ -172,6 +216,13 @@ class Reference:
                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
         assert L.awref_sizeof_extz() == C.sizeof(KswExtz)
+        self.has_summary = hasattr(L, "awref_sequence_summary")
+        if self.has_summary:
+            _summary_argtypes(L.awref_sequence_summary)
+            assert L.awref_sizeof_summary() == C.sizeof(SummaryOut)
+            L.awref_sequence_summary_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                       C.c_void_p, C.c_void_p, C.c_int]
+            L.awref_sequence_summary_batch.restype = C.c_double
 
     def ksw_extd2(self, query: bytes, target: bytes, mat, q, e, q2, e2, w=-1, zdrop=-1, end_bonus=0,
                   flag=0, m=5, variant=0, stop_interval=0, stop_at=-1) -> KswResult:
@@ -241,6 +292,27 @@ class Reference:
                                         score.ctypes.data,
                                         nops.ctypes.data, C.byref(done))
         return {"score": score[:n], "n_ops": nops[:n], "seconds": secs, "done": done.value, "threads": nthreads}
+
+    def sequence_summary(self, query: bytes, reference: bytes, modulos=None):
+        """The compiled selector's summarizeSequencePair (ref_selector_shim.cpp)."""
+        return _summary_call(self.lib.awref_sequence_summary, query, reference, modulos)
+
+    def sequence_summary_batch(self, queries, references, nthreads=None):
+        """n pairs on the host threads: (seconds, summaries array [n, 2], identical flags)."""
+        import numpy as np
+        nthreads = nthreads or os.cpu_count() or 1
+        n = len(queries)
+        qb = [C.create_string_buffer(q, len(q) + 1) for q in queries]
+        rb = [C.create_string_buffer(r, len(r) + 1) for r in references]
+        qp = (C.c_void_p * n)(*[C.addressof(b) for b in qb])
+        rp = (C.c_void_p * n)(*[C.addressof(b) for b in rb])
+        ql = np.array([len(q) for q in queries], dtype=np.int64)
+        rl = np.array([len(r) for r in references], dtype=np.int64)
+        out = (SummaryOut * (2 * n))()
+        ident = np.zeros(n, dtype=np.int32)
+        secs = self.lib.awref_sequence_summary_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, out,
+                                                     ident.ctypes.data, nthreads)
+        return secs, out, ident
 
     def wfa_align(self, pattern: bytes, text: bytes, x, o1, e1, o2, e2, singletrack=False, memory_mode=0):
         score = C.c_int(0)

@@ -148,6 +148,52 @@ def run_wfa(ref: oracle.Reference, c):
     return {"status": st, "score": score, "ops": ops}
 
 
+def summary_cases():
+    """Interval pairs for the selector's sequence pass (summarizeSequencePair)."""
+    rng = np.random.default_rng(9090)
+    cases = []
+    for i in range(20):
+        L = int(np.exp(rng.uniform(np.log(10), np.log(6000))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.2, 4.0)
+        qa, ta = bytearray(W.to_ascii(q)), bytearray(W.to_ascii(t))
+        if i % 4 == 1:
+            for j in rng.integers(0, max(1, len(qa)), 5):
+                if len(qa):
+                    qa[j] = ord("N")
+        if i % 4 == 2:
+            for j in rng.integers(0, max(1, len(ta)), 40):
+                if len(ta):
+                    ta[j] = ord(chr(ta[j]).lower())  # lowercase counts as the same base
+        cases.append(dict(name=f"sum-{i}", query=qa.decode(), target=ta.decode()))
+    rnd = W.to_ascii(W.random_dna(rng, 3000)).decode()
+    edge = [("sum-empty", "", ""), ("sum-empty-query", "", "ACGTACGTAC"), ("sum-len1", "A", "C"),
+            ("sum-len9", "ACGTACGTA", "ACGTACGTA"), ("sum-len21", "ACGTTGCAACGTTGCAACGTA", "ACGTTGCAACGTTGCAACGTT"),
+            ("sum-polyA", "A" * 5000, "A" * 4990), ("sum-N-runs", ("ACGTN" * 7 + "NNNN" + "ACGT" * 10) * 20, rnd[:900]),
+            ("sum-identical", rnd, rnd), ("sum-dinucleotide", "AC" * 2000, "CA" * 2000),
+            ("sum-iupac", "ACGTRYKMSWBDHVN" * 100, "acgtrykmswbdhvn" * 100)]
+    for name, q, t in edge:
+        cases.append(dict(name=name, query=q, target=t))
+    return cases
+
+
+def sketch_digest(side):
+    import hashlib
+    h = hashlib.sha256()
+    for sk in side["sketches"]:
+        for hv, pos in sk:
+            h.update(int(hv).to_bytes(8, "little") + int(pos).to_bytes(4, "little"))
+    return h.hexdigest()
+
+
+def run_summary(ref: oracle.Reference, c):
+    ident, sides = ref.sequence_summary(c["query"].encode(), c["target"].encode())
+    return {"identical": ident,
+            "sides": [{"fingerprint": s["fingerprint"], "ambiguous_fraction": s["ambiguous_fraction"],
+                       "normalized_entropy": s["normalized_entropy"],
+                       "low_complexity_fraction": s["low_complexity_fraction"],
+                       "counts": [len(k) for k in s["sketches"]], "digest": sketch_digest(s)} for s in sides]}
+
+
 def main():
     ref = oracle.Reference()
     ks = ksw_cases()
@@ -162,7 +208,13 @@ def main():
     with open(os.path.join(HERE, "wfa_golden.json"), "w") as f:
         json.dump({"generator": "tests/golden/make_golden.py", "reference_isa": ref.isa, "cases": wc}, f,
                   separators=(",", ":"))
-    print(f"wrote {len(ks)} KSW2 and {len(wc)} WFA golden cases (reference ISA {ref.isa})")
+    sc = summary_cases()
+    for c in sc:
+        c["result"] = run_summary(ref, c)
+    with open(os.path.join(HERE, "summary_golden.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": sc}, f, separators=(",", ":"))
+    print(f"wrote {len(ks)} KSW2, {len(wc)} WFA and {len(sc)} selector-summary golden cases "
+          f"(reference ISA {ref.isa})")
 
 
 if __name__ == "__main__":

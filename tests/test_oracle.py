@@ -148,3 +148,62 @@ def test_wfa_piggyback_restatement_matches_reference(restatement, reference, mem
         assert restatement.wfa_align(p, tx, *pen, memory_mode=memory_mode) == exp, (i, len(p), len(tx), pen)
         # the piggyback traceback and the high-memory traceback break ties alike
         assert reference.wfa_align(p, tx, *pen, memory_mode=0) == exp, (i, pen)
+
+
+SUMMARY_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "summary_golden.json")
+
+
+def summary_matches(got, exp, entropy_rel=1e-12):
+    """A summarizeSequencePair result against a golden record: identity, fingerprints,
+    sketch counts and digest, and the fractions (entropy within entropy_rel)."""
+    from golden.make_golden import sketch_digest
+    ident, sides = got
+    if ident != exp["identical"]:
+        return False
+    for s, e in zip(sides, exp["sides"]):
+        if s["fingerprint"] != e["fingerprint"] or [len(k) for k in s["sketches"]] != e["counts"]:
+            return False
+        if sketch_digest(s) != e["digest"]:
+            return False
+        if s["ambiguous_fraction"] != e["ambiguous_fraction"]:
+            return False
+        if s["low_complexity_fraction"] != e["low_complexity_fraction"]:
+            return False
+        if abs(s["normalized_entropy"] - e["normalized_entropy"]) > entropy_rel * max(1.0, e["normalized_entropy"]):
+            return False
+    return True
+
+
+def test_summary_restatement_matches_golden(restatement):
+    """The selector's sequence pass restated (summary_oracle.c) against the golden records
+    of the compiled selector."""
+    with open(SUMMARY_GOLDEN) as f:
+        g = json.load(f)
+    bad = [c["name"] for c in g["cases"]
+           if not summary_matches(restatement.sequence_summary(c["query"].encode(), c["target"].encode()),
+                                  c["result"])]
+    assert not bad, bad
+
+
+def test_summary_restatement_matches_reference(restatement, reference):
+    if not reference.has_summary:
+        pytest.skip("compiled reference without the selector shim")
+    rng = np.random.default_rng(61)
+    for i in range(40):
+        L = int(np.exp(rng.uniform(np.log(1), np.log(20000))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.3, 4.0)
+        qa, ta = bytearray(W.to_ascii(q)), bytearray(W.to_ascii(t))
+        if i % 3 == 0 and len(qa):
+            for j in rng.integers(0, len(qa), 7):
+                qa[j] = ord("N")
+        if i % 5 == 0:  # low complexity
+            qa = bytearray(b"AAAAAAAAAAAAAAAACCCCCCCCCCG" * (len(qa) // 27 + 1))
+        mods = None if i % 2 else [int(x) for x in rng.integers(1, 9, 3)]
+        a = restatement.sequence_summary(bytes(qa), bytes(ta), mods)
+        b = reference.sequence_summary(bytes(qa), bytes(ta), mods)
+        assert a[0] == b[0]
+        for x, y in zip(a[1], b[1]):
+            assert x["sketches"] == y["sketches"] and x["fingerprint"] == y["fingerprint"], i
+            assert x["ambiguous_fraction"] == y["ambiguous_fraction"], i
+            assert x["low_complexity_fraction"] == y["low_complexity_fraction"], i
+            assert abs(x["normalized_entropy"] - y["normalized_entropy"]) <= 1e-12, i
