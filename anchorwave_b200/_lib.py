@@ -31,7 +31,7 @@ EXPORTS = [
     "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc", "aw_cigar_rows_batch",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
     "wavefront_align_batch_gpu", "wavefront_gpu_memory", "aw_sequence_summary_batch",
-    "aw_sequence_summary_sketches", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
+    "aw_sequence_summary_sketches", "aw_sequence_summary_sketch_view", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
     "aw_serve_result_free", "aw_serve_close",
 ]
 
@@ -128,10 +128,12 @@ def _load(path: str = LIB_PATH):
     lib.wavefront_align_batch_gpu.restype = i32
     lib.wavefront_gpu_memory.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     lib.wavefront_gpu_memory.restype = i32
-    lib.aw_sequence_summary_batch.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp]
+    lib.aw_sequence_summary_batch.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, C.POINTER(C.c_float)]
     lib.aw_sequence_summary_batch.restype = i32
     lib.aw_sequence_summary_sketches.argtypes = [vp, vp, i64]
     lib.aw_sequence_summary_sketches.restype = i64
+    lib.aw_sequence_summary_sketch_view.argtypes = [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    lib.aw_sequence_summary_sketch_view.restype = i64
     lib.aw_serve_open.argtypes = [C.POINTER(ServeConfig)]
     lib.aw_serve_open.restype = vp
     lib.aw_serve_submit.argtypes = [vp, C.c_uint64, i32, i32, C.c_char_p, i32, C.c_char_p, i32]

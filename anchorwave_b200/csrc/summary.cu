@@ -341,6 +341,7 @@ __global__ void gather_kernel(const SegDev *segs, int nseg, const int64_t *out_o
     for (int64_t i = lane; i < kept[g]; i += 32) out_hash[dst + i] = cand_hash[src + i], out_pos[dst + i] = cand_pos[src + i];
 }
 
+// Page-locked host buffer that only grows (copies to and from it run at full link rate).
 struct PinnedBytes {
     uint8_t *p = nullptr;
     size_t cap = 0;
@@ -353,6 +354,7 @@ struct PinnedBytes {
         if (e == cudaSuccess) cap = want;
         return e;
     }
+    template <class T> T *as() const { return (T *)p; }
     ~PinnedBytes() {
         if (p) cudaFreeHost(p);
     }
@@ -362,14 +364,17 @@ struct SummaryBuffers {
     PinnedBytes staging;
     DevBuf bases, seqs, tile_seq, amb, tail, ent, tile_ent, tile_cnt, tile_off, seg_start, seg_cnt;
     DevBuf chunk_first, chunk_base, cand_hash, cand_pos, segs, tkey, tcnt, kept, out_off, out_hash, out_pos;
-    std::vector<uint64_t> sk_hash;
-    std::vector<uint32_t> sk_pos;
+    PinnedBytes sk_hash, sk_pos;  // the last call's sketch entries
+    int64_t sk_n = 0;
     cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     ~SummaryBuffers() {
         for (DevBuf *b : {&bases, &seqs, &tile_seq, &amb, &tail, &ent, &tile_ent, &tile_cnt, &tile_off, &seg_start, &seg_cnt,
                           &chunk_first, &chunk_base, &cand_hash, &cand_pos, &segs, &tkey, &tcnt, &kept, &out_off,
                           &out_hash, &out_pos})
             b->release();
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
         if (st) cudaStreamDestroy(st);
     }
 };
@@ -411,7 +416,8 @@ static int64_t summary_chunk_candidates() {
 
 extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const int64_t *qlen,
                                          const char *const *reference, const int64_t *rlen,
-                                         const uint64_t *modulos, aw_sequence_summary_t *out, int *identical) {
+                                         const uint64_t *modulos, aw_sequence_summary_t *out, int *identical,
+                                         float *device_ms) {
     if (n < 0 || (n > 0 && (!query || !qlen || !reference || !rlen || !out || !identical))) {
         set_error("aw_sequence_summary_batch: invalid arguments");
         return AW_E_INVAL;
@@ -424,7 +430,8 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
         (void)reaper;
     }
     SummaryBuffers &B = *tls_sum;
-    B.sk_hash.clear(), B.sk_pos.clear();
+    B.sk_n = 0;
+    if (device_ms) *device_ms = 0.f;
     if (n == 0) return AW_OK;
     const int nseq = 2 * n;
     std::vector<SeqDev> hs(nseq);
@@ -471,9 +478,25 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
         }                                                                                             \
     } while (0)
     if (!B.st) SCUDA(cudaStreamCreateWithFlags(&B.st, cudaStreamNonBlocking));
-    // fingerprints and identity on host threads while the device runs
-    std::vector<uint64_t> fp(nseq);
+    if (!B.e0) SCUDA(cudaEventCreate(&B.e0));
+    if (!B.e1) SCUDA(cudaEventCreate(&B.e1));
+    SCUDA(B.staging.ensure((size_t)total + 16));
+    // host threads (one per 4 MB of bases, at most 8): the staging copy first, then the
+    // fingerprints and identity flags while the device runs
     const int nth = (int)std::min<int64_t>(8, std::max<int64_t>(1, total >> 22));
+    auto stage_work = [&](int w) {
+        for (int i = w; i < n; i += nth) {
+            if (qlen[i]) memcpy(B.staging.p + hs[2 * i].off, query[i], (size_t)qlen[i]);
+            if (rlen[i]) memcpy(B.staging.p + hs[2 * i + 1].off, reference[i], (size_t)rlen[i]);
+        }
+    };
+    {
+        std::vector<std::thread> sth;
+        for (int w = 1; w < nth; ++w) sth.emplace_back(stage_work, w);
+        stage_work(0);
+        for (auto &x : sth) x.join();
+    }
+    std::vector<uint64_t> fp(nseq);
     std::vector<std::thread> fth;
     auto fp_work = [&](int w) {
         for (int j = w; j < nseq; j += nth) {
@@ -506,11 +529,8 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
     SCUDA(B.seg_start.ensure(8 * 3 * (size_t)nseq));
     SCUDA(B.seg_cnt.ensure(8 * 3 * (size_t)nseq));
     cudaStream_t st = B.st;
-    SCUDA(B.staging.ensure((size_t)total + 16));
-    for (int i = 0; i < n; ++i) {
-        if (qlen[i]) memcpy(B.staging.p + hs[2 * i].off, query[i], (size_t)qlen[i]);
-        if (rlen[i]) memcpy(B.staging.p + hs[2 * i + 1].off, reference[i], (size_t)rlen[i]);
-    }
+    float ms_total = 0.f;
+    SCUDA(cudaEventRecord(B.e0, st));
     if (total) SCUDA(cudaMemcpyAsync(B.bases.p, B.staging.p, (size_t)total, cudaMemcpyHostToDevice, st));
     SCUDA(cudaMemcpyAsync(B.seqs.p, hs.data(), sizeof(SeqDev) * (size_t)nseq, cudaMemcpyHostToDevice, st));
     SCUDA(cudaMemcpyAsync(B.tile_seq.p, tseq.data(), 4 * tseq.size(), cudaMemcpyHostToDevice, st));
@@ -541,7 +561,18 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
     SCUDA(cudaMemcpyAsync(hent.data(), B.ent.p, 8 * (size_t)nseq, cudaMemcpyDeviceToHost, st));
     SCUDA(cudaMemcpyAsync(sstart.data(), B.seg_start.p, 8 * sstart.size(), cudaMemcpyDeviceToHost, st));
     SCUDA(cudaMemcpyAsync(scnt.data(), B.seg_cnt.p, 8 * scnt.size(), cudaMemcpyDeviceToHost, st));
+    SCUDA(cudaEventRecord(B.e1, st));
     SCUDA(cudaStreamSynchronize(st));
+    {
+        float ms = 0.f;
+        SCUDA(cudaEventElapsedTime(&ms, B.e0, B.e1));
+        ms_total += ms;
+    }
+    // the kept entries are at most the candidates: one page-locked output of that size
+    int64_t all_cands = 0;
+    for (int64_t c : scnt) all_cands += c;
+    SCUDA(B.sk_hash.ensure(8 * (size_t)all_cands + 8));
+    SCUDA(B.sk_pos.ensure(4 * (size_t)all_cands + 4));
     // 3-5. chunks of whole sequences (a query and its reference together is not needed:
     // the sketches are per sequence)
     int64_t out_total = 0;
@@ -590,6 +621,7 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
         SCUDA(cudaMemcpyAsync(B.chunk_first.p, first, sizeof(first), cudaMemcpyHostToDevice, st));
         SCUDA(cudaMemcpyAsync(B.chunk_base.p, base, sizeof(base), cudaMemcpyHostToDevice, st));
         SCUDA(cudaMemcpyAsync(B.segs.p, hsg.data(), sizeof(SegDev) * (size_t)nsg, cudaMemcpyHostToDevice, st));
+        SCUDA(cudaEventRecord(B.e0, st));
         SCUDA(cudaMemsetAsync(B.tcnt.p, 0, 4 * (size_t)tslots, st));
         const int32_t t0 = hs[j0].first_tile;
         const int64_t nt = (int64_t)hs[j1 - 1].first_tile + hs[j1 - 1].ntiles - t0;
@@ -611,16 +643,20 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
                                                      B.kept.as<uint32_t>(), B.out_hash.as<uint64_t>(),
                                                      B.out_pos.as<uint32_t>());
         SCUDA(cudaGetLastError());
+        SCUDA(cudaEventRecord(B.e1, st));
         std::vector<int64_t> hoff((size_t)nsg + 1);
         SCUDA(cudaMemcpyAsync(hoff.data(), B.out_off.p, 8 * hoff.size(), cudaMemcpyDeviceToHost, st));
         SCUDA(cudaStreamSynchronize(st));
+        {
+            float ms = 0.f;
+            SCUDA(cudaEventElapsedTime(&ms, B.e0, B.e1));
+            ms_total += ms;
+        }
         const int64_t kept_total = hoff[(size_t)nsg];
-        B.sk_hash.resize((size_t)(out_total + kept_total));
-        B.sk_pos.resize((size_t)(out_total + kept_total));
         if (kept_total) {
-            SCUDA(cudaMemcpyAsync(B.sk_hash.data() + out_total, B.out_hash.p, 8 * (size_t)kept_total,
+            SCUDA(cudaMemcpyAsync(B.sk_hash.as<uint64_t>() + out_total, B.out_hash.p, 8 * (size_t)kept_total,
                                   cudaMemcpyDeviceToHost, st));
-            SCUDA(cudaMemcpyAsync(B.sk_pos.data() + out_total, B.out_pos.p, 4 * (size_t)kept_total,
+            SCUDA(cudaMemcpyAsync(B.sk_pos.as<uint32_t>() + out_total, B.out_pos.p, 4 * (size_t)kept_total,
                                   cudaMemcpyDeviceToHost, st));
             SCUDA(cudaStreamSynchronize(st));
         }
@@ -631,6 +667,8 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
         out_total += kept_total;
         j0 = j1;
     }
+    B.sk_n = out_total;
+    if (device_ms) *device_ms = ms_total;
     fp_work(0);
     for (auto &x : fth) x.join();
     for (int j = 0; j < nseq; ++j) {
@@ -651,15 +689,22 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
 
 extern "C" int64_t aw_sequence_summary_sketches(uint64_t *hash, uint32_t *position, int64_t capacity) {
     if (!tls_sum) return 0;
-    const int64_t n = (int64_t)tls_sum->sk_hash.size();
+    const int64_t n = tls_sum->sk_n;
     if (!hash && !position) return n;
     if (capacity < n || !hash || !position) {
         set_error("aw_sequence_summary_sketches: capacity below the number of entries");
         return AW_E_INVAL;
     }
     if (n) {
-        memcpy(hash, tls_sum->sk_hash.data(), 8 * (size_t)n);
-        memcpy(position, tls_sum->sk_pos.data(), 4 * (size_t)n);
+        memcpy(hash, tls_sum->sk_hash.p, 8 * (size_t)n);
+        memcpy(position, tls_sum->sk_pos.p, 4 * (size_t)n);
     }
     return n;
+}
+
+extern "C" int64_t aw_sequence_summary_sketch_view(const uint64_t **hash, const uint32_t **position) {
+    if (!tls_sum || !hash || !position) return tls_sum ? tls_sum->sk_n : 0;
+    *hash = tls_sum->sk_hash.as<uint64_t>();
+    *position = tls_sum->sk_pos.as<uint32_t>();
+    return tls_sum->sk_n;
 }

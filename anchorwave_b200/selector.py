@@ -25,38 +25,43 @@ class SequenceSummary(C.Structure):
                 ("sketch_offset", C.c_int64 * 3), ("sketch_count", C.c_int64 * 3)]
 
 
-def sequence_summary_raw(queries: Sequence[bytes], references: Sequence[bytes], modulos=None):
-    """One call: (summaries[2n], identical[n], sketch hashes, sketch positions)."""
+def sequence_summary_raw(queries: Sequence[bytes], references: Sequence[bytes], modulos=None, copy=True):
+    """One call: (summaries[2n], identical[n], sketch hashes, sketch positions, device ms).
+    copy=False returns views of the library's page-locked buffers (valid until the next call
+    on this thread)."""
     n = len(queries)
     out = (SequenceSummary * max(2 * n, 1))()
     ident = np.zeros(max(n, 1), dtype=np.int32)
-    qb = [C.create_string_buffer(q, len(q) + 1) for q in queries]
-    rb = [C.create_string_buffer(r, len(r) + 1) for r in references]
-    qp = (C.c_void_p * max(n, 1))(*[C.addressof(b) for b in qb])
-    rp = (C.c_void_p * max(n, 1))(*[C.addressof(b) for b in rb])
+    # pointers straight into the bytes objects (no copies)
+    qp = (C.c_char_p * max(n, 1))(*queries)
+    rp = (C.c_char_p * max(n, 1))(*references)
     ql = np.array([len(q) for q in queries] or [0], dtype=np.int64)
     rl = np.array([len(r) for r in references] or [0], dtype=np.int64)
     mod = None
     if modulos is not None:
         mod = np.ascontiguousarray(np.asarray(modulos, dtype=np.uint64).reshape(n, 3))
+    ms = C.c_float(0.0)
     rc = lib.aw_sequence_summary_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data,
-                                       mod.ctypes.data if mod is not None else None, out, ident.ctypes.data)
+                                       mod.ctypes.data if mod is not None else None, out, ident.ctypes.data,
+                                       C.byref(ms))
     if rc != 0:
         raise AwError(f"aw_sequence_summary_batch failed ({rc}): {last_error()}")
-    total = lib.aw_sequence_summary_sketches(None, None, 0)
-    h = np.zeros(max(total, 1), dtype=np.uint64)
-    p = np.zeros(max(total, 1), dtype=np.uint32)
-    got = lib.aw_sequence_summary_sketches(h.ctypes.data, p.ctypes.data, total)
-    if got != total:
-        raise AwError(f"aw_sequence_summary_sketches failed ({got}): {last_error()}")
-    return out, ident[:n], h[:total], p[:total]
+    hp, pp = C.c_void_p(), C.c_void_p()
+    total = lib.aw_sequence_summary_sketch_view(C.byref(hp), C.byref(pp))
+    if total == 0:
+        return out, ident[:n], np.zeros(0, np.uint64), np.zeros(0, np.uint32), ms.value
+    h = np.ctypeslib.as_array(C.cast(hp, C.POINTER(C.c_uint64)), shape=(total,))
+    p = np.ctypeslib.as_array(C.cast(pp, C.POINTER(C.c_uint32)), shape=(total,))
+    if copy:
+        h, p = h.copy(), p.copy()
+    return out, ident[:n], h, p, ms.value
 
 
 def sequence_summary_batch(queries: Sequence[bytes], references: Sequence[bytes],
                            modulos=None) -> List[Tuple[bool, list]]:
     """Per pair (identical, [query summary, reference summary]); each summary a dict with
     fingerprint, the three fractions and sketches = [[(hash, position), ...] for k = 9, 15, 21]."""
-    out, ident, h, p = sequence_summary_raw(queries, references, modulos)
+    out, ident, h, p, _ = sequence_summary_raw(queries, references, modulos)
     res = []
     for i in range(len(queries)):
         sides = []

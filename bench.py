@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--long-banded-min", type=int, default=100_000)
     ap.add_argument("--long-banded-max", type=int, default=150_000)
     ap.add_argument("--wfa-pairs", type=int, default=16384, help="pairs of the batched WFA workload (0 skips it)")
+    ap.add_argument("--no-selector-summary", action="store_true",
+                    help="skip the selector sequence-pass measurement")
     ap.add_argument("--wfa-pool-gb", type=float, default=0.0,
                     help="device wavefront pool of the WFA workload (0: most of the free memory)")
     return ap.parse_args()
@@ -332,6 +334,57 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
     return out
 
 
+def selector_summary_measurement(ps, rank: int, cpu: bool):
+    """The selector's sequence pass (summarizeSequencePair: k-mer sketches at k = 9, 15, 21,
+    composition, entropy, fingerprints) over the intervals of the headline workload, through
+    aw_sequence_summary_batch with host buffers (bases/s of both sequences), and the
+    reference's compiled selector on the host threads over the same pairs (fingerprints,
+    sketch sizes and fractions compared)."""
+    import time
+
+    import numpy as np
+
+    from anchorwave_b200 import selector
+    from anchorwave_b200 import workloads as W
+    qs = [W.to_ascii(q) for q in ps.queries]
+    ts = [W.to_ascii(t) for t in ps.targets]
+    bases = sum(len(q) for q in qs) + sum(len(t) for t in ts)
+    selector.sequence_summary_raw(qs[:32], ts[:32])
+    secs, dev = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        out, ident, h, p, ms = selector.sequence_summary_raw(qs, ts, copy=False)
+        secs.append(time.perf_counter() - t0)
+        dev.append(ms)
+    best = min(secs)
+    res = {"pairs": len(qs), "bases": bases, "e2e_bases_per_s": bases / best, "e2e_ms": 1e3 * best,
+           "device_ms": min(dev), "device_bases_per_s": bases / (min(dev) * 1e-3),
+           "sketch_entries": int(len(h)), "h2d_bytes": bases, "d2h_bytes": int(len(h)) * 12 + len(out) * 80}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        try:
+            ref = oracle.Reference()
+        except FileNotFoundError as e:
+            res["cpu_reference"] = {"unavailable": str(e)}
+            return res
+        if not ref.has_summary:
+            res["cpu_reference"] = {"unavailable": "compiled reference without the selector shim"}
+            return res
+        rsecs, rout, rident = ref.sequence_summary_batch(qs, ts)
+        same = bool(np.array_equal(rident, ident))
+        for j in range(2 * len(qs)):
+            a, b = out[j], rout[j]
+            same &= (a.fingerprint == b.fingerprint and list(a.sketch_count) == list(b.count) and
+                     a.ambiguous_fraction == b.ambiguous_fraction and
+                     a.low_complexity_fraction == b.low_complexity_fraction and
+                     abs(a.normalized_entropy - b.normalized_entropy) <= 1e-9)
+        res["cpu_reference"] = {"bases_per_s": bases / rsecs, "seconds": rsecs, "threads": os.cpu_count(),
+                                "summaries_identical": same}
+        res["vs_cpu_reference"] = res["e2e_bases_per_s"] / (bases / rsecs)
+    return res
+
+
 def long_banded_measurement(rank: int, cpu: bool, npairs: int = 16, lmin: int = 100_000, lmax: int = 150_000):
     """The long-interval banded and Singletrack workload at reduced lengths (16 pairs,
     100-150 kb, w = 10% of the shorter length, repeat-rich queries with long indels): band
@@ -491,6 +544,8 @@ def main():
         args.long_banded_max)
     wfa_res = (wfa_measurement(args.wfa_pairs, rank, rank == 0 and not args.no_cpu_baseline, args.wfa_pool_gb)
                if args.wfa_pairs > 0 else None)
+    summary_res = (None if args.no_selector_summary else
+                   selector_summary_measurement(ps, rank, rank == 0 and not args.no_cpu_baseline))
 
     if rank != 0:
         barrier(pg)
@@ -533,6 +588,7 @@ def main():
         "serving": serving,
         "long_banded": long_banded,
         "wfa": wfa_res,
+        "selector_summary": summary_res,
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
     }

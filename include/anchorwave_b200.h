@@ -176,10 +176,14 @@ typedef struct {
  * stay with the calling thread until its next call.  Returns 0 or a negative AW_E_*. */
 int aw_sequence_summary_batch(int n, const char *const *query, const int64_t *qlen,
                               const char *const *reference, const int64_t *rlen,
-                              const uint64_t *modulos, aw_sequence_summary_t *out, int *identical);
+                              const uint64_t *modulos, aw_sequence_summary_t *out, int *identical,
+                              float *device_ms);
 /* Copies the calling thread's last sketches (capacity entries at least; hash and position
  * both NULL: returns the number of entries only).  Returns the number of entries. */
 int64_t aw_sequence_summary_sketches(uint64_t *hash, uint32_t *position, int64_t capacity);
+/* The same entries without a copy: pointers into the calling thread's page-locked
+ * buffers, valid until its next aw_sequence_summary_batch.  Returns the number of entries. */
+int64_t aw_sequence_summary_sketch_view(const uint64_t **hash, const uint32_t **position);
 
 /* ---- serving loop (continuous batching) --------------------------------------- */
 
