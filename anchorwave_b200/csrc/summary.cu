@@ -48,9 +48,18 @@ constexpr int SUM_PER_THREAD = SUM_TILE / SUM_THREADS;  // 4 consecutive positio
 constexpr uint32_t SUM_MAX_OCC = 4;
 constexpr uint64_t SUM_TARGET[3] = {1024, 4096, 1024};
 
+// Divisibility by a sampling modulo d = d0 * 2^s (d0 odd) without a division
+// (Granlund & Montgomery, "Division by invariant integers using multiplication", 1994;
+// Warren, Hacker's Delight, 2nd ed., 10-17): d | h exactly when
+// rotr(h * d0^-1 mod 2^64, s) <= floor((2^64 - 1) / d).
+struct DivTest {
+    uint64_t inv, limit;
+    uint32_t shift, pad;
+};
+
 struct SeqDev {
     int64_t off, len;
-    uint64_t mod[3];
+    DivTest div[3];
     int32_t first_tile, ntiles;
 };
 
@@ -64,6 +73,12 @@ __device__ __forceinline__ uint64_t mix_hash(uint64_t v) {
     v *= 0x94d049bb133111ebULL;
     v ^= v >> 31;
     return v;
+}
+
+__device__ __forceinline__ bool divisible(uint64_t h, const DivTest &d) {
+    uint64_t x = h * d.inv;
+    if (d.shift) x = (x >> d.shift) | (x << (64 - d.shift));
+    return x <= d.limit;
 }
 
 __device__ __forceinline__ int8_t base_code(uint8_t b) {
@@ -153,7 +168,7 @@ __global__ void __launch_bounds__(SUM_THREADS) summary_tile_kernel(
             const uint64_t k = kmer_len(sc);
             if (run < k) continue;
             const uint64_t h = mix_hash(val & ((1ULL << (2 * k)) - 1));
-            if (h % S.mod[sc] == 0) sf[u][sc] = true, sh[u][sc] = h, ++nsamp[sc];
+            if (divisible(h, S.div[sc])) sf[u][sc] = true, sh[u][sc] = h, ++nsamp[sc];
         }
     }
     if (COUNT) {
@@ -381,6 +396,18 @@ struct SummaryBuffers {
 
 thread_local SummaryBuffers *tls_sum = nullptr;
 
+DivTest make_div_test(uint64_t d) {
+    DivTest t;
+    t.shift = (uint32_t)__builtin_ctzll(d);
+    const uint64_t d0 = d >> t.shift;
+    uint64_t x = d0;  // correct to 3 bits for odd d0; each Newton step doubles them
+    for (int i = 0; i < 5; ++i) x *= 2 - d0 * x;
+    t.inv = x;
+    t.limit = UINT64_MAX / d;
+    t.pad = 0;
+    return t;
+}
+
 uint64_t mix_hash_host(uint64_t v) {
     v ^= v >> 30;
     v *= 0xbf58476d1ce4e5b9ULL;
@@ -459,7 +486,7 @@ extern "C" int aw_sequence_summary_batch(int n, const char *const *query, const 
         for (int t = 0; t < 2; ++t) {
             SeqDev &S = hs[2 * i + t];
             S.off = total, S.len = t ? rlen[i] : qlen[i];
-            memcpy(S.mod, mod, sizeof(mod));
+            for (int sc = 0; sc < 3; ++sc) S.div[sc] = make_div_test(mod[sc]);
             S.first_tile = (int32_t)ntiles;
             S.ntiles = (int32_t)((S.len + SUM_TILE - 1) / SUM_TILE);
             total += S.len, ntiles += S.ntiles;
