@@ -23,7 +23,7 @@ class KswExtz(C.Structure):
 
 # Every symbol the header declares; tests check that the library exports each one.
 EXPORTS = [
-    "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "aw_ksw_extd2_batch",
+    "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "ksw_extd2_singletrack_sse_gpu", "aw_ksw_extd2_batch",
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_graph", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_release_thread_buffers",
@@ -74,6 +74,8 @@ def _load(path: str = LIB_PATH):
     lib.ksw_extd2_gpu.restype = None
     lib.ksw_extd2_singletrack_gpu.argtypes = ksw_args
     lib.ksw_extd2_singletrack_gpu.restype = None
+    lib.ksw_extd2_singletrack_sse_gpu.argtypes = ksw_args
+    lib.ksw_extd2_singletrack_sse_gpu.restype = None
     lib.aw_ksw_extd2_batch.argtypes = [i32, vp, vp, vp, vp, vp, i8, vp, i8, i8, i8, i8, i32, i32, i32, vp]
     lib.aw_ksw_extd2_batch.restype = i32
     lib.aw_ksw_plan_new.argtypes = [i32, vp, vp, vp, i8, vp, i8, i8, i8, i8, i32, i32, i32]

@@ -19,6 +19,8 @@
 #define AW_EZ_SPLICE_MASK    0x700
 #define AW_EZ_SEMIGLOBAL_END 0x800
 #define AW_EZ_SINGLETRACK    0x1000
+// with AW_EZ_SINGLETRACK: ksw_extd2_singletrack_sse (16-byte blocks and its end rules)
+#define AW_EZ_SSE_SINGLETRACK 0x4000
 
 namespace aw {
 

@@ -961,14 +961,21 @@ void ksw_extd2_gpu(void *km, int qlen, const uint8_t *query, int tlen, const uin
                    const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int w, int zdrop,
                    int end_bonus, int flag, ksw_extz_t *ez) {
     single_call(km, qlen, query, tlen, target, m, mat, q, e, q2, e2, w, zdrop, end_bonus,
-                flag & ~AW_EZ_SINGLETRACK, ez);
+                flag & ~(AW_EZ_SINGLETRACK | AW_EZ_SSE_SINGLETRACK), ez);
 }
 
 void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tlen, const uint8_t *target,
                                int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int w,
                                int zdrop, int end_bonus, int flag, ksw_extz_t *ez) {
     single_call(km, qlen, query, tlen, target, m, mat, q, e, q2, e2, w, zdrop, end_bonus,
-                flag | AW_EZ_SINGLETRACK, ez);
+                (flag | AW_EZ_SINGLETRACK) & ~AW_EZ_SSE_SINGLETRACK, ez);
+}
+
+void ksw_extd2_singletrack_sse_gpu(void *km, int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                                   int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2, int w,
+                                   int zdrop, int end_bonus, int flag, ksw_extz_t *ez) {
+    single_call(km, qlen, query, tlen, target, m, mat, q, e, q2, e2, w, zdrop, end_bonus,
+                flag | AW_EZ_SINGLETRACK | AW_EZ_SSE_SINGLETRACK, ez);
 }
 
 }  // extern "C"

@@ -114,6 +114,21 @@ struct Ez {
     int max, max_q, max_t, mqe, mqe_t, mte, mte_q, score, zdropped, reach_end, stopped;
 };
 
+// mte / mqe of a finished anti-diagonal r: with ">=" and mte_q = r - en0 as AnchorWave's
+// ksw_extd2 (ksw2_extd2_sse.c:369-372); ksw_extd2_singletrack_sse keeps minimap2's
+// strict ">" and mte_q = r - en with en rounded up to its 16-byte block
+// (minimap2/ksw2_singletrack.cpp:583-586).
+__device__ __forceinline__ void end_rules(Ez &z, const int32_t *H, int r, int st0, int en0, int qlen, int tlen,
+                                          bool sse_st) {
+    if (sse_st) {
+        if (en0 == tlen - 1 && H[en0] > z.mte) z.mte = H[en0], z.mte_q = r - ((en0 + 16) / 16 * 16 - 1);
+        if (r - st0 == qlen - 1 && H[st0] > z.mqe) z.mqe = H[st0], z.mqe_t = st0;
+    } else {
+        if (en0 == tlen - 1 && H[en0] >= z.mte) z.mte = H[en0], z.mte_q = r - en0;
+        if (r - st0 == qlen - 1 && H[st0] >= z.mqe) z.mqe = H[st0], z.mqe_t = st0;
+    }
+}
+
 __device__ bool apply_zdrop(Ez &ez, int H, int r, int t, int zdrop, int e) {
     if (H > ez.max) {
         ez.max = H, ez.max_t = t, ez.max_q = r - t;
@@ -242,7 +257,8 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
     const int qlen = P.qlen, tlen = P.tlen, B = A.B, flag = A.flag;
     const bool with_cigar = !(flag & AW_EZ_SCORE_ONLY);
     const bool approx_max = !!(flag & AW_EZ_APPROX_MAX);
-    const bool singletrack = B > 16 && !!(flag & AW_EZ_SINGLETRACK);
+    const bool sse_st = !!(flag & AW_EZ_SSE_SINGLETRACK) && !!(flag & AW_EZ_SINGLETRACK);
+    const bool singletrack = (B > 16 || sse_st) && !!(flag & AW_EZ_SINGLETRACK);
     const bool right = !!(flag & AW_EZ_RIGHT);
     const bool generic = !!(flag & AW_EZ_GENERIC_SC);
     const uint8_t *qs = A.qcodes + P.qoff, *ts = A.tcodes + P.toff;
@@ -334,7 +350,8 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
                 }
             }
         } else {
-            for (int pos = st0 + tid; pos <= en0; pos += NT) W.s[pos] = A.mat[ts[pos] * m + qs[qrr0 + pos]];
+            // query base r - pos, through the reversed-query index of the reference's qrr
+            for (int pos = st0 + tid; pos <= en0; pos += NT) W.s[pos] = A.mat[ts[pos] * m + qr_ext(qrr0 + pos, qs, qlen)];
         }
         __syncthreads();
         // cells, in NT-wide chunks starting at the block-aligned stB
@@ -443,8 +460,7 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
                     for (int t = en1; t < en0; ++t)
                         if (W.H[t] > max_H) max_H = W.H[t], max_t = t;
                     Ez &z = s_ez;
-                    if (en0 == tlen - 1 && W.H[en0] >= z.mte) z.mte = W.H[en0], z.mte_q = r - en0;
-                    if (r - st0 == qlen - 1 && W.H[st0] >= z.mqe) z.mqe = W.H[st0], z.mqe_t = st0;
+                    end_rules(z, W.H, r, st0, en0, qlen, tlen, sse_st);
                     if (apply_zdrop(z, max_H, r, max_t, A.zdrop, e2)) s_brk = 1;
                     else if (r == qlen + tlen - 2 && en0 == tlen - 1) z.score = W.H[tlen - 1];
                 }
@@ -452,8 +468,7 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
                 W.H[0] = W.v[0] - S.qe_pre;
                 Ez &z = s_ez;
                 const int max_H = W.H[0], max_t = 0;
-                if (en0 == tlen - 1 && W.H[en0] >= z.mte) z.mte = W.H[en0], z.mte_q = r - en0;
-                if (r - st0 == qlen - 1 && W.H[st0] >= z.mqe) z.mqe = W.H[st0], z.mqe_t = st0;
+                end_rules(z, W.H, r, st0, en0, qlen, tlen, sse_st);
                 if (apply_zdrop(z, max_H, r, max_t, A.zdrop, e2)) s_brk = 1;
                 else if (r == qlen + tlen - 2 && en0 == tlen - 1) z.score = W.H[tlen - 1];
             }
@@ -487,7 +502,9 @@ __global__ void __launch_bounds__(NT) ksw_exact_kernel(ExactArgs A) {
         Cig c{A.cig + P.cig_off, 0};
         const int64_t n_col = E.row;
         if (singletrack) {
-            if (!z.stopped && !z.zdropped && !(flag & (AW_EZ_EXTZ_ONLY | AW_EZ_SEMIGLOBAL_END))) {
+            // ksw_extd2_singletrack_sse reconstructs whatever the EXTZ/SEMIGLOBAL flags
+            // (minimap2/ksw2_singletrack.cpp:606-615)
+            if (!z.stopped && !z.zdropped && (sse_st || !(flag & (AW_EZ_EXTZ_ONLY | AW_EZ_SEMIGLOBAL_END)))) {
                 const bool ok = singletrack_bt(c, qlen, qs, tlen, ts, m, A.mat, S, n_col, W.off, W.off_end,
                                                (const int8_t *)W.p, (const int8_t *)W.p2);
                 if (!ok) c.n = 0;
@@ -558,9 +575,12 @@ int run_exact_ksw(size_t n_exact, const int32_t *d_ids, const uint8_t *d_q, cons
         std::lock_guard<std::mutex> lk(g_mu);
         B = g_block;
     }
+    // ksw_extd2_singletrack_sse works on 16-byte blocks whatever the host's ISA
+    const bool sse_st = (flag & AW_EZ_SSE_SINGLETRACK) && (flag & AW_EZ_SINGLETRACK);
+    if (sse_st) B = 16;
     const int stop_interval = t_stop_interval, stop_at = t_stop_at;
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY);
-    const bool stk = B > 16 && (flag & AW_EZ_SINGLETRACK);
+    const bool stk = (B > 16 || sse_st) && (flag & AW_EZ_SINGLETRACK);
     // per-pair workspace sizes
     std::vector<ExactPair> eps;
     std::vector<int64_t> sizes;

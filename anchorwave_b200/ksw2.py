@@ -104,6 +104,17 @@ def ksw_extd2_singletrack(query, target, mat, q, e, q2, e2, w=-1, zdrop=-1, end_
     return _take(ez)
 
 
+def ksw_extd2_singletrack_sse(query, target, mat, q, e, q2, e2, w=-1, zdrop=-1, end_bonus=0, flag=0,
+                              m=5) -> KswResult:
+    """ksw_extd2_singletrack_sse (minimap2/ksw2_singletrack.cpp:202-626), the Singletrack entry of
+    builds without AVX2, on the GPU."""
+    qa, ta = _codes(query), _codes(target)
+    ez = KswExtz()
+    lib.ksw_extd2_singletrack_sse_gpu(None, len(qa), qa.ctypes.data, len(ta), ta.ctypes.data, m, _mat(mat), q, e,
+                                      q2, e2, w, zdrop, end_bonus, flag, C.byref(ez))
+    return _take(ez)
+
+
 def _ptr_array(arrs: Sequence[np.ndarray]):
     ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
     return ptrs

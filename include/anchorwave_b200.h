@@ -60,6 +60,21 @@ void ksw_extd2_singletrack_gpu(void *km, int qlen, const uint8_t *query, int tle
                                int8_t e, int8_t q2, int8_t e2, int w, int zdrop, int end_bonus,
                                int flag, ksw_extz_t *ez);
 
+/*
+ * Replaces ksw_extd2_singletrack_sse (minimap2/ksw2_singletrack.hpp:17-32;
+ * ksw2_singletrack.cpp:202-626), the Singletrack entry of builds without AVX2
+ * (alignSlidingWindow.cpp:942-948): 16-byte-block band semantics, mqe/mte on a strict
+ * ">", mte_q = r - en with en rounded up to its block, and the reconstruction whatever the
+ * EXTZ/SEMIGLOBAL flags.  Same signature; the batch entries take the same behaviour from
+ * flag AW_EZ_SINGLETRACK | AW_EZ_SSE_SINGLETRACK.
+ */
+void ksw_extd2_singletrack_sse_gpu(void *km, int qlen, const uint8_t *query, int tlen,
+                                   const uint8_t *target, int8_t m, const int8_t *mat, int8_t q,
+                                   int8_t e, int8_t q2, int8_t e2, int w, int zdrop, int end_bonus,
+                                   int flag, ksw_extz_t *ez);
+#define AW_EZ_SINGLETRACK     0x1000  /* flag: the Singletrack traceback */
+#define AW_EZ_SSE_SINGLETRACK 0x4000  /* flag, with AW_EZ_SINGLETRACK: as ksw_extd2_singletrack_sse */
+
 /* ---- batched KSW2 ------------------------------------------------------------ */
 
 /*

@@ -18,6 +18,11 @@
  *   ksw_reset_extz            minimap2/ksw2.h:194-199
  *   ksw_apply_zdrop           minimap2/ksw2.h:201-217
  *   ksw2_singletrack_backtrace_affine2p  minimap2/ksw2_singletrack.cpp:63-176
+ *   ksw_extd2_singletrack_sse  minimap2/ksw2_singletrack.cpp:202-626 (block = 16 with the
+ *                              Singletrack flag: the same DP and tracks, minimap2's original
+ *                              end rules -- mqe/mte on a strict ">", mte_q = r - en with en
+ *                              rounded up to its 16-byte block, :583-586 -- and the
+ *                              reconstruction whatever the EXTZ/SEMIGLOBAL flags, :606-615)
  *
  * The SIMD kernels keep difference-encoded int8 cells (u,v,x,y,x2,y2) in
  * arrays indexed by target position t, and recompute every anti-diagonal r
@@ -226,7 +231,8 @@ void oracle_ksw_extd2(int block, int qlen, const uint8_t *query, int tlen, const
     int r, t, qe = q + e, n_col_, *off = 0, *off_end = 0, tlen_, qlen_, last_st, last_en;
     int max_sc, min_sc, long_thres, long_diff, wl, wr;
     int with_cigar = !(flag & OR_SCORE_ONLY), approx_max = !!(flag & OR_APPROX_MAX);
-    int singletrack = (B > 16) && !!(flag & OR_SINGLETRACK);
+    int singletrack = !!(flag & OR_SINGLETRACK);
+    const int sse_st = singletrack && B == 16; /* ksw_extd2_singletrack_sse */
     int32_t *H = 0, H0 = 0, last_H0_t = 0;
     int8_t *mem, *u, *v, *x, *y, *x2, *y2, *s;
     uint8_t *sf, *qr, *p = 0, *p2 = 0;
@@ -420,8 +426,13 @@ void oracle_ksw_extd2(int block, int qlen, const uint8_t *query, int tlen, const
                 }
             } else
                 H[0] = v[0] - qe, max_H = H[0], max_t = 0;
-            if (en0 == tlen - 1 && H[en0] >= ez->mte) ez->mte = H[en0], ez->mte_q = r - en0;
-            if (r - st0 == qlen - 1 && H[st0] >= ez->mqe) ez->mqe = H[st0], ez->mqe_t = st0;
+            if (sse_st) {
+                if (en0 == tlen - 1 && H[en0] > ez->mte) ez->mte = H[en0], ez->mte_q = r - ((en0 + 16) / 16 * 16 - 1);
+                if (r - st0 == qlen - 1 && H[st0] > ez->mqe) ez->mqe = H[st0], ez->mqe_t = st0;
+            } else {
+                if (en0 == tlen - 1 && H[en0] >= ez->mte) ez->mte = H[en0], ez->mte_q = r - en0;
+                if (r - st0 == qlen - 1 && H[st0] >= ez->mqe) ez->mqe = H[st0], ez->mqe_t = st0;
+            }
             if (or_zdrop(ez, max_H, r, max_t, zdrop, e2)) break;
             if (r == qlen + tlen - 2 && en0 == tlen - 1) ez->score = H[tlen - 1];
         } else {
@@ -446,7 +457,7 @@ void oracle_ksw_extd2(int block, int qlen, const uint8_t *query, int tlen, const
     free(mem);
     free(H);
     if (with_cigar && singletrack) {
-        if (!ez->stopped && !ez->zdropped && !(flag & (OR_EXTZ_ONLY | OR_SEMIGLOBAL_END))) {
+        if (!ez->stopped && !ez->zdropped && (sse_st || !(flag & (OR_EXTZ_ONLY | OR_SEMIGLOBAL_END)))) {
             or_singletrack_bt(qlen, query, tlen, target, m, mat, q, e, q2, e2, row, off, off_end,
                               (const int8_t *)p, (const int8_t *)p2, ez);
             if (ez->n_cigar == 0) ez->zdropped = 1;

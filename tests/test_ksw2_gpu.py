@@ -196,3 +196,22 @@ def test_anchorwave_wrappers(gpu, restatement):
     assert s2 == o.score
     s3, aq3, ad3, stopped = gpu.align_ksw2_singletrack(qs, ts, -4, -4, -2, -24, -1)
     assert not stopped and s3 == o.score
+
+
+def test_exact_kernel_generic_scores(gpu, restatement):
+    """Z-drop sends pairs to the exact anti-diagonal kernel; with KSW_EZ_GENERIC_SC its score
+    fill reads the matrix with the reversed-query index (regression: it read the forward
+    query there), with and without the Singletrack traceback, left and right aligned."""
+    rng = np.random.default_rng(404)
+    mat = [2 if a == b else (-4 if a < 4 and b < 4 else -1) for a in range(5) for b in range(5)]
+    for i in range(60):
+        L = int(np.exp(rng.uniform(np.log(2), np.log(1500))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.2, 4.0)
+        flag = oracle.KSW_EZ_GENERIC_SC | (oracle.KSW_EZ_RIGHT if i % 2 else 0)
+        w = -1 if i % 3 else int(rng.integers(1, max(2, L // 2)))
+        for st in (False, True):
+            f = gpu.ksw_extd2_singletrack if st else gpu.ksw_extd2
+            g = f(q, t, mat, 4, 2, 24, 1, w=w, zdrop=200, flag=flag)
+            o = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, w=w, zdrop=200,
+                                      flag=flag | (oracle.KSW_EZ_SINGLETRACK if st else 0), block=64)
+            assert g.key() == o.key(), (i, L, w, hex(flag), st)

@@ -83,7 +83,10 @@ def test_restatement_matches_reference_random(restatement, isa):
                                   block=ref.block)
         b = ref.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop, flag=flag)
         assert a.key() == b.key(), (it, L, w, hex(flag), pen)
-        if isa != "sse" and not (flag & (oracle.KSW_EZ_SCORE_ONLY | oracle.KSW_EZ_SEMIGLOBAL_END | oracle.KSW_EZ_EXTZ_ONLY)):
+        # Singletrack entry of the library's ISA (ksw_extd2_singletrack_sse on the SSE build,
+        # which also takes the score-only, semiglobal and extension flags)
+        if isa == "sse" or not (flag & (oracle.KSW_EZ_SCORE_ONLY | oracle.KSW_EZ_SEMIGLOBAL_END |
+                                         oracle.KSW_EZ_EXTZ_ONLY)):
             a = restatement.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop,
                                       flag=flag | oracle.KSW_EZ_SINGLETRACK, block=ref.block)
             b = ref.ksw_extd2(qc.tobytes(), tc.tobytes(), mat, *pen, w=w, zdrop=zdrop, flag=flag, variant=2)
@@ -207,3 +210,24 @@ def test_summary_restatement_matches_reference(restatement, reference):
             assert x["ambiguous_fraction"] == y["ambiguous_fraction"], i
             assert x["low_complexity_fraction"] == y["low_complexity_fraction"], i
             assert abs(x["normalized_entropy"] - y["normalized_entropy"]) <= 1e-12, i
+
+
+def test_sse_singletrack_restatement_matches_reference(restatement, reference):
+    """ksw_extd2_singletrack_sse (the reference's entry 3 on any host) against the restatement
+    with 16-byte blocks and the Singletrack flag: end rules, band, and every flag."""
+    rng = np.random.default_rng(77)
+    flags = [0, oracle.KSW_EZ_SEMIGLOBAL_END, oracle.KSW_EZ_EXTZ_ONLY, oracle.KSW_EZ_REV_CIGAR,
+             oracle.KSW_EZ_SCORE_ONLY, oracle.KSW_EZ_APPROX_MAX | oracle.KSW_EZ_APPROX_DROP,
+             oracle.KSW_EZ_RIGHT | oracle.KSW_EZ_GENERIC_SC]
+    mat = oracle.anchorwave_matrix(-4)
+    for it in range(140):
+        L = int(np.exp(rng.uniform(np.log(2), np.log(1500))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.25, 4.0)
+        flag = flags[it % len(flags)]
+        w = -1 if it % 2 == 0 else int(rng.integers(0, max(1, L // 3)))
+        zdrop = -1 if it % 3 else 100
+        pen = PEN[it % len(PEN)]
+        a = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, *pen, w=w, zdrop=zdrop,
+                                  flag=flag | oracle.KSW_EZ_SINGLETRACK, block=16)
+        b = reference.ksw_extd2(q.tobytes(), t.tobytes(), mat, *pen, w=w, zdrop=zdrop, flag=flag, variant=3)
+        assert a.key() == b.key(), (it, L, w, hex(flag), pen)
