@@ -61,3 +61,42 @@ def test_decode_and_rescore_match_reference_semantics(restatement):
         assert qp == len(qs) and tp == len(ts) and len(aq) == len(ad)
         # in full mode the emitted CIGAR's two-piece score is the DP optimum
         assert ksw2.score_gapped_two_piece_affine(aq, ad, -4, -4, -2, -24, -1) == r.score
+
+
+def test_wfa_attribute_checks_on_the_host():
+    """wavefront_aligner_new_gpu rejects what WFA2-lib rejects (wavefront_penalties.c:141-150)
+    and the memory modes it does not provide, before touching a device."""
+    from anchorwave_b200._lib import WfaAttr
+    lib = _lib.lib
+    bad = [WfaAttr(0, 4, 2, 24, 1, 0, 0, 0), WfaAttr(4, -1, 2, 24, 1, 0, 0, 0), WfaAttr(4, 4, 0, 24, 1, 0, 0, 0),
+           WfaAttr(4, 4, 2, 24, 0, 0, 0, 0), WfaAttr(4, 4, 2, 24, 1, 0, 3, 0), WfaAttr(4, 4, 2, 24, 1, 0, -1, 0)]
+    for a in bad:
+        assert not lib.wavefront_aligner_new_gpu(ctypes.byref(a))
+        assert _lib.last_error()
+    assert not lib.wavefront_aligner_new_gpu(ctypes.byref(bad[4]))
+    assert "memory_mode" in _lib.last_error()
+
+
+def test_sequence_summary_argument_checks_on_the_host():
+    """aw_sequence_summary_batch validates its arguments before any device work: an empty
+    batch succeeds with no entries, NULL arrays and a zero sampling modulo are rejected."""
+    lib = _lib.lib
+    assert lib.aw_sequence_summary_batch(0, None, None, None, None, None, None, None, None) == 0
+    assert lib.aw_sequence_summary_sketches(None, None, 0) == 0
+    assert lib.aw_sequence_summary_batch(1, None, None, None, None, None, None, None, None) < 0
+    q = (ctypes.c_char_p * 1)(b"ACGT")
+    ln = (ctypes.c_int64 * 1)(4)
+    out = (ctypes.c_uint8 * 160)()
+    ident = (ctypes.c_int * 1)()
+    mods = (ctypes.c_uint64 * 3)(0, 1, 1)
+    assert lib.aw_sequence_summary_batch(1, q, ln, q, ln, mods, out, ident, None) < 0
+    assert "modulo" in _lib.last_error()
+    neg = (ctypes.c_int64 * 1)(-1)
+    assert lib.aw_sequence_summary_batch(1, q, neg, q, ln, None, out, ident, None) < 0
+
+
+def test_summary_struct_layouts_agree():
+    """aw_sequence_summary_t as the Python mirror and the oracles see it."""
+    from anchorwave_b200.selector import SequenceSummary
+    assert ctypes.sizeof(SequenceSummary) == 80
+    assert ctypes.sizeof(oracle.SummaryOut) == 56
