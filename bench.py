@@ -19,6 +19,14 @@ and the CIGARs.
     per cell / DP-phase CUDA-event time) is set against the packed-field peak measured live
     by aw_int16x2_peak_ops() (the 32-bit peak, aw_int32_peak_ops(), is reported beside it);
     the traceback store stream is reported against HBM bandwidth.
+  * serving: a 20,000-request trace through the continuous-batching server (saturated and at
+    70% offered load with p50/p99 latency).
+  * long_banded: 16 pairs of 100-150 kb, w = 10%, banded and Singletrack, beside the
+    reference's CPU code on the same pairs.
+  * wfa: 16,384 pairs of 100 bp-10 kb (0.5-5%), high memory (standard and Singletrack) and
+    medium memory (piggyback), device memory per pair, beside WFA2-lib in the same mode.
+  * selector_summary: the selector's sequence pass (k-mer sketches, composition, entropy,
+    fingerprints) over the headline pairs, beside the compiled selector.
 
 `--impl reference` times the reference CPU implementation (oracle/_ref) on the same workload,
 metric and unit.  With torchrun (N>1) every rank aligns its own batch (weak scaling, no
