@@ -48,6 +48,9 @@ sys.path.insert(0, ROOT)
 
 OPS_PER_CELL_CIGAR = 47
 OPS_PER_CELL_SCORE = 31
+# dram__bytes_read.sum + dram__bytes_write.sum per DP cell of ksw_full_kernel in one ncu
+# capture (48-pair case: 3.2 MB read + 1.64 GB written for 1.64e9 cells)
+NCU_DRAM_BYTES_PER_CELL = 1.002
 METRIC = "batched GCUPS & pairs/s vs plain per-call on 1 B200, bit-exact; p50/p99 latency"
 
 
@@ -582,7 +585,13 @@ def main():
         "batched_vs_plain_pairs_per_s": pairs_per_s / world / plain["pairs_per_s"],
         "phase_ms": {"dp": dp_mean, "traceback": float(np.mean(bt_ms))},
         "roofline": {"bound": "int16x2", "achieved": achieved_ops / 1e12, "peak": simd_peak / 1e12, "unit": "TOPS",
-                     "frac": achieved_ops / simd_peak if simd_peak else None, "traffic": None,
+                     "frac": achieved_ops / simd_peak if simd_peak else None,
+                     # DRAM bytes of one DP phase: the bytes per DP cell of an ncu capture of
+                     # the strip kernel (dram__bytes_read + write, 1.643 GB for 1.64e9 cells
+                     # of a 48-pair case) scaled by this step's DP cells; the algorithmic
+                     # bytes are the 1-byte-per-cell traceback (tb_bytes)
+                     "traffic": NCU_DRAM_BYTES_PER_CELL * cells, "traffic_unit": "bytes per DP phase",
+                     "algorithmic_bytes": st["tb_bytes"],
                      "peak_source": "aw_int16x2_peak_ops() live microbenchmark (chains of FMA-pipe adds and "
                                     "ALU-pipe SIMD max/min on two 16-bit fields per register, "
                                     "2 field-ops per instruction)",
