@@ -9,7 +9,8 @@
 //     AlignmentResourceScheduler.cpp:706 restated for device memory);
 //   * per-thread pooled device/pinned buffers (grow-only) and a private stream
 //     pair, so concurrent host threads never share state (the reference's
-//     one-call-per-worker threading contract, SURVEY boundary table);
+//     one-call-per-worker threading contract: each AnchorTaskExecutor worker
+//     calls ksw_extd2 on its own, src/service/AnchorTaskExecutor.cpp:54, :374);
 //   * CIGAR ownership exactly as ksw_push_cigar (minimap2/ksw2.h:144-154).
 #include "aw_internal.h"
 #include "ksw2_band.h"

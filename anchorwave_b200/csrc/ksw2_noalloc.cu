@@ -20,8 +20,17 @@
 //     serialised by the caller;
 //   * the first call on a device resolves the array's device address with
 //     cudaGetSymbolAddress (this loads the module), so that first call should be
-//     made before any stream capture begins.
+//     made before any stream capture begins; the address is kept for the life of
+//     the process, so the device must not be reset (cudaDeviceReset) between calls;
+//   * the calling thread's deadline (aw_ksw_set_deadline) does not apply here (arming
+//     it needs a device word this entry does not allocate), and the deterministic
+//     stop (aw_ksw_set_stop_antidiagonal) is refused: it runs on the anti-diagonal
+//     kernel, which this entry does not provide;
+//   * a bounded wait between the cooperating warps that gives up (a stalled strip
+//     pipeline) is reported as zdropped = 1 with no CIGAR -- the full-matrix path
+//     never z-drops, so zdropped = 1 from this entry always means that failure.
 #include "aw_internal.h"
+#include "ksw2_exact.h"
 #include "../../include/anchorwave_b200.h"
 
 #include <mutex>
@@ -120,6 +129,11 @@ extern "C" int aw_ksw_extd2_device_noalloc(int qlen, const uint8_t *d_query, int
     if (!d_result || !mat || (qlen > 0 && !d_query) || (tlen > 0 && !d_target)) {
         set_error("aw_ksw_extd2_device_noalloc: null argument");
         return AW_E_INVAL;
+    }
+    if (exact_stop_enabled()) {
+        set_error("aw_ksw_extd2_device_noalloc: the calling thread has a deterministic stop set "
+                  "(aw_ksw_set_stop_antidiagonal), which needs the anti-diagonal kernel; clear it first");
+        return AW_E_UNSUPPORTED;
     }
     KswScore S;
     const int rc = full_path_params(qlen, tlen, m, mat, q, e, q2, e2, flag, &S);

@@ -11,16 +11,21 @@ and the CIGARs.
     plan's stream; GCUPS = total DP cells / time.
   * e2e: the same batch through the public C-ABI call aw_ksw_extd2_batch with host buffers
     (pinned staging, H2D of the sequences, D2H of results and CIGARs) per step.
-  * plain_per_call: the plain per-call GPU form (one ksw_extd2_gpu call per pair) on a sample.
+  * plain_per_call: the plain per-call GPU form (one ksw_extd2_gpu call per pair) on a
+    512-pair sample of the same workload (batched_vs_plain_pairs_per_s compares the two).
+  * plain_5kb: the plain single-pair workload as specified (1,000 seeded 5 kb pairs with a
+    500 bp deletion, one ksw_extd2_gpu call each, p50/p99), beside the compiled reference's
+    per-call latency (single-threaded calls) on the same pairs, results compared.
   * cpu_baseline: AnchorWave's own AVX KSW2 compiled from the reference tree (oracle/_ref),
-    all host threads, bounded sample.
+    all host threads, bounded sample; every pair it finishes is compared field by field
+    (ksw_extz_t + CIGAR, through a result hash) with the device-resident results (parity).
   * roofline: the strip kernel is bound by integer issue; it computes two cells per
     instruction in 16-bit fields, so the achieved op rate (DP cells x 47 reference int ops
     per cell / DP-phase CUDA-event time) is set against the packed-field peak measured live
     by aw_int16x2_peak_ops() (the 32-bit peak, aw_int32_peak_ops(), is reported beside it);
     the traceback store stream is reported against HBM bandwidth.
   * serving: a 20,000-request trace through the continuous-batching server (saturated and at
-    70% offered load with p50/p99 latency).
+    80% offered load with p50/p99 latency).
   * long_banded: 16 pairs of 100-150 kb, w = 10%, banded and Singletrack, beside the
     reference's CPU code on the same pairs.
   * wfa: 16,384 pairs of 100 bp-10 kb (0.5-5%), high memory (standard and Singletrack) and
@@ -29,8 +34,12 @@ and the CIGARs.
     fingerprints) over the headline pairs, beside the compiled selector.
 
 `--impl reference` times the reference CPU implementation (oracle/_ref) on the same workload,
-metric and unit.  With torchrun (N>1) every rank aligns its own batch (weak scaling, no
-collective on the data path); rank 0 prints the line.
+metric and unit: each step is a time-bounded sample that continues where the previous step
+stopped, so the timed steps walk the whole batch.  With torchrun (N>1) every rank aligns its
+own batch (weak scaling, no collective on the data path); rank 0 prints the line.
+
+The line ends with `cpu_baseline` (parity included) and a compact `summary` of the
+sub-measurements (batched vs plain, p50/p99 latencies, parity counts, WFA and long-pair rates).
 """
 from __future__ import annotations
 
@@ -64,7 +73,10 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plain-sample", type=int, default=64)
+    ap.add_argument("--plain-sample", type=int, default=512,
+                    help="pairs of the batched workload aligned one ksw_extd2_gpu call at a time")
+    ap.add_argument("--plain-pairs", type=int, default=1000,
+                    help="pairs of the plain 5 kb workload (0 skips it)")
     ap.add_argument("--serve-requests", type=int, default=20000,
                     help="requests of the serving trace (0 skips the serving measurement)")
     ap.add_argument("--no-long-banded", action="store_true", help="skip the long banded/Singletrack sample")
@@ -178,6 +190,27 @@ def workload(args, rank):
     return W.batched_full_set(args.pairs, seed=args.seed + rank)
 
 
+def run_config(ps, world):
+    """The config dict of both arms (identical keys and values)."""
+    cells = ps.cells()
+    return {"workload": ps.name, "pairs": len(ps), "cells": cells,
+            "scoring": "match 0, mismatch -4, gap 4+2l/24+l", "form": "ksw_extd2 global with CIGAR",
+            "parallelism": f"replicas x{world}",
+            "l2": f"each step writes about {cells / 1e9:.0f} GB of traceback (1 B per cell), far above the "
+                  f"126 MB L2"}
+
+
+def sig(x, digits=4):
+    """Rounds floats to `digits` significant digits (compact summary)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: sig(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [sig(v, digits) for v in x]
+    return x
+
+
 def run_reference_arm(args):
     rank, world, local, pg = dist_init(args.gpus)
     if rank != 0:
@@ -192,21 +225,24 @@ def run_reference_arm(args):
     ps = workload(args, 0)
     mat = oracle.anchorwave_matrix(-4)
     import numpy as np
+    n = len(ps)
     rng = np.random.default_rng(12345)
-    order = rng.permutation(len(ps))
-    qs = [ps.queries[i].tobytes() for i in order]
-    ts = [ps.targets[i].tobytes() for i in order]
-    cells_of = [len(ps.queries[i]) * len(ps.targets[i]) for i in order]
+    order = rng.permutation(n)
     nthreads = os.cpu_count() or 1
     budget = max(2.0, min(30.0, 60.0 / max(1, args.steps + args.warmup)))
+    state = {"start": 0}
 
     def step():
+        # a time-bounded sample that continues where the previous step stopped, so that the
+        # steps walk the whole batch in the seeded order
+        rot = np.roll(order, -state["start"])
+        qs = [ps.queries[i].tobytes() for i in rot]
+        ts = [ps.targets[i].tobytes() for i in rot]
         r = ref.ksw_batch(qs, ts, mat, 4, 2, 24, 1, nthreads=nthreads, time_budget_s=budget)
         # pairs handed out before the deadline are all finished by the time the call returns
-        done = r["done"]
-        hs = r["hash"]
-        finished = [i for i in range(len(qs)) if hs[i] != 0][:done]
-        cells = sum(cells_of[i] for i in finished)
+        finished = [j for j in range(n) if r["hash"][j] != 0][: r["done"]]
+        cells = sum(len(qs[j]) * len(ts[j]) for j in finished)
+        state["start"] = (state["start"] + len(finished)) % n
         return cells, len(finished), r["seconds"]
 
     for _ in range(args.warmup):
@@ -218,16 +254,17 @@ def run_reference_arm(args):
         tot_p += p
         tot_s += s
     gcups = tot_c / tot_s / 1e9
+    sample = (f"each step aligns the workload's pairs in seeded order for {budget:.1f} s, continuing where the "
+              f"previous step stopped ({int(tot_p)} pairs over the {args.steps} timed steps = "
+              f"{tot_p / n:.2f} passes of the {n}-pair batch); ksw_extd2_{ref.isa} from the reference sources")
     line = {"metric": METRIC, "impl": "reference", "value": gcups, "unit": "GCUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
             "data": "synthetic (seeded; stands in for B73/Mo17 intervals)",
             "pairs_per_s": tot_p / tot_s,
-            "config": {"workload": ps.name, "pairs": len(ps), "scoring": "match 0, mismatch -4, gap 4+2l/24+l",
-                       "form": "ksw_extd2 global with CIGAR"},
+            "config": run_config(ps, args.gpus),
             "cpu_baseline": {"value": gcups, "unit": "GCUPS", "cores": nthreads, "kind": "reference",
-                             "sample": f"pairs of the workload in seeded random order, {budget:.1f} s per step, "
-                                       f"ksw_extd2_{ref.isa} from the reference sources"},
+                             "sample": sample},
             "e2e": {"value": gcups, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -238,6 +275,8 @@ def run_reference_arm(args):
 # best saturated rate and 70%-load latency on the trace (more workers split the budget into
 # smaller arenas, so the long banded class runs in more waves).
 SERVE_SLOTS, SERVE_BATCH = 2, 1024
+# offered load of the latency run, as a fraction of the saturated request rate
+SERVE_LOAD = 0.8
 
 
 def serving_measurement(nreq: int, rank: int):
@@ -245,7 +284,7 @@ def serving_measurement(nreq: int, rank: int):
     low-divergence intervals up to 10 kb on WFA, > 20 kb banded KSW2, the rest full KSW2; 10%
     with repeat structure) through the
     continuous-batching server: saturated throughput with all requests queued at once, then
-    p50/p99 latency with Poisson arrivals at 70% of that rate."""
+    p50/p99 latency with Poisson arrivals at 80% of that rate."""
     import numpy as np
 
     from anchorwave_b200 import ksw2, serve
@@ -281,16 +320,16 @@ def serving_measurement(nreq: int, rank: int):
 
     dt_sat, st_sat = run(None)
     sat = len(reqs) / dt_sat
-    dt, st = run(0.7 * sat)
+    dt, st = run(SERVE_LOAD * sat)
     return {"requests": len(reqs), "cells": cells, "saturated_requests_per_s": sat,
             "saturated_gcups": cells / dt_sat / 1e9,
             "saturated_server_requests_per_s": len(reqs) / st_sat["elapsed_s"] if st_sat["elapsed_s"] else None,
-            "offered_requests_per_s": 0.7 * sat,
+            "offered_requests_per_s": SERVE_LOAD * sat, "load": SERVE_LOAD,
             "requests_per_s": len(reqs) / dt, "gcups": cells / dt / 1e9,
             "latency_ms_p50": 1e3 * st["latency_p50_s"], "latency_ms_p99": 1e3 * st["latency_p99_s"],
             "micro_batches": st["micro_batches"], "slots": SERVE_SLOTS, "max_batch": SERVE_BATCH,
             "trace": "log-normal lengths (median 2 kb, sigma 1) clipped to 50 bp-50 kb, WFA for d<=5% "
-                     "and <=10 kb, >20 kb banded (w=10%), 10% repeat-rich; Poisson arrivals at 70% of saturation; "
+                     "and <=10 kb, >20 kb banded (w=10%), 10% repeat-rich; Poisson arrivals at 80% of saturation; "
                      "cells = sum of qlen*tlen"}
 
 
@@ -299,7 +338,8 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
     0.5-5%, penalties x=4, o1=4, e1=2, o2=24, e2=1), standard and Singletrack in high memory
     and the medium-memory (piggyback) mode: pairs/s on the device and through the C call with
     host buffers, device memory per alignment, and the reference's WFA2 code in the same mode
-    on the host cores on the same pairs (scores and CIGAR lengths compared)."""
+    on the host cores on the same pairs (status, score and the whole CIGAR operation string of
+    every pair the reference finished compared)."""
     import numpy as np
 
     from anchorwave_b200 import wfa
@@ -318,7 +358,7 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
         pair_max, total = al.memory()
         al.close()
         st, sc, offs, nops, ops, ms, secs = min(runs, key=lambda r: r[5])
-        dev[name] = (st, sc, nops)
+        dev[name] = (st, sc, offs, nops, ops.raw)
         out[name] = {"device_ms": ms, "pairs_per_s": len(ps) / (ms * 1e-3),
                      "e2e_pairs_per_s": len(ps) / min(r[6] for r in runs),
                      "gcups_equivalent": ps.cells() / (ms * 1e-3) / 1e9,
@@ -336,11 +376,14 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
             # the helper takes (queries, targets) and aligns pattern = target, text = query
             r = ref.wfa_batch(txts, pats, 4, 4, 2, 24, 1, singletrack=stk, time_budget_s=10.0, memory_mode=mem)
             done = [i for i in range(len(ps)) if r["n_ops"][i] > 0]
-            st, sc, nops = dev[name]
-            same = all(st[i] == 0 and sc[i] == r["score"][i] and nops[i] == r["n_ops"][i] for i in done)
+            st, sc, offs, nops, ops = dev[name]
+            rops, roff = r["ops"], r["ops_offset"]
+            # status, score and the whole operation string of every pair the reference finished
+            same = all(st[i] == 0 and sc[i] == r["score"][i] and nops[i] == r["n_ops"][i] and
+                       ops[offs[i]:offs[i] + nops[i]] == rops[roff[i]:roff[i] + nops[i]].tobytes() for i in done)
             cpu_pps = r["done"] / r["seconds"]
             out[name]["cpu_reference"] = {"pairs_per_s": cpu_pps, "threads": r["threads"], "pairs": len(done),
-                                          "scores_and_cigar_lengths_identical": same}
+                                          "status_score_cigar_identical": same}
             out[name]["vs_cpu_reference"] = out[name]["pairs_per_s"] / cpu_pps
     return out
 
@@ -446,7 +489,10 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 16, lmin: int = 
     return out
 
 
-def cpu_baseline(ps, budget):
+def cpu_baseline(ps, budget, res_dev):
+    """The compiled reference (native ISA, all host threads) on the workload in seeded random
+    order for `budget` seconds; every pair it finishes is compared with the device result
+    (all ksw_extz_t fields and the CIGAR, through the shim's result hash)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
 
@@ -461,10 +507,55 @@ def cpu_baseline(ps, budget):
                       time_budget_s=budget)
     done_idx = [i for i in range(len(qs)) if r["hash"][i] != 0]
     cells = sum(len(qs[i]) * len(ts[i]) for i in done_idx)
+    bad = [int(order[i]) for i in done_idx if oracle.result_hash(res_dev[order[i]]) != int(r["hash"][i])]
+    for i in bad[:5]:
+        print(f"[bench] pair {i} differs from the reference", file=sys.stderr)
     return {"value": cells / r["seconds"] / 1e9, "unit": "GCUPS", "cores": nthreads, "kind": "reference",
             "pairs_per_s": len(done_idx) / r["seconds"],
-            "sample": f"{len(done_idx)} pairs of the workload in seeded random order within {budget:.0f} s, "
+            "parity": {"pairs_checked": len(done_idx), "identical": not bad, "differing": len(bad),
+                       "fields": "all ksw_extz_t fields + CIGAR vs the device-resident results"},
+            "sample": f"{len(done_idx)} of {len(ps)} pairs in seeded random order within {budget:.0f} s, "
                       f"ksw_extd2_{ref.isa} compiled from the reference sources, {nthreads} threads"}
+
+
+def plain_measurement(npairs: int, cpu: bool):
+    """The plain single-pair workload: seeded 5 kb pairs (5% substitutions, 1% short indels,
+    one 500 bp deletion), one ksw_extd2_gpu call per pair (host buffers in, malloc'd CIGAR
+    out), per-call latency p50/p99; beside it the compiled reference's per-call latency
+    (each call single-threaded, the calls spread over the host threads) on the same pairs,
+    and every result compared."""
+    import numpy as np
+
+    from anchorwave_b200 import ksw2
+    from anchorwave_b200 import workloads as W
+    ps = W.plain_set(npairs, seed0=0)
+    mat = ksw2.anchorwave_matrix(-4)
+    ksw2.ksw_extd2(ps.queries[0], ps.targets[0], mat, 4, 2, 24, 1)
+    lat, res = [], []
+    for q, t in zip(ps.queries, ps.targets):
+        t0 = time.perf_counter()
+        res.append(ksw2.ksw_extd2(q, t, mat, 4, 2, 24, 1))
+        lat.append(time.perf_counter() - t0)
+    cells = ps.cells()
+    out = {"workload": ps.name, "pairs": len(ps), "cells": cells, "pairs_per_s": len(ps) / sum(lat),
+           "gcups": cells / sum(lat) / 1e9, "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
+           "latency_ms_p99": 1e3 * float(np.percentile(lat, 99))}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        try:
+            ref = oracle.Reference()
+        except FileNotFoundError as e:
+            out["cpu_reference"] = {"unavailable": str(e)}
+            return out
+        r = ref.ksw_batch([q.tobytes() for q in ps.queries], [t.tobytes() for t in ps.targets], mat, 4, 2, 24, 1)
+        ps_sec = r["pair_seconds"]
+        same = all(oracle.result_hash(g) == int(h) for g, h in zip(res, r["hash"]))
+        out["cpu_reference"] = {"latency_ms_p50": 1e3 * float(np.percentile(ps_sec, 50)),
+                                "latency_ms_p99": 1e3 * float(np.percentile(ps_sec, 99)),
+                                "threads": r["threads"], "isa": ref.isa, "results_identical": same,
+                                "pairs_checked": len(ps)}
+    return out
 
 
 def main():
@@ -536,27 +627,28 @@ def main():
     rng = np.random.default_rng(777)
     sample = rng.choice(n, size=min(args.plain_sample, n), replace=False)
     ksw2.ksw_extd2(ps.queries[sample[0]], ps.targets[sample[0]], mat, 4, 2, 24, 1)
-    lat, pc_cells = [], 0
+    lat, pc_cells, pc_same = [], 0, True
     for i in sample:
         t0 = time.perf_counter()
-        ksw2.ksw_extd2(ps.queries[i], ps.targets[i], mat, 4, 2, 24, 1)
+        r1 = ksw2.ksw_extd2(ps.queries[i], ps.targets[i], mat, 4, 2, 24, 1)
         lat.append(time.perf_counter() - t0)
+        pc_same &= r1.key() == res_dev[i].key()
         pc_cells += len(ps.queries[i]) * len(ps.targets[i])
     plain = {"gcups": pc_cells / sum(lat) / 1e9, "pairs_per_s": len(lat) / sum(lat),
              "latency_ms_p50": 1e3 * float(np.percentile(lat, 50)),
-             "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)), "sample_pairs": len(lat)}
+             "latency_ms_p99": 1e3 * float(np.percentile(lat, 99)), "sample_pairs": len(lat),
+             "results_identical_to_batched": pc_same}
+    cpu_on = rank == 0 and not args.no_cpu_baseline
+    plain5 = plain_measurement(args.plain_pairs, cpu_on) if args.plain_pairs > 0 else None
 
     # the batch calls above keep ~100 GB of traceback arena pooled on this thread; give it
     # back before the other workloads size their own device pools
     ksw2.release_thread_buffers()
     serving = serving_measurement(args.serve_requests, rank) if args.serve_requests > 0 else None
     long_banded = None if args.no_long_banded else long_banded_measurement(
-        rank, rank == 0 and not args.no_cpu_baseline, args.long_banded_pairs, args.long_banded_min,
-        args.long_banded_max)
-    wfa_res = (wfa_measurement(args.wfa_pairs, rank, rank == 0 and not args.no_cpu_baseline, args.wfa_pool_gb)
-               if args.wfa_pairs > 0 else None)
-    summary_res = (None if args.no_selector_summary else
-                   selector_summary_measurement(ps, rank, rank == 0 and not args.no_cpu_baseline))
+        rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max)
+    wfa_res = (wfa_measurement(args.wfa_pairs, rank, cpu_on, args.wfa_pool_gb) if args.wfa_pairs > 0 else None)
+    summary_res = (None if args.no_selector_summary else selector_summary_measurement(ps, rank, cpu_on))
 
     if rank != 0:
         barrier(pg)
@@ -566,31 +658,33 @@ def main():
     dp_mean = float(np.mean(dp_ms))
     achieved_ops = cells * OPS_PER_CELL_CIGAR / (dp_mean * 1e-3)
     tb_gbs = st["tb_bytes"] / (dp_mean * 1e-3) / 1e9
+    batched_vs_plain = pairs_per_s / world / plain["pairs_per_s"]
     line = {
         "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8",
         "data": "synthetic (seeded; stands in for B73/Mo17 intervals)",
         "pairs_per_s": pairs_per_s,
-        "config": {"workload": ps.name, "pairs": n, "cells": cells, "scoring": "match 0, mismatch -4, gap 4+2l/24+l",
-                   "form": "ksw_extd2 global with CIGAR", "parallelism": f"replicas x{world}",
-                   "l2": f"each step writes {st['tb_bytes'] / 1e9:.0f} GB of traceback, far above the 126 MB L2",
-                   "waves": st["waves"]},
+        "config": run_config(ps, world),
+        "plan": {"waves": st["waves"], "traceback_bytes": st["tb_bytes"]},
         "latency_ms": {"batch_step_p50": float(np.percentile(step_ms, 50)),
                        "batch_step_p99": float(np.percentile(step_ms, 99)),
                        "serving_p50": serving["latency_ms_p50"] if serving else None,
                        "serving_p99": serving["latency_ms_p99"] if serving else None,
                        "plain_per_call_p50": plain["latency_ms_p50"], "plain_per_call_p99": plain["latency_ms_p99"]},
         "plain_per_call": plain,
-        "batched_vs_plain_pairs_per_s": pairs_per_s / world / plain["pairs_per_s"],
+        "plain_5kb": plain5,
+        "batched_vs_plain_pairs_per_s": batched_vs_plain,
         "phase_ms": {"dp": dp_mean, "traceback": float(np.mean(bt_ms))},
         "roofline": {"bound": "int16x2", "achieved": achieved_ops / 1e12, "peak": simd_peak / 1e12, "unit": "TOPS",
                      "frac": achieved_ops / simd_peak if simd_peak else None,
                      # DRAM bytes of one DP phase: the bytes per DP cell of an ncu capture of
                      # the strip kernel (dram__bytes_read + write, 1.643 GB for 1.64e9 cells
-                     # of a 48-pair case) scaled by this step's DP cells; the algorithmic
-                     # bytes are the 1-byte-per-cell traceback (tb_bytes)
+                     # of a 48-pair case, CIGAR mode) scaled by this step's DP cells; the
+                     # algorithmic bytes are the 1-byte-per-cell traceback (tb_bytes)
                      "traffic": NCU_DRAM_BYTES_PER_CELL * cells, "traffic_unit": "bytes per DP phase",
+                     "traffic_source": "estimate: bytes per DP cell of the CIGAR-mode ncu capture in "
+                                       "profiles/ksw_full_kernel_batched_full.md x this step's cells",
                      "algorithmic_bytes": st["tb_bytes"],
                      "peak_source": "aw_int16x2_peak_ops() live microbenchmark (chains of FMA-pipe adds and "
                                     "ALU-pipe SIMD max/min on two 16-bit fields per register, "
@@ -611,12 +705,61 @@ def main():
     }
     if not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(ps, args.cpu_budget)
+            line["cpu_baseline"] = cpu_baseline(ps, args.cpu_budget, res_dev)
         except FileNotFoundError as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    line["summary"] = compact_summary(line)
     print(json.dumps(line))
     barrier(pg)
     return 0
+
+
+def compact_summary(line):
+    """The sub-measurements in a few hundred characters, last on the line."""
+    def get(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict):
+                return None
+            d = d.get(k)
+        return d
+    out = {"batched_vs_plain_pairs_per_s": line["batched_vs_plain_pairs_per_s"],
+           "batched_pairs_per_s": line["pairs_per_s"],
+           "plain_mixed": {k: line["plain_per_call"][k] for k in ("pairs_per_s", "latency_ms_p50", "latency_ms_p99",
+                                                                 "sample_pairs")}}
+    p5 = line.get("plain_5kb")
+    if p5:
+        out["plain_5kb"] = {"pairs": p5["pairs"], "p50_ms": p5["latency_ms_p50"], "p99_ms": p5["latency_ms_p99"],
+                            "ref_p50_ms": get(p5, "cpu_reference", "latency_ms_p50"),
+                            "ref_p99_ms": get(p5, "cpu_reference", "latency_ms_p99"),
+                            "identical": get(p5, "cpu_reference", "results_identical")}
+    sv = line.get("serving")
+    if sv:
+        out["serving"] = {k: sv.get(k) for k in ("requests", "saturated_requests_per_s", "requests_per_s",
+                                                 "latency_ms_p50", "latency_ms_p99", "load")}
+    par = {"batched_full": get(line, "cpu_baseline", "parity")}
+    if par["batched_full"]:
+        par["batched_full"] = {k: par["batched_full"][k] for k in ("pairs_checked", "identical")}
+    lb = line.get("long_banded")
+    if lb:
+        out["long_banded"] = {"pairs": lb["pairs"]}
+        for nm in ("banded", "singletrack"):
+            if nm in lb:
+                out["long_banded"][nm] = {"gcups": lb[nm].get("gcups"), "vs_ref": lb[nm].get("vs_cpu_reference")}
+                par[f"long_{nm}"] = get(lb, nm, "cpu_reference", "results_identical")
+    wf = line.get("wfa")
+    if wf:
+        out["wfa"] = {}
+        for nm in ("standard", "singletrack", "medium"):
+            if nm in wf:
+                out["wfa"][nm] = {"pairs_per_s": wf[nm]["pairs_per_s"], "vs_ref": wf[nm].get("vs_cpu_reference")}
+                par[f"wfa_{nm}"] = {"pairs_checked": get(wf, nm, "cpu_reference", "pairs"),
+                                    "identical": get(wf, nm, "cpu_reference", "status_score_cigar_identical")}
+    ss = line.get("selector_summary")
+    if ss:
+        out["selector_pass"] = {"bases_per_s": ss.get("e2e_bases_per_s"), "vs_ref": ss.get("vs_cpu_reference")}
+        par["selector_pass"] = get(ss, "cpu_reference", "summaries_identical")
+    out["parity"] = par
+    return sig(out)
 
 
 if __name__ == "__main__":

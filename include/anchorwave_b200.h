@@ -279,10 +279,16 @@ typedef struct {
  * strip-boundary columns do not fit it (about 5,600 x 5,600 cells) are rejected
  * with AW_E_NOMEM.  Calls share that array: calls whose GPU work overlaps race
  * and must be serialised by the caller.  The first call on a device resolves the
- * array's address (cudaGetSymbolAddress), so make it before any stream capture.
+ * array's address (cudaGetSymbolAddress), so make it before any stream capture;
+ * the address is kept until exit, so do not reset the device between calls.
  * Flags beyond SCORE_ONLY / RIGHT / GENERIC_SC / REV_CIGAR / SEMIGLOBAL_END, and
  * parameters outside the strip kernel's exact int8 envelope, return
- * AW_E_UNSUPPORTED.  Returns AW_OK or a negative AW_E* code (aw_last_error()).
+ * AW_E_UNSUPPORTED, and so does a deterministic stop set on the calling thread
+ * (aw_ksw_set_stop_antidiagonal); the thread's deadline (aw_ksw_set_deadline) is
+ * not applied.  The full-matrix path never z-drops, so d_result->zdropped = 1
+ * (with n_cigar = 0) means that a bounded wait between the cooperating warps gave
+ * up; the call itself has already returned AW_OK by then, as the work is only
+ * enqueued.  Returns AW_OK or a negative AW_E* code (aw_last_error()).
  */
 int aw_ksw_extd2_device_noalloc(int qlen, const uint8_t *d_query, int tlen, const uint8_t *d_target,
                                 int8_t m, const int8_t *mat, int8_t q, int8_t e, int8_t q2, int8_t e2,

@@ -210,11 +210,12 @@ class Reference:
         L.awref_ksw_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p,
-                                      C.c_void_p, C.POINTER(C.c_int)]
+                                      C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
         L.awref_wfa_batch.restype = C.c_double
         L.awref_wfa_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                      C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+                                      C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.POINTER(C.c_int)]
         assert L.awref_sizeof_extz() == C.sizeof(KswExtz)
         self.has_summary = hasattr(L, "awref_sequence_summary")
         if self.has_summary:
@@ -259,14 +260,15 @@ class Reference:
         score = np.zeros(max(n, 1), dtype=np.int32)
         ncig = np.zeros(max(n, 1), dtype=np.int32)
         hsh = np.zeros(max(n, 1), dtype=np.uint64)
+        psec = np.zeros(max(n, 1), dtype=np.float64)
         done = C.c_int(0)
         matc = _i8(mat)
         secs = self.lib.awref_ksw_batch(n, ql.ctypes.data, qoff.ctypes.data, qbuf.ctypes.data, tl.ctypes.data,
                                         toff.ctypes.data, tbuf.ctypes.data, matc, q, e, q2, e2, w, flag, variant,
                                         nthreads, time_budget_s, score.ctypes.data, ncig.ctypes.data,
-                                        hsh.ctypes.data, C.byref(done))
-        return {"score": score[:n], "n_cigar": ncig[:n], "hash": hsh[:n], "seconds": secs, "done": done.value,
-                "threads": nthreads}
+                                        hsh.ctypes.data, psec.ctypes.data, C.byref(done))
+        return {"score": score[:n], "n_cigar": ncig[:n], "hash": hsh[:n], "pair_seconds": psec[:n],
+                "seconds": secs, "done": done.value, "threads": nthreads}
 
     def wfa_batch(self, queries, targets, x, o1, e1, o2, e2, singletrack=False, nthreads=None,
                   time_budget_s=0.0, memory_mode=0):
@@ -285,13 +287,18 @@ class Reference:
         tbuf = np.frombuffer(b"".join(targets) or b"\0", dtype=np.uint8).copy()
         score = np.zeros(max(n, 1), dtype=np.int32)
         nops = np.zeros(max(n, 1), dtype=np.int32)
+        ooff = np.zeros(max(n, 1), dtype=np.int64)
+        if n:
+            ooff[1:n] = np.cumsum(ql[:-1].astype(np.int64) + tl[:-1] + 8)
+        obuf = np.zeros(int(ooff[n - 1] + ql[-1] + tl[-1] + 8) if n else 1, dtype=np.uint8)
         done = C.c_int(0)
         secs = self.lib.awref_wfa_batch(n, ql.ctypes.data, qoff.ctypes.data, qbuf.ctypes.data, tl.ctypes.data,
                                         toff.ctypes.data, tbuf.ctypes.data, x, o1, e1, o2, e2,
                                         int(bool(singletrack)), int(memory_mode), nthreads, time_budget_s,
-                                        score.ctypes.data,
-                                        nops.ctypes.data, C.byref(done))
-        return {"score": score[:n], "n_ops": nops[:n], "seconds": secs, "done": done.value, "threads": nthreads}
+                                        score.ctypes.data, nops.ctypes.data, obuf.ctypes.data, ooff.ctypes.data,
+                                        C.byref(done))
+        return {"score": score[:n], "n_ops": nops[:n], "ops": obuf, "ops_offset": ooff[:n], "seconds": secs,
+                "done": done.value, "threads": nthreads}
 
     def sequence_summary(self, query: bytes, reference: bytes, modulos=None):
         """The compiled selector's summarizeSequencePair (ref_selector_shim.cpp)."""

@@ -166,6 +166,9 @@ typedef struct {
     int wfa_x, wfa_o1, wfa_e1, wfa_o2, wfa_e2, wfa_singletrack, wfa_memory_mode;
     int32_t *score_out, *ncig_out;
     uint64_t *hash_out;
+    double *sec_out;          /* per-pair seconds of the call (optional) */
+    char *ops_out;            /* WFA: operations of pair i at ops_off[i] (optional) */
+    const int64_t *ops_off;
     double deadline;          /* CLOCK_MONOTONIC seconds; <= 0 disables */
     volatile int next;
     volatile int done;
@@ -191,9 +194,11 @@ static void *awref_batch_worker(void *arg) {
         if (b->kind == 0) {
             ksw_extz_t ez;
             memset(&ez, 0, sizeof(ez));
+            const double t0 = b->sec_out ? awref_now() : 0;
             awref_ksw_extd2(b->variant, b->qlen[i], qs, b->tlen[i], ts, 5, b->mat,
                             (int8_t)b->q, (int8_t)b->e, (int8_t)b->q2, (int8_t)b->e2,
                             b->w, -1, 0, b->flag, &ez);
+            if (b->sec_out) b->sec_out[i] = awref_now() - t0;
             if (b->score_out) b->score_out[i] = ez.score;
             if (b->ncig_out) b->ncig_out[i] = ez.n_cigar;
             if (b->hash_out) b->hash_out[i] = awref_extz_hash(&ez);
@@ -204,10 +209,13 @@ static void *awref_batch_worker(void *arg) {
             int need = b->qlen[i] + b->tlen[i] + 8;
             if (need > ops_cap) { free(ops); ops_cap = need; ops = (char *)malloc((size_t)ops_cap); }
             int sc = 0, nops = 0;
+            const double t0 = b->sec_out ? awref_now() : 0;
             int st = awref_wfa_run(al, (const char *)ts, b->tlen[i], (const char *)qs,
                                    b->qlen[i], &sc, ops, ops_cap, &nops);
+            if (b->sec_out) b->sec_out[i] = awref_now() - t0;
             if (b->score_out) b->score_out[i] = st == 0 ? sc : INT32_MIN;
             if (b->ncig_out) b->ncig_out[i] = nops;
+            if (b->ops_out && st == 0) memcpy(b->ops_out + b->ops_off[i], ops, (size_t)nops);
         }
         __sync_fetch_and_add(&b->done, 1);
     }
@@ -231,36 +239,40 @@ static double awref_run_batch(awref_batch_t *b, int nthreads, int *n_done) {
 /* KSW2 over a pair list with nthreads workers pulling indices from a shared
  * counter (the AnchorTaskExecutor pattern).  Sequences are 0..4 codes packed
  * back to back; qoff/toff give each pair's start.  Stops taking new pairs after
- * time_budget_s (<= 0: no budget).  Returns wall seconds. */
+ * time_budget_s (<= 0: no budget).  Per pair (each optional): score, n_cigar, the
+ * result hash (awref_extz_hash) and the seconds of its call.  Returns wall seconds. */
 double awref_ksw_batch(int n, const int *qlen, const int64_t *qoff, const uint8_t *qbuf,
                        const int *tlen, const int64_t *toff, const uint8_t *tbuf,
                        const int8_t *mat, int q, int e, int q2, int e2, int w, int flag,
                        int variant, int nthreads, double time_budget_s,
-                       int32_t *score_out, int32_t *ncig_out, uint64_t *hash_out, int *n_done) {
+                       int32_t *score_out, int32_t *ncig_out, uint64_t *hash_out, double *sec_out,
+                       int *n_done) {
     awref_batch_t b;
     memset(&b, 0, sizeof(b));
     b.kind = 0; b.n = n; b.qlen = qlen; b.tlen = tlen; b.qoff = qoff; b.toff = toff;
     b.qbuf = qbuf; b.tbuf = tbuf; b.mat = mat; b.q = q; b.e = e; b.q2 = q2; b.e2 = e2;
     b.w = w; b.flag = flag; b.variant = variant; b.score_out = score_out; b.ncig_out = ncig_out;
-    b.hash_out = hash_out;
+    b.hash_out = hash_out; b.sec_out = sec_out;
     b.deadline = time_budget_s > 0 ? awref_now() + time_budget_s : 0;
     return awref_run_batch(&b, nthreads, n_done);
 }
 
 /* WFA over a pair list (ASCII sequences; pattern = target/reference, text =
  * query), one thread-local aligner per worker (standard or Singletrack in high
- * memory, or the medium / low piggyback modes). */
+ * memory, or the medium / low piggyback modes).  ops_out (optional) receives pair
+ * i's CIGAR operations at ops_off[i] (room for qlen + tlen + 8 characters each). */
 double awref_wfa_batch(int n, const int *qlen, const int64_t *qoff, const uint8_t *qbuf,
                        const int *tlen, const int64_t *toff, const uint8_t *tbuf,
                        int x, int o1, int e1, int o2, int e2, int singletrack, int memory_mode,
                        int nthreads, double time_budget_s,
-                       int32_t *score_out, int32_t *nops_out, int *n_done) {
+                       int32_t *score_out, int32_t *nops_out, char *ops_out, const int64_t *ops_off,
+                       int *n_done) {
     awref_batch_t b;
     memset(&b, 0, sizeof(b));
     b.kind = 1; b.n = n; b.qlen = qlen; b.tlen = tlen; b.qoff = qoff; b.toff = toff;
     b.qbuf = qbuf; b.tbuf = tbuf; b.wfa_x = x; b.wfa_o1 = o1; b.wfa_e1 = e1;
     b.wfa_o2 = o2; b.wfa_e2 = e2; b.wfa_singletrack = singletrack; b.wfa_memory_mode = memory_mode;
-    b.score_out = score_out; b.ncig_out = nops_out;
+    b.score_out = score_out; b.ncig_out = nops_out; b.ops_out = ops_out; b.ops_off = ops_off;
     b.deadline = time_budget_s > 0 ? awref_now() + time_budget_s : 0;
     return awref_run_batch(&b, nthreads, n_done);
 }
