@@ -32,8 +32,24 @@ EXPORTS = [
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
     "wavefront_align_batch_gpu", "wavefront_gpu_memory", "aw_sequence_summary_batch",
     "aw_sequence_summary_sketches", "aw_sequence_summary_sketch_view", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
-    "aw_serve_result_free", "aw_serve_close",
+    "aw_serve_result_free", "aw_serve_close", "wavefront_aligner_new_wfa2_gpu", "wavefront_align_wfa2_gpu",
+    "wavefront_aligner_delete_wfa2_gpu", "wavefront_aligner_attr_default_gpu", "aw_align_score_certified_batch",
+    "aw_certified_result_free", "aw_align_sliding_window_batch", "aw_window_result_free",
 ]
+
+
+class CertResultC(C.Structure):
+    """aw_certified_result_t (include/anchorwave_b200.h)."""
+    _fields_ = [("status", C.c_int), ("score", C.c_int64), ("optimal_score", C.c_int64),
+                ("final_band_width", C.c_int64), ("traceback_attempts", C.c_int64),
+                ("alignment_q", C.c_void_p), ("alignment_d", C.c_void_p), ("alignment_len", C.c_int64),
+                ("best_effort_q", C.c_void_p), ("best_effort_d", C.c_void_p), ("best_effort_len", C.c_int64)]
+
+
+class WindowResultC(C.Structure):
+    """aw_window_result_t (include/anchorwave_b200.h)."""
+    _fields_ = [("score", C.c_int64), ("alignment_q", C.c_void_p), ("alignment_d", C.c_void_p),
+                ("alignment_len", C.c_int64)]
 
 
 class ServeConfig(C.Structure):
@@ -112,6 +128,16 @@ def _load(path: str = LIB_PATH):
     lib.aw_ksw_plan_graph.restype = i32
     lib.aw_cigar_rows_batch.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64]
     lib.aw_cigar_rows_batch.restype = i32
+    lib.aw_align_score_certified_batch.argtypes = [i32, vp, vp, vp, vp, i64, i64, i32, i32, i32, i32, i32,
+                                                   C.c_double, vp, C.POINTER(CertResultC)]
+    lib.aw_align_score_certified_batch.restype = i32
+    lib.aw_certified_result_free.argtypes = [C.POINTER(CertResultC)]
+    lib.aw_certified_result_free.restype = None
+    lib.aw_align_sliding_window_batch.argtypes = [i32, vp, vp, vp, vp, i64, i32, i32, i32, i32, i32, i32,
+                                                  C.POINTER(WindowResultC)]
+    lib.aw_align_sliding_window_batch.restype = i32
+    lib.aw_window_result_free.argtypes = [C.POINTER(WindowResultC)]
+    lib.aw_window_result_free.restype = None
     lib.aw_int32_peak_ops.argtypes = []
     lib.aw_int32_peak_ops.restype = C.c_double
     lib.aw_int16x2_peak_ops.argtypes = []

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libaw_b200.so")
-SOURCES = ["ksw2_full.cu", "ksw2_band.cu", "ksw2_exact.cu", "ksw2_api.cu", "ksw2_noalloc.cu", "wfa.cu", "wfa_api.cu", "serve.cu", "peak.cu", "rows.cu", "summary.cu"]
+SOURCES = ["ksw2_full.cu", "ksw2_band.cu", "ksw2_exact.cu", "ksw2_api.cu", "ksw2_noalloc.cu", "wfa.cu", "wfa_api.cu",
+           "wfa2_compat.cu", "serve.cu", "peak.cu", "rows.cu", "rescue.cu", "summary.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

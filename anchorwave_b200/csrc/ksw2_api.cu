@@ -320,6 +320,7 @@ struct aw_ksw_plan {
     std::vector<int32_t> exact_ids;  // pairs for the exact kernel
     std::vector<int32_t> band_ids;   // pairs for the banded kernel
     BandPlan band;
+    int refused = 0;                 // Singletrack pairs refused for the budget (reported zdropped)
     int64_t tb_cap = 0, bnd_cap = 0;
     int64_t cells = 0, tb_total = 0;
     int launches = 0;
@@ -469,10 +470,22 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
         pl->waves.push_back(W);
     }
     if (!pl->band_ids.empty()) {
+        std::vector<int32_t> refused;
         if (band_plan_build(pl->band, pl->band_ids, pl->qlen, pl->tlen, pl->w, pl->pairs, P.flag, exact_block(),
-                            budget, band_columns(pl))) {
+                            budget, band_columns(pl), &refused)) {
             set_error("pair traceback exceeds the HBM traceback budget");
             return AW_E_NOMEM;
+        }
+        if (!refused.empty()) {
+            // Singletrack pairs beyond the budget: the reference's allocation-failure result
+            // (ksw2_extd2_avx.c:206-210), the other pairs of the batch run as planned
+            for (int32_t i : refused) pl->route[i] = 0, pl->early_zdrop[i] = 1;
+            pl->band_ids.erase(std::remove_if(pl->band_ids.begin(), pl->band_ids.end(),
+                                              [&](int32_t i) { return pl->route[i] != 3; }),
+                               pl->band_ids.end());
+            pl->refused = (int)refused.size();
+            set_error("Singletrack traceback of a pair exceeds the HBM traceback budget: pair reported "
+                      "as zdropped (allocation failure)");
         }
         pl->tb_cap = std::max(pl->tb_cap, pl->band.tb_cap);
         pl->tb_total += pl->band.tb_total;

@@ -755,6 +755,9 @@ void *band_kernel_for(int flag, int block) {
 
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Device bytes of a pair's boundary columns (entries rounded as the wave packs them).
+int64_t band_bnd_bytes(int64_t entries) { return (entries + 31) / 32 * 32 * (int64_t)sizeof(uint2); }
+
 }  // namespace
 
 int band_break(int qlen, int tlen, int w) {
@@ -792,7 +795,7 @@ int64_t band_cells(int qlen, int tlen, int w) {
 
 int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::vector<int> &qlen,
                     const std::vector<int> &tlen, const std::vector<int> &w, const std::vector<KswPair> &pairs,
-                    int flag, int block, int64_t tb_budget, int nc) {
+                    int flag, int block, int64_t tb_budget, int nc, std::vector<int32_t> *refused) {
     bp = BandPlan();
     bp.block = block;
     bp.nc = nc == 4 ? 4 : 8;
@@ -804,12 +807,13 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
     struct PairGeo {
         int32_t id, ww, rb;
         int64_t tb, bnd;
-        bool ckpt = false;
+        bool ckpt = false, refused = false;
         std::vector<BandStripDev> strips;
         std::vector<int64_t> start;  // estimated start step of each strip
         std::vector<int64_t> stb;    // traceback bytes of each strip
         std::vector<std::pair<int, int>> groups;  // recomputed pairs: strip groups [s0, s1)
         std::vector<int64_t> gtb;
+        int64_t gtb_max = 0;
     };
     std::vector<PairGeo> geo(ids.size());
     for (size_t a = 0; a < ids.size(); ++a) {
@@ -855,23 +859,32 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             G.start.push_back(T);
         }
         G.tb = (G.tb + 255) / 256 * 256;
-        bp.tb_total += G.tb;
-        bp.cells += band_cells(ql, tl, ww);
-        if (G.tb > tb_budget) {
+        const int64_t bnd_bytes = band_bnd_bytes(G.bnd);
+        if (G.tb + bnd_bytes > tb_budget) {
             // Traceback beyond the budget: the first pass stores only the strips' boundary
-            // columns; the walk then recomputes groups of strips that fit the budget, from
-            // the last group to the first, each from the stored column on its left.  The
-            // Singletrack reconstruction probes arbitrarily far left in one gap search, so it
-            // is not split this way.
-            if (st) return AW_E_NOMEM_INTERNAL;
+            // columns; the walk then recomputes groups of strips, from the last group to the
+            // first, each from the stored column on its left.  Groups take at most half of
+            // the budget, so that the boundary columns of the pairs of a wave fit beside
+            // them.  The Singletrack reconstruction probes arbitrarily far left in one gap
+            // search, so it is not split this way: such a pair is refused like an allocation
+            // failure of the reference (ksw2_extd2_avx.c:206-210: reset result, zdropped = 1).
+            const int64_t gbudget = tb_budget / 2;
+            bool fits = !st && bnd_bytes <= tb_budget - gbudget;
+            for (int s = 0; fits && s < (int)G.strips.size(); ++s) fits = G.stb[s] <= gbudget;
+            if (!fits) {
+                if (!refused) return AW_E_NOMEM_INTERNAL;
+                G.refused = true;
+                refused->push_back(G.id);
+                continue;
+            }
             G.ckpt = true;
             int s0 = 0;
             int64_t acc = 0;
             for (int s = 0; s < (int)G.strips.size(); ++s) {
-                if (G.stb[s] > tb_budget) return AW_E_NOMEM_INTERNAL;
-                if (acc + G.stb[s] > tb_budget) {
+                if (acc + G.stb[s] > gbudget) {
                     G.groups.push_back({s0, s});
                     G.gtb.push_back(acc);
+                    G.gtb_max = std::max(G.gtb_max, acc);
                     s0 = s, acc = 0;
                 }
                 G.strips[s].tb_off = acc;  // relative to the group's buffer
@@ -879,28 +892,41 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             }
             G.groups.push_back({s0, (int)G.strips.size()});
             G.gtb.push_back(acc);
+            G.gtb_max = std::max(G.gtb_max, acc);
             G.tb = 0;  // the first pass stores no traceback
         }
+        bp.tb_total += G.tb;
+        bp.cells += band_cells(ql, tl, ww);
     }
-    // pairs largest first into the fewest waves under the budget (LPT multiway fit)
-    std::vector<size_t> ord(ids.size());
-    for (size_t a = 0; a < ord.size(); ++a) ord[a] = a;
+    // pairs largest first into the fewest waves under the budget (LPT multiway fit).  A
+    // wave holds its pairs' boundary columns for the whole wave, and its traceback arena
+    // serves first the pairs stored in full, then (after their walks) one group of a
+    // recomputed pair at a time: bnd + max(tb, largest group) <= budget.
+    std::vector<size_t> ord;
+    for (size_t a = 0; a < ids.size(); ++a)
+        if (!geo[a].refused) ord.push_back(a);
     std::sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
         const int64_t cx = (int64_t)qlen[geo[x].id] * geo[x].ww, cy = (int64_t)qlen[geo[y].id] * geo[y].ww;
         return cx != cy ? cx > cy : geo[x].id < geo[y].id;
     });
     std::vector<std::vector<size_t>> wv;
-    std::vector<int64_t> wload;
+    std::vector<int64_t> wtb, wbnd, wgtb;
+    auto foot = [&](int64_t tb, int64_t bnd, int64_t gtb) { return bnd + std::max(tb, gtb); };
     for (size_t a : ord) {
+        const PairGeo &G = geo[a];
+        const int64_t pb = band_bnd_bytes(G.bnd);
         int best = -1;
-        for (size_t k = 0; k < wv.size(); ++k)
-            if (wload[k] + geo[a].tb <= tb_budget && (best < 0 || wload[k] < wload[best])) best = (int)k;
+        for (size_t k = 0; k < wv.size(); ++k) {
+            const int64_t f = foot(wtb[k] + G.tb, wbnd[k] + pb, std::max(wgtb[k], G.gtb_max));
+            if (f <= tb_budget && (best < 0 || foot(wtb[k], wbnd[k], wgtb[k]) < foot(wtb[best], wbnd[best], wgtb[best])))
+                best = (int)k;
+        }
         if (best < 0) {
             wv.emplace_back();
-            wload.push_back(0);
+            wtb.push_back(0), wbnd.push_back(0), wgtb.push_back(0);
             best = (int)wv.size() - 1;
         }
-        wload[best] += geo[a].tb;
+        wtb[best] += G.tb, wbnd[best] += pb, wgtb[best] = std::max(wgtb[best], G.gtb_max);
         wv[best].push_back(a);
     }
     for (size_t k = 0; k < wv.size(); ++k) {

@@ -82,12 +82,14 @@ int band_break(int qlen, int tlen, int w);
 // Sum over anti-diagonals of the in-band cell count en0-st0+1 up to the band break.
 int64_t band_cells(int qlen, int tlen, int w);
 
-// Builds the strip geometry, traceback waves (each under tb_budget bytes) and the
-// processing order of the given pairs.  Returns AW_E_NOMEM_INTERNAL when one pair's
-// traceback alone exceeds the budget.
+// Builds the strip geometry, waves (each wave's boundary columns plus its traceback arena
+// under tb_budget bytes) and the processing order of the given pairs.  A pair that cannot
+// run within the budget even with its traceback recomputed group by group (Singletrack
+// pairs cannot be split) is appended to *refused and left out of the plan; with refused ==
+// nullptr the build fails with AW_E_NOMEM_INTERNAL instead.
 int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::vector<int> &qlen,
                     const std::vector<int> &tlen, const std::vector<int> &w, const std::vector<KswPair> &pairs,
-                    int flag, int block, int64_t tb_budget, int nc);
+                    int flag, int block, int64_t tb_budget, int nc, std::vector<int32_t> *refused);
 
 // Progress counters sit one 128-byte line apart (one line per strip).
 constexpr int PROG_STRIDE = 32;

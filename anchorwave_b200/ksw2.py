@@ -21,7 +21,7 @@ from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from ._lib import AwError, KswExtz, check, last_error, lib, libc
+from ._lib import AwError, CertResultC, KswExtz, WindowResultC, check, last_error, lib, libc
 
 KSW_NEG_INF = -0x40000000
 KSW_EZ_SCORE_ONLY = 0x01
@@ -450,152 +450,58 @@ class CertifiedResult:
     alignment_d: str = ""
 
 
-def _reconstructs(aln: str, seq: str) -> bool:
-    """gappedAlignmentReconstructs (alignSlidingWindow.cpp:662-675)."""
-    return aln.replace("-", "") == seq
+def _seq_arrays(seqs):
+    """ASCII sequences as (pointer array, lengths, keep-alive buffers) for the C entries."""
+    bufs = [C.create_string_buffer(x.encode() if isinstance(x, str) else bytes(x),
+                                   len(x) + 1) for x in seqs]
+    ptrs = (C.c_void_p * max(1, len(bufs)))(*[C.addressof(b) for b in bufs])
+    lens = np.array([len(x) for x in seqs] or [0], dtype=np.int64)
+    return ptrs, lens, bufs
 
 
-def _band_schedule(len_diff: int, initial: int, maximum_band: int):
-    """The bands alignScoreCertifiedKsw2 tries, in order (alignSlidingWindow.cpp:1296-1347),
-    and the smallest band it evaluates only when all of them fail (:1351-1352)."""
-    requested = max(len_diff, max(1, initial))
-    doubled = requested * 2
-    bands = []
-    band = min(maximum_band, max(requested, doubled))
-    while len_diff <= band <= maximum_band:
-        bands.append(band)
-        if band == maximum_band:
-            break
-        nxt = min(maximum_band, max(band + 1, band * 2))
-        if nxt <= band:
-            break
-        band = nxt
-    fallback = requested if requested < min(maximum_band, doubled) else None
-    return bands, fallback, (bands[-1] if bands else band)
+_CERT_STATUS = {0: CERT_COMPLETED, 1: CERT_TIME_LIMIT, 2: CERT_NOT_CERTIFIED, 3: CERT_FAILED}
 
 
-def _banded_rows(results, dna_q, dna_d, pen):
-    """alignSlidingWindow_minimap2's decoding and re-scoring (alignSlidingWindow.cpp:855-884)
-    of one banded result; rows stay empty when the band does not reach the end."""
-    mis, o1, e1, o2, e2 = pen
-    try:
-        aq, ad, _, _ = decode_cigar(results.cigar, dna_q, dna_d)
-    except ValueError:
-        aq, ad = "", ""
-    return score_gapped_two_piece_affine(aq, ad, mis, o1, e1, o2, e2), aq, ad
+def _text(ptr, n) -> str:
+    return C.string_at(ptr, n).decode() if ptr and n > 0 else ""
 
 
 def align_score_certified_ksw2_batch(pairs, initial_band_width: int, maximum_band_width: int,
                                      mismatching_penalty: int, open1: int, extend1: int, open2: int, extend2: int,
                                      maximum_runtime_seconds: float = 0.0,
                                      precomputed_optimal_scores=None) -> List[CertifiedResult]:
-    """alignScoreCertifiedKsw2 (alignSlidingWindow.cpp:1197-1400) for many intervals at once:
-    one score-only batch gives every optimal score, then the i-th band of every interval
-    not yet certified runs as one banded batch, until a band's re-scored alignment reaches the
-    optimal score.  Each interval gets the result a call of its own would give.  The
-    selector's chained traceback (a selection plan) stays on the caller's side.  Penalties
-    are AnchorWave's (negative); maximum_runtime_seconds > 0 arms the cooperative stop."""
-    pen = (mismatching_penalty, open1, extend1, open2, extend2)
-    mat = anchorwave_matrix(mismatching_penalty)
+    """alignScoreCertifiedKsw2 (alignSlidingWindow.cpp:1197-1400) for many intervals at once,
+    through aw_align_score_certified_batch: one score-only batch gives every optimal score,
+    then the next band of every interval not yet certified runs as one banded batch, until
+    a band's re-scored alignment reaches the optimal score.  Each interval gets the result
+    a call of its own would give.  The selector's chained traceback (a selection plan) stays
+    on the caller's side.  Penalties are AnchorWave's (negative); maximum_runtime_seconds > 0
+    arms the cooperative stop."""
     n = len(pairs)
-    out = [CertifiedResult() for _ in range(n)]
-    todo = []
-    for i, (dq, dd) in enumerate(pairs):
-        r = out[i]
-        if min(len(dq), len(dd)) == 0:
-            r.alignment_q = dq if dq else "-" * len(dd)
-            r.alignment_d = dd if dd else "-" * len(dq)
-            r.score = ksw2_score_only(dq, dd, *pen)[0]
-            r.optimal_score, r.final_band_width, r.traceback_attempts, r.status = r.score, 0, 1, CERT_COMPLETED
-        elif initial_band_width < 0 or maximum_band_width < 0 or maximum_band_width < abs(len(dq) - len(dd)):
-            r.status = CERT_NOT_CERTIFIED
-        else:
-            todo.append(i)
-
-    def run(ids, bands, flag_extra):
-        """One batched call per scoring flag (GENERIC_SC when a base is not ACGT)."""
-        res = {}
-        groups = {}
-        for i, b in zip(ids, bands):
-            qs, f1 = encode(pairs[i][0])
-            ts, f2 = encode(pairs[i][1])
-            groups.setdefault(f1 | f2, []).append((i, qs, ts, b))
-        for f, g in groups.items():
-            rr = ksw_extd2_batch([x[1] for x in g], [x[2] for x in g], mat, -open1, -extend1, -open2, -extend2,
-                                 w=[x[3] for x in g], flag=f | flag_extra)
-            for (i, _, _, _), r in zip(g, rr):
-                res[i] = r
-        return res
-
-    with deadline(maximum_runtime_seconds if maximum_runtime_seconds and maximum_runtime_seconds > 0 else 0.0):
-        if precomputed_optimal_scores is not None:
-            for i in todo:
-                out[i].optimal_score = int(precomputed_optimal_scores[i])
-        else:
-            sc = run(todo, [-1] * len(todo), KSW_EZ_SCORE_ONLY)
-            for i in todo:
-                out[i].optimal_score = sc[i].score
-                if sc[i].stopped:
-                    out[i].status = CERT_TIME_LIMIT
-        active = []
-        plan = {}
-        for i in todo:
-            r = out[i]
-            if r.status == CERT_TIME_LIMIT:
-                continue
-            if r.optimal_score == KSW_NEG_INF:
-                r.status = CERT_FAILED
-                continue
-            dq, dd = pairs[i]
-            maximum_band = min(max(len(dq), len(dd)), maximum_band_width)
-            plan[i] = _band_schedule(abs(len(dq) - len(dd)), initial_band_width, maximum_band)
-            active.append(i)
-        step = 0
-        done = set()
-        while True:
-            ids = [i for i in active if i not in done and step < len(plan[i][0])]
-            if not ids:
-                break
-            rr = run(ids, [plan[i][0][step] for i in ids], 0)
-            for i in ids:
-                r = out[i]
-                r.traceback_attempts += 1
-                if rr[i].stopped:
-                    r.status = CERT_TIME_LIMIT
-                    done.add(i)
-                    continue
-                s, aq, ad = _banded_rows(rr[i], pairs[i][0], pairs[i][1], pen)
-                valid = len(aq) == len(ad) and _reconstructs(aq, pairs[i][0]) and _reconstructs(ad, pairs[i][1])
-                if s == r.optimal_score and valid:
-                    r.score, r.final_band_width, r.alignment_q, r.alignment_d = s, plan[i][0][step], aq, ad
-                    r.status = CERT_COMPLETED
-                    done.add(i)
-                elif valid and (not r.best_effort_query_alignment or s > r.score):
-                    r.score, r.best_effort_query_alignment, r.best_effort_reference_alignment = s, aq, ad
-            step += 1
-        # the smallest band, evaluated only on failure (alignSlidingWindow.cpp:1351-1393)
-        ids = [i for i in active if i not in done and plan[i][1] is not None]
-        rr = run(ids, [plan[i][1] for i in ids], 0) if ids else {}
-        for i in ids:
-            r = out[i]
-            r.traceback_attempts += 1
-            if rr[i].stopped:
-                r.status = CERT_TIME_LIMIT
-                done.add(i)
-                continue
-            s, aq, ad = _banded_rows(rr[i], pairs[i][0], pairs[i][1], pen)
-            valid = len(aq) == len(ad) and _reconstructs(aq, pairs[i][0]) and _reconstructs(ad, pairs[i][1])
-            if s == r.optimal_score and valid:
-                r.score, r.final_band_width, r.alignment_q, r.alignment_d = s, plan[i][1], aq, ad
-                r.status = CERT_COMPLETED
-                done.add(i)
-            elif valid and (not r.best_effort_query_alignment or s > r.score):
-                r.score, r.best_effort_query_alignment, r.best_effort_reference_alignment = s, aq, ad
-        for i in active:
-            if i not in done:
-                out[i].final_band_width = plan[i][2]
-                out[i].status = CERT_NOT_CERTIFIED
-    return out
+    if n == 0:
+        return []
+    qp, ql, qb = _seq_arrays([p[0] for p in pairs])
+    rp, rl, rb = _seq_arrays([p[1] for p in pairs])
+    pre = None
+    if precomputed_optimal_scores is not None:
+        pre = np.ascontiguousarray(np.asarray(precomputed_optimal_scores, dtype=np.int64))
+    out = (CertResultC * n)()
+    rc = lib.aw_align_score_certified_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, int(initial_band_width),
+                                            int(maximum_band_width), mismatching_penalty, open1, extend1, open2,
+                                            extend2, float(maximum_runtime_seconds or 0.0),
+                                            pre.ctypes.data if pre is not None else None, out)
+    res = []
+    for o in out:
+        r = CertifiedResult(status=_CERT_STATUS[o.status], score=o.score, optimal_score=o.optimal_score,
+                            final_band_width=o.final_band_width, traceback_attempts=o.traceback_attempts,
+                            alignment_q=_text(o.alignment_q, o.alignment_len),
+                            alignment_d=_text(o.alignment_d, o.alignment_len),
+                            best_effort_query_alignment=_text(o.best_effort_q, o.best_effort_len),
+                            best_effort_reference_alignment=_text(o.best_effort_d, o.best_effort_len))
+        lib.aw_certified_result_free(C.byref(o))
+        res.append(r)
+    check(rc, "aw_align_score_certified_batch")
+    return res
 
 
 def align_score_certified_ksw2(dna_q: str, dna_d: str, initial_band_width: int, maximum_band_width: int,
@@ -610,103 +516,32 @@ def align_score_certified_ksw2(dna_q: str, dna_d: str, initial_band_width: int, 
 
 # ---- sliding-window semiglobal alignment (alignSlidingWindow.cpp:457-590) ----------------
 
-def _subsequence(seq: str, start: int, end: int) -> str:
-    """getSubsequence (src/impl/getSubsequence.cpp:191-211): 1-based inclusive, clamped."""
-    if not seq:
-        return ""
-    if start > end:
-        start, end = end, start
-    start = max(1, start)
-    if start > len(seq):
-        start = end = len(seq)
-    elif end > len(seq):
-        end = len(seq)
-    return seq[start - 1:end]
-
-
 def align_sliding_window_batch(pairs, sliding_window_size: int, matching_score: int, mismatching_penalty: int,
                                open1: int, extend1: int, open2: int, extend2: int) -> List[Tuple[int, str, str]]:
-    """alignSlidingWindow (alignSlidingWindow.cpp:457-590) for many intervals: an interval whose
-    (len_d / W) * (len_q / W) <= 1 gets one global alignment; the others advance window by
-    window (W + 1 bases of each sequence, semiglobal KSW2 ending at the better of the last row
-    and the last column), and the i-th window of every interval still advancing runs in one
-    batched call.  Returns (score of the whole alignment under the two-piece objective,
-    aligned query, aligned reference) per interval, as a call of its own would."""
-    W = int(sliding_window_size)
-    if W > 1073741824:
+    """alignSlidingWindow (alignSlidingWindow.cpp:457-590) for many intervals, through
+    aw_align_sliding_window_batch: an interval whose (len_d / W) * (len_q / W) <= 1 gets one
+    global alignment; the others advance window by window (W + 1 bases of each sequence,
+    semiglobal KSW2 ending at the better of the last row and the last column), and the k-th
+    window of every interval still advancing runs in one batched call.  Returns (score of the
+    whole alignment under the two-piece objective, aligned query, aligned reference) per
+    interval, as a call of its own would."""
+    if int(sliding_window_size) > 1073741824:
         raise ValueError("the windows size is too large")
     n = len(pairs)
-    aq = [[] for _ in range(n)]
-    ad = [[] for _ in range(n)]
-    qstart, dstart = [1] * n, [1] * n
-    whole = [i for i, (q, d) in enumerate(pairs) if (len(d) / W) * (len(q) / W) <= 1]
-    if extend2 + matching_score < 0:
-        wpen = (mismatching_penalty + matching_score, open1 + matching_score, extend1 + matching_score,
-                open2 + matching_score, extend2 + matching_score)
-    else:
-        wpen = (mismatching_penalty + matching_score - 1, open1 + matching_score - 1, extend1 + matching_score - 1,
-                open2 + matching_score - 1, -1)
-
-    def batched(items, mis, o1, e1, o2, e2, flag_extra):
-        """(index, query, target) -> result, one call per scoring flag."""
-        mat = anchorwave_matrix(mis)
-        groups, res = {}, {}
-        for i, q, d in items:
-            qs, f1 = encode(q)
-            ts, f2 = encode(d)
-            groups.setdefault(f1 | f2, []).append((i, qs, ts))
-        for f, g in groups.items():
-            rr = ksw_extd2_batch([x[1] for x in g], [x[2] for x in g], mat, -o1, -e1, -o2, -e2, flag=f | flag_extra)
-            for (i, _, _), r in zip(g, rr):
-                res[i] = r
-        return res
-
-    # whole intervals: minimap2AlignmentWithArena (global, CIGAR)
-    if whole:
-        rr = batched([(i, pairs[i][0], pairs[i][1]) for i in whole], mismatching_penalty, open1, extend1, open2,
-                     extend2, 0)
-        for i in whole:
-            q, d = pairs[i]
-            a, b, qp, tp = decode_cigar(rr[i].cigar, q, d)
-            assert qp == len(q) and tp == len(d)
-            aq[i].append(a), ad[i].append(b)
-            qstart[i], dstart[i] = len(q) + 1, len(d) + 1
-    wset = set(whole)
-    while True:
-        items = []
-        for i, (q, d) in enumerate(pairs):
-            if i in wset or not (dstart[i] <= len(d) and qstart[i] <= len(q)):
-                continue
-            items.append((i, _subsequence(q, qstart[i], qstart[i] + W), _subsequence(d, dstart[i], dstart[i] + W)))
-        if not items:
-            break
-        rr = batched(items, *wpen, KSW_EZ_SEMIGLOBAL_END)
-        for i, qw, dw in items:
-            r = rr[i]
-            if r.mqe > r.mte:
-                end_t, end_q = r.mqe_t + 1, len(qw)
-            else:
-                end_t, end_q = len(dw), r.mte_q + 1
-            a, b, qp, tp = decode_cigar(r.cigar, qw, dw)
-            if qp != end_q or tp != end_t:
-                raise RuntimeError("KSW2 semiglobal traceback did not reconstruct its reported endpoint")
-            aq[i].append(a), ad[i].append(b)
-            qstart[i] += end_q
-            dstart[i] += end_t
-    out = []
-    for i, (q, d) in enumerate(pairs):
-        tail = 0
-        c1 = len(d) - dstart[i]
-        if c1 >= 0:
-            aq[i].append("-" * (c1 + 1)), ad[i].append(d[dstart[i] - 1:dstart[i] + c1])
-            tail += c1 + 1
-        c2 = len(q) - qstart[i]
-        if c2 >= 0:
-            aq[i].append(q[qstart[i] - 1:qstart[i] + c2]), ad[i].append("-" * (c2 + 1))
-            tail += c2 + 1
-        a, b = "".join(aq[i]), "".join(ad[i])
-        out.append((score_gapped_two_piece_affine(a, b, mismatching_penalty, open1, extend1, open2, extend2), a, b))
-    return out
+    if n == 0:
+        return []
+    qp, ql, qb = _seq_arrays([p[0] for p in pairs])
+    rp, rl, rb = _seq_arrays([p[1] for p in pairs])
+    out = (WindowResultC * n)()
+    rc = lib.aw_align_sliding_window_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, int(sliding_window_size),
+                                           matching_score, mismatching_penalty, open1, extend1, open2, extend2, out)
+    res = []
+    for o in out:
+        res.append((o.score, _text(o.alignment_q, o.alignment_len), _text(o.alignment_d, o.alignment_len)))
+        lib.aw_window_result_free(C.byref(o))
+    if rc != 0:
+        raise RuntimeError(f"aw_align_sliding_window_batch failed ({rc}): {last_error()}")
+    return res
 
 
 def align_sliding_window(dna_q: str, dna_d: str, sliding_window_size: int, matching_score: int,

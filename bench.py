@@ -26,8 +26,9 @@ and the CIGARs.
     the traceback store stream is reported against HBM bandwidth.
   * serving: a 20,000-request trace through the continuous-batching server (saturated and at
     80% offered load with p50/p99 latency).
-  * long_banded: 16 pairs of 100-150 kb, w = 10%, banded and Singletrack, beside the
-    reference's CPU code on the same pairs.
+  * long_banded: 64 pairs of 100 kb-1 Mb, w = 10%, banded and Singletrack (one execution
+    each), every CIGAR checked and re-scored, beside the reference's CPU code on the pairs
+    whose host traceback fits a safe share of the host memory.
   * wfa: 16,384 pairs of 100 bp-10 kb (0.5-5%), high memory (standard and Singletrack) and
     medium memory (piggyback), device memory per pair, beside WFA2-lib in the same mode.
   * selector_summary: the selector's sequence pass (k-mer sketches, composition, entropy,
@@ -80,9 +81,10 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=20000,
                     help="requests of the serving trace (0 skips the serving measurement)")
     ap.add_argument("--no-long-banded", action="store_true", help="skip the long banded/Singletrack sample")
-    ap.add_argument("--long-banded-pairs", type=int, default=16)
+    ap.add_argument("--long-banded-pairs", type=int, default=64)
     ap.add_argument("--long-banded-min", type=int, default=100_000)
-    ap.add_argument("--long-banded-max", type=int, default=150_000)
+    ap.add_argument("--long-banded-max", type=int, default=1_000_000)
+    ap.add_argument("--long-banded-indel", type=int, default=50_000, help="longest of the long indels")
     ap.add_argument("--wfa-pairs", type=int, default=16384, help="pairs of the batched WFA workload (0 skips it)")
     ap.add_argument("--no-selector-summary", action="store_true",
                     help="skip the selector sequence-pass measurement")
@@ -439,31 +441,75 @@ def selector_summary_measurement(ps, rank: int, cpu: bool):
     return res
 
 
-def long_banded_measurement(rank: int, cpu: bool, npairs: int = 16, lmin: int = 100_000, lmax: int = 150_000):
-    """The long-interval banded and Singletrack workload at reduced lengths (16 pairs,
-    100-150 kb, w = 10% of the shorter length, repeat-rich queries with long indels): band
-    GCUPS on the GPU for both tracebacks, and the reference's own CPU code on the same
-    pairs (one thread per pair) with a per-pair result-hash comparison."""
+def cigar_check(res, q, t, mis=4, o1=4, e1=2, o2=24, e2=1):
+    """(valid, rescored): the CIGAR consumes the whole query and target, and its two-piece
+    affine score (match 0, mismatch -mis, gap min(o1 + l*e1, o2 + l*e2))."""
+    import numpy as np
+    qp = tp = 0
+    sc = 0
+    for c in res.cigar:
+        ln, op = c >> 4, c & 0xF
+        if op == 0:
+            sc -= mis * int(np.count_nonzero(q[qp:qp + ln] != t[tp:tp + ln]))
+            qp += ln
+            tp += ln
+        elif op in (1, 2):
+            sc -= min(o1 + ln * e1, o2 + ln * e2)
+            qp += ln if op == 1 else 0
+            tp += ln if op == 2 else 0
+        else:
+            return False, None
+    return qp == len(q) and tp == len(t), sc
+
+
+def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 100_000, lmax: int = 1_000_000,
+                            long_max: int = 50_000):
+    """The long-interval banded and Singletrack workload (target length U(lmin, lmax), 30% of
+    the query replaced by repeat structure, 3% substitutions, 5-20 long indels of U(1,
+    long_max), w = 10% of the shorter length): one execution of the whole set per traceback,
+    band GCUPS on the device (pairs whose traceback exceeds the HBM budget recompute it group
+    by group; Singletrack pairs beyond the budget are refused like an allocation failure of the
+    reference, zdropped = 1, and counted), every CIGAR checked to span both sequences and
+    re-scored against ez.score; the reference's own CPU code on the pairs whose host traceback
+    fits a safe share of the host memory (one thread per pair), results compared."""
     import numpy as np
 
     from anchorwave_b200 import ksw2
     from anchorwave_b200 import workloads as W
-    ps = W.long_banded_set(npairs, seed=3 + rank, lmin=lmin, lmax=lmax, long_max=max(1, lmin // 10))
+    ps = W.long_banded_set(npairs, seed=3 + rank, lmin=lmin, lmax=lmax, long_max=long_max)
     mat = ksw2.anchorwave_matrix(-4)
-    bcells = sum(W.band_cells(len(q), len(t), w) for q, t, w in zip(ps.queries, ps.targets, ps.band))
+    pair_cells = [W.band_cells(len(q), len(t), w) for q, t, w in zip(ps.queries, ps.targets, ps.band)]
+    bcells = sum(pair_cells)
     out = {"workload": ps.name, "pairs": len(ps), "band_cells": bcells,
            "shape": f"target U({lmin // 1000} kb, {lmax // 1000} kb), 30% repeats, 3% substitutions, "
-                    f"long indels up to {max(1, lmin // 10) // 1000} kb, w = 10%"}
+                    f"5-20 long indels of U(1, {long_max // 1000} kb), w = 10% of the shorter length"}
+    # kernels loaded before the timed executions
+    warm = ksw2.KswPlan(ps.queries[:1], ps.targets[:1], mat, 4, 2, 24, 1, w=[64], flag=0x1000)
+    warm.upload()
+    warm.execute()
+    warm.close()
     results = {}
     for name, flag in (("banded", 0), ("singletrack", 0x1000)):
         plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1, w=ps.band, flag=flag)
         plan.upload()
-        plan.execute()
-        ms = min(plan.execute() for _ in range(2))
+        ms = plan.execute()
         dp, bt = plan.timing()
-        results[name] = plan.download()
+        st = plan.stats()
+        res = plan.download()
         plan.close()
-        out[name] = {"ms": ms, "dp_ms": dp, "traceback_ms": bt, "gcups": bcells / (ms * 1e-3) / 1e9}
+        results[name] = res
+        refused = [i for i, r in enumerate(res) if r.zdropped and r.n_cigar == 0]
+        ran = [i for i in range(len(ps)) if i not in set(refused)]
+        rcells = sum(pair_cells[i] for i in ran)
+        valid = rescored = 0
+        for i in ran:
+            ok, sc = cigar_check(res[i], ps.queries[i], ps.targets[i])
+            valid += ok
+            rescored += ok and sc == res[i].score
+        out[name] = {"ms": ms, "dp_ms": dp, "traceback_ms": bt, "gcups": rcells / (ms * 1e-3) / 1e9,
+                     "pairs_run": len(ran), "refused_over_budget": len(refused), "waves": st["waves"],
+                     "cigars_spanning_both": valid, "cigars_rescoring_to_score": rescored}
+        ksw2.release_thread_buffers()
     if cpu:
         from concurrent.futures import ThreadPoolExecutor
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -473,19 +519,44 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 16, lmin: int = 
         except FileNotFoundError as e:
             out["cpu_reference"] = {"unavailable": str(e)}
             return out
-        for name, variant in (("banded", 0), ("singletrack", 2)):
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+        except Exception:
+            avail = 16 << 30
+        nthreads = os.cpu_count() or 1
+        for name, variant, tracks in (("banded", 0, 1), ("singletrack", 2, 2)):
+            # the reference's traceback matrix: (qlen + tlen - 1) x (ceil((w+1)/block) + 1) blocks per track
+            def host_bytes(i):
+                ql, tl, w = len(ps.queries[i]), len(ps.targets[i]), ps.band[i]
+                return tracks * (ql + tl) * ((w + 1 + ref.block - 1) // ref.block + 1) * ref.block
+            pick, tot = [], 0
+            for i in sorted(range(len(ps)), key=host_bytes):
+                if len(pick) >= nthreads or tot + host_bytes(i) > min(48 << 30, avail // 4):
+                    break
+                if results[name][i].zdropped and results[name][i].n_cigar == 0:
+                    continue
+                pick.append(i)
+                tot += host_bytes(i)
+            if not pick:
+                out[name]["cpu_reference"] = {"unavailable": "no pair's traceback fits the host memory share"}
+                continue
+
             def one(i):
                 r = ref.ksw_batch([ps.queries[i].tobytes()], [ps.targets[i].tobytes()], mat, 4, 2, 24, 1,
                                   w=ps.band[i], variant=variant, nthreads=1)
                 return int(r["hash"][0])
             t0 = time.perf_counter()
-            with ThreadPoolExecutor(len(ps)) as ex:
-                hashes = list(ex.map(one, range(len(ps))))
+            with ThreadPoolExecutor(len(pick)) as ex:
+                hashes = list(ex.map(one, pick))
             secs = time.perf_counter() - t0
-            same = all(oracle.result_hash(g) == h for g, h in zip(results[name], hashes))
-            out[name]["cpu_reference"] = {"seconds": secs, "gcups": bcells / secs / 1e9, "threads": len(ps),
-                                          "isa": ref.isa, "results_identical": same}
-            out[name]["vs_cpu_reference"] = out[name]["gcups"] / (bcells / secs / 1e9)
+            same = all(oracle.result_hash(results[name][i]) == h for i, h in zip(pick, hashes))
+            pc = sum(pair_cells[i] for i in pick)
+            out[name]["cpu_reference"] = {"pairs": len(pick), "band_cells": pc, "seconds": secs,
+                                          "gcups": pc / secs / 1e9, "threads": len(pick), "isa": ref.isa,
+                                          "results_identical": same,
+                                          "sample": "the pairs with the smallest host traceback, one thread each"}
+            out[name]["vs_cpu_reference"] = out[name]["gcups"] / (pc / secs / 1e9)
     return out
 
 
@@ -646,7 +717,7 @@ def main():
     ksw2.release_thread_buffers()
     serving = serving_measurement(args.serve_requests, rank) if args.serve_requests > 0 else None
     long_banded = None if args.no_long_banded else long_banded_measurement(
-        rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max)
+        rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max, args.long_banded_indel)
     wfa_res = (wfa_measurement(args.wfa_pairs, rank, cpu_on, args.wfa_pool_gb) if args.wfa_pairs > 0 else None)
     summary_res = (None if args.no_selector_summary else selector_summary_measurement(ps, rank, cpu_on))
 
@@ -741,11 +812,17 @@ def compact_summary(line):
         par["batched_full"] = {k: par["batched_full"][k] for k in ("pairs_checked", "identical")}
     lb = line.get("long_banded")
     if lb:
-        out["long_banded"] = {"pairs": lb["pairs"]}
+        out["long_banded"] = {"pairs": lb["pairs"], "band_cells": lb["band_cells"]}
         for nm in ("banded", "singletrack"):
             if nm in lb:
-                out["long_banded"][nm] = {"gcups": lb[nm].get("gcups"), "vs_ref": lb[nm].get("vs_cpu_reference")}
-                par[f"long_{nm}"] = get(lb, nm, "cpu_reference", "results_identical")
+                x = lb[nm]
+                out["long_banded"][nm] = {"gcups": x.get("gcups"), "s": x["ms"] / 1e3, "run": x["pairs_run"],
+                                          "refused": x["refused_over_budget"],
+                                          "valid": x["cigars_spanning_both"],
+                                          "rescored": x["cigars_rescoring_to_score"],
+                                          "vs_ref": x.get("vs_cpu_reference")}
+                par[f"long_{nm}"] = {"pairs_checked": get(x, "cpu_reference", "pairs"),
+                                     "identical": get(x, "cpu_reference", "results_identical")}
     wf = line.get("wfa")
     if wf:
         out["wfa"] = {}

@@ -129,6 +129,66 @@ int aw_cigar_rows_batch(int n, const uint32_t *const *cigar, const int *n_cigar,
                         const int *qlen, const char *const *target, const int *tlen, char *row_q, char *row_d,
                         int64_t *row_off, int *row_len, int64_t capacity);
 
+/* ---- rescue procedures (batched) ---------------------------------------------- */
+
+/* Result of alignScoreCertifiedKsw2 (src/myImportandFunction/alignSlidingWindow.h:31-49:
+ * Ksw2CertifiedStatus and Ksw2CertifiedResult) for one interval.  status: 0 Completed,
+ * 1 TimeLimit, 2 NotCertified, 3 Failed.  alignment_q/_d: the certified rows (malloc'd,
+ * NUL-terminated, alignment_len characters), only when Completed; best_effort_q/_d: the
+ * best valid banded rows of a failed certification.  Free with aw_certified_result_free. */
+typedef struct {
+    int status;
+    int64_t score, optimal_score, final_band_width, traceback_attempts;
+    char *alignment_q, *alignment_d;
+    int64_t alignment_len;
+    char *best_effort_q, *best_effort_d;
+    int64_t best_effort_len;
+} aw_certified_result_t;
+
+/*
+ * alignScoreCertifiedKsw2 (src/myImportandFunction/alignSlidingWindow.cpp:1197-1400) for n
+ * intervals at once, called from the executor at :1835: the unbanded score-only optimum of
+ * every interval in one batch, then round by round the next band of every interval not yet
+ * certified in one banded batch, until its re-scored alignment reaches the optimum; the
+ * skipped smallest band runs only on failure.  Every interval gets the result a call of its
+ * own would give (the selector's chained traceback, used when a selection plan is passed,
+ * stays with the caller).  Sequences are ASCII; penalties AnchorWave's (negative);
+ * maximum_runtime_seconds > 0 arms the calling thread's deadline (aw_ksw_set_deadline) for
+ * the call; precomputed_optimal_scores (n values, or NULL) skips the score-only batch.
+ * Returns AW_OK or a negative AW_E* code; out[i] is filled either way.
+ */
+int aw_align_score_certified_batch(int n, const char *const *query, const int64_t *qlen,
+                                   const char *const *reference, const int64_t *rlen,
+                                   int64_t initial_band_width, int64_t maximum_band_width,
+                                   int32_t mismatching_penalty, int32_t open1, int32_t extend1, int32_t open2,
+                                   int32_t extend2, double maximum_runtime_seconds,
+                                   const int64_t *precomputed_optimal_scores, aw_certified_result_t *out);
+void aw_certified_result_free(aw_certified_result_t *result);
+
+/* Result of the sliding-window alignment: the whole alignment's two-piece affine score and
+ * its rows (malloc'd, NUL-terminated).  Free with aw_window_result_free. */
+typedef struct {
+    int64_t score;
+    char *alignment_q, *alignment_d;
+    int64_t alignment_len;
+} aw_window_result_t;
+
+/*
+ * alignSlidingWindow (src/myImportandFunction/alignSlidingWindow.cpp:457-590), the
+ * approximate-tier fallback called from the executor at :2683, for n intervals at once: an
+ * interval with (rlen/W)*(qlen/W) <= 1 gets one global alignment; the others advance window
+ * by window (W+1 bases of each sequence, semiglobal KSW2 ending at the better of the last row
+ * and the last column), the k-th window of every interval still advancing in one batched
+ * call; trailing gaps close the alignment, which is re-scored with the two-piece objective.
+ * Sequences ASCII, penalties negative.  Returns AW_OK or a negative AW_E* code (an endpoint
+ * the traceback does not reconstruct is AW_E_INVAL, the reference's runtime_error).
+ */
+int aw_align_sliding_window_batch(int n, const char *const *query, const int64_t *qlen,
+                                  const char *const *reference, const int64_t *rlen, int64_t sliding_window_size,
+                                  int32_t matching_score, int32_t mismatching_penalty, int32_t open1,
+                                  int32_t extend1, int32_t open2, int32_t extend2, aw_window_result_t *out);
+void aw_window_result_free(aw_window_result_t *result);
+
 /* ---- WFA (gap-affine-2p, end to end) ------------------------------------------ */
 
 /* Attributes of WfaAlignment.cpp:143-170: match 0, these penalties (positive), no

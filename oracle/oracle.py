@@ -321,6 +321,67 @@ class Reference:
                                                      ident.ctypes.data, nthreads)
         return secs, out, ident
 
+    # ---- AnchorWave's rescue procedures and row decoding (ref_rescue_shim.cpp) -------------
+    def _rescue_args(self):
+        L = self.lib
+        if getattr(self, "_rescue_ready", False):
+            return
+        vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int
+        L.awref_score_certified.argtypes = [C.c_char_p, i64, C.c_char_p, i64, i64, i64, i32, i32, i32, i32, i32,
+                                            C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), vp, vp,
+                                            i64, C.POINTER(i64), vp, vp, C.POINTER(i64)]
+        L.awref_score_certified.restype = i32
+        L.awref_sliding_window.argtypes = [C.c_char_p, i64, C.c_char_p, i64, i64, i32, i32, i32, i32, i32, i32, vp,
+                                           vp, i64, C.POINTER(i64)]
+        L.awref_sliding_window.restype = i64
+        for fn in (L.awref_minimap2_rows,):
+            fn.argtypes = [C.c_char_p, i64, C.c_char_p, i64, i32, i32, i32, i32, i32, vp, vp, i64, C.POINTER(i64)]
+            fn.restype = i64
+        L.awref_banded_rows.argtypes = [C.c_char_p, i64, C.c_char_p, i64, i64, i32, i32, i32, i32, i32, vp, vp, i64,
+                                        C.POINTER(i64)]
+        L.awref_banded_rows.restype = i64
+        self._rescue_ready = True
+
+    def score_certified(self, dq: str, dd: str, initial_band: int, maximum_band: int, pen):
+        """alignScoreCertifiedKsw2 (alignSlidingWindow.cpp:1197-1400), no selection plan, no
+        deadline: dict with status (0 Completed, 1 TimeLimit, 2 NotCertified, 3 Failed), score,
+        optimal_score, final_band_width, traceback_attempts, rows and best-effort rows."""
+        self._rescue_args()
+        q, d = dq.encode(), dd.encode()
+        cap = len(q) + len(d) + 1
+        bufs = [C.create_string_buffer(cap) for _ in range(4)]
+        v = [C.c_int64(0) for _ in range(6)]
+        st = self.lib.awref_score_certified(q, len(q), d, len(d), initial_band, maximum_band, *pen, *[C.byref(x) for x in v[:4]],
+                                            bufs[0], bufs[1], cap, C.byref(v[4]), bufs[2], bufs[3], C.byref(v[5]))
+        rows = lambda b, n: b.raw[:n].decode() if n > 0 else ""
+        return {"status": st, "score": v[0].value, "optimal_score": v[1].value, "final_band_width": v[2].value,
+                "traceback_attempts": v[3].value, "alignment_q": rows(bufs[0], v[4].value),
+                "alignment_d": rows(bufs[1], v[4].value), "best_effort_q": rows(bufs[2], v[5].value),
+                "best_effort_d": rows(bufs[3], v[5].value)}
+
+    def _rows_call(self, fn, q: bytes, d: bytes, *args):
+        cap = len(q) + len(d) + 1
+        a, b = C.create_string_buffer(cap), C.create_string_buffer(cap)
+        n = C.c_int64(0)
+        s = fn(q, len(q), d, len(d), *args, a, b, cap, C.byref(n))
+        return s, a.raw[:n.value].decode(), b.raw[:n.value].decode()
+
+    def sliding_window(self, dq: str, dd: str, window: int, match: int, pen):
+        """alignSlidingWindow (alignSlidingWindow.cpp:457-590): (score, query row, reference row)."""
+        self._rescue_args()
+        return self._rows_call(self.lib.awref_sliding_window, dq.encode(), dd.encode(), window, match, *pen)
+
+    def minimap2_rows(self, dq: str, dd: str, pen):
+        """minimap2AlignmentWithArena (alignSlidingWindow.cpp:241-332): ksw_extd2 of the native ISA
+        and its CIGAR decoded into rows (:307-324): (ez.score, query row, reference row)."""
+        self._rescue_args()
+        return self._rows_call(self.lib.awref_minimap2_rows, dq.encode(), dd.encode(), *pen)
+
+    def banded_rows(self, dq: str, dd: str, band: int, pen):
+        """alignSlidingWindow_minimap2 (alignSlidingWindow.cpp:800-890): (re-score, rows)."""
+        self._rescue_args()
+        return self._rows_call(self.lib.awref_banded_rows, dq.encode(), dd.encode(), band, *pen)
+
     def wfa_align(self, pattern: bytes, text: bytes, x, o1, e1, o2, e2, singletrack=False, memory_mode=0):
         score = C.c_int(0)
         nops = C.c_int(0)

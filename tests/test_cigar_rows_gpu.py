@@ -1,7 +1,8 @@
-"""Gapped rows decoded on the device (aw_cigar_rows_batch) against the host decoding of the
-same CIGARs (alignSlidingWindow.cpp:307-324), for KSW2 results with mismatches, long indels,
-N bases and lowercase letters (the rows keep the caller's characters), and the rejected
-inputs."""
+"""Gapped rows decoded on the device (aw_cigar_rows_batch) from the GPU's KSW2 CIGARs against
+the compiled reference's minimap2AlignmentWithArena (alignSlidingWindow.cpp:241-332: its own
+ksw_extd2 call and the CIGAR decoding of :307-324) on the same intervals, for results with
+mismatches, long indels, N bases and lowercase letters (the rows keep the caller's
+characters), and the rejected inputs."""
 import numpy as np
 import pytest
 
@@ -12,7 +13,7 @@ from anchorwave_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def test_rows_match_host_decoding(gpu):
+def test_rows_match_compiled_reference(gpu, reference):
     rng = np.random.default_rng(12)
     qs, ts = [], []
     for i in range(64):
@@ -33,7 +34,8 @@ def test_rows_match_host_decoding(gpu):
         res.append(ksw2.ksw_extd2(qc, tc, ksw2.anchorwave_matrix(-4), 4, 2, 24, 1, flag=f1 | f2))
     rows = ksw2.cigar_rows_batch([r.cigar for r in res], qs, ts)
     for q, t, r, (rq, rd) in zip(qs, ts, res, rows):
-        eq, ed, _, _ = ksw2.decode_cigar(r.cigar, q, t)
+        score, eq, ed = reference.minimap2_rows(q, t, (-4, -4, -2, -24, -1))
+        assert score == r.score
         assert (rq, rd) == (eq, ed)
         assert rq.replace("-", "") == q and rd.replace("-", "") == t
 

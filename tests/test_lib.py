@@ -1,4 +1,4 @@
-"""CPU: the C-ABI library loads and exports every function include/anchorwave_b200.h declares;
+"""CPU: the C-ABI library loads and exports every function and object the include/*.h headers declare;
 host-side helpers (workload generators, CIGAR decoding, two-piece rescoring) behave like the
 reference's; without a GPU the entry points fail loudly instead of falling back to the CPU."""
 import ctypes
@@ -10,14 +10,24 @@ import numpy as np
 import oracle
 from anchorwave_b200 import _lib, ksw2, workloads as W
 
-HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "anchorwave_b200.h")
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include")
+HEADERS = sorted(os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h"))
 
 
 def header_functions():
-    text = open(HEADER).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\(", text, flags=re.M)
-    return sorted(set(n for n in names if n not in ("defined",)))
+    names = set()
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        text = "\n".join(ln for ln in text.splitlines() if not ln.lstrip().startswith("typedef"))
+        names |= set(re.findall(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\(", text, flags=re.M))
+    return sorted(n for n in names if n not in ("defined",))
+
+
+def header_data_symbols():
+    names = set()
+    for h in HEADERS:
+        names |= set(re.findall(r"^extern const \w+ (\w+);", open(h).read(), flags=re.M))
+    return sorted(names)
 
 
 def test_header_declares_expected_entry_points():
@@ -28,9 +38,11 @@ def test_header_declares_expected_entry_points():
 
 def test_library_exports_every_header_symbol():
     lib = ctypes.CDLL(_lib.LIB_PATH)
-    missing = [n for n in header_functions() if not hasattr(lib, n)]
+    missing = [n for n in header_functions() + header_data_symbols() if not hasattr(lib, n)]
     assert not missing, missing
-    assert set(_lib.EXPORTS) <= set(header_functions())
+    assert "wavefront_aligner_new_wfa2_gpu" in header_functions()
+    assert header_data_symbols() == ["wavefront_aligner_attr_default_gpu"]
+    assert set(_lib.EXPORTS) <= set(header_functions()) | set(header_data_symbols())
 
 
 def test_no_cpu_fallback_without_gpu():
