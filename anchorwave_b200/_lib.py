@@ -34,7 +34,7 @@ EXPORTS = [
     "aw_sequence_summary_sketches", "aw_sequence_summary_sketch_view", "aw_serve_open", "aw_serve_submit", "aw_serve_poll", "aw_serve_stats",
     "aw_serve_result_free", "aw_serve_close", "wavefront_aligner_new_wfa2_gpu", "wavefront_align_wfa2_gpu",
     "wavefront_aligner_delete_wfa2_gpu", "wavefront_aligner_attr_default_gpu", "aw_align_score_certified_batch",
-    "aw_certified_result_free", "aw_align_sliding_window_batch", "aw_window_result_free",
+    "aw_certified_result_free", "aw_align_sliding_window_batch", "aw_window_result_free", "aw_serve_submit_route",
 ]
 
 
@@ -58,6 +58,11 @@ class ServeConfig(C.Structure):
                 ("mat", C.c_int8 * 64), ("q", C.c_int8), ("e", C.c_int8), ("q2", C.c_int8), ("e2", C.c_int8),
                 ("wfa_x", C.c_int), ("wfa_o1", C.c_int), ("wfa_e1", C.c_int), ("wfa_o2", C.c_int),
                 ("wfa_e2", C.c_int)]
+
+
+class ServeRoute(C.Structure):
+    """aw_serve_route_t."""
+    _fields_ = [("method", C.c_int), ("band", C.c_int), ("band_max", C.c_int), ("window", C.c_int64)]
 
 
 class ServeResult(C.Structure):
@@ -128,12 +133,12 @@ def _load(path: str = LIB_PATH):
     lib.aw_ksw_plan_graph.restype = i32
     lib.aw_cigar_rows_batch.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64]
     lib.aw_cigar_rows_batch.restype = i32
-    lib.aw_align_score_certified_batch.argtypes = [i32, vp, vp, vp, vp, i64, i64, i32, i32, i32, i32, i32,
+    lib.aw_align_score_certified_batch.argtypes = [i32, vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32,
                                                    C.c_double, vp, C.POINTER(CertResultC)]
     lib.aw_align_score_certified_batch.restype = i32
     lib.aw_certified_result_free.argtypes = [C.POINTER(CertResultC)]
     lib.aw_certified_result_free.restype = None
-    lib.aw_align_sliding_window_batch.argtypes = [i32, vp, vp, vp, vp, i64, i32, i32, i32, i32, i32, i32,
+    lib.aw_align_sliding_window_batch.argtypes = [i32, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32,
                                                   C.POINTER(WindowResultC)]
     lib.aw_align_sliding_window_batch.restype = i32
     lib.aw_window_result_free.argtypes = [C.POINTER(WindowResultC)]
@@ -166,6 +171,8 @@ def _load(path: str = LIB_PATH):
     lib.aw_serve_open.restype = vp
     lib.aw_serve_submit.argtypes = [vp, C.c_uint64, i32, i32, C.c_char_p, i32, C.c_char_p, i32]
     lib.aw_serve_submit.restype = i32
+    lib.aw_serve_submit_route.argtypes = [vp, C.c_uint64, C.POINTER(ServeRoute), C.c_char_p, i32, C.c_char_p, i32]
+    lib.aw_serve_submit_route.restype = i32
     lib.aw_serve_poll.argtypes = [vp, C.POINTER(ServeResult), i32, i32]
     lib.aw_serve_poll.restype = i32
     lib.aw_serve_stats.argtypes = [vp, C.POINTER(ServeStats)]

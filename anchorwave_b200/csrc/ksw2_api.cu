@@ -95,7 +95,7 @@ struct PinBuf {
 struct Buffers {
     DevBuf qcodes, tcodes, pairs, order, out, cig, packed, packed_off, tb, bnd, queue, error;
     DevBuf exact_ws, deadline;
-    DevBuf band_pairs, band_strips, band_units, band_res, band_progress, band_bnd, band_queue, band_walk;
+    DevBuf band_pairs, band_strips, band_units, band_res, band_progress, band_bnd, band_queue, band_walk, band_groups;
     PinBuf h_band;
     PinBuf h_codes, h_pairs, h_order, h_out, h_packed, h_packed_off, h_small;
     cudaStream_t st = nullptr, st2 = nullptr;
@@ -109,6 +109,7 @@ struct Buffers {
         queue.release(); error.release(); exact_ws.release(); deadline.release();
         band_pairs.release(); band_strips.release(); band_units.release(); band_res.release();
         band_progress.release(); band_bnd.release(); band_queue.release(); band_walk.release(); h_band.release();
+        band_groups.release();
         h_codes.release(); h_pairs.release(); h_order.release(); h_out.release();
         h_packed.release(); h_packed_off.release(); h_small.release();
         for (auto e : ev_k) cudaEventDestroy(e);
@@ -320,7 +321,7 @@ struct aw_ksw_plan {
     std::vector<int32_t> exact_ids;  // pairs for the exact kernel
     std::vector<int32_t> band_ids;   // pairs for the banded kernel
     BandPlan band;
-    int refused = 0;                 // Singletrack pairs refused for the budget (reported zdropped)
+    int refused = 0;                 // banded pairs refused for the budget (reported zdropped)
     int64_t tb_cap = 0, bnd_cap = 0;
     int64_t cells = 0, tb_total = 0;
     int launches = 0;
@@ -477,15 +478,16 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
             return AW_E_NOMEM;
         }
         if (!refused.empty()) {
-            // Singletrack pairs beyond the budget: the reference's allocation-failure result
-            // (ksw2_extd2_avx.c:206-210), the other pairs of the batch run as planned
+            // pairs that cannot run within the budget: the reference's allocation-failure
+            // result (ksw2_extd2_avx.c:206-210), the other pairs of the batch run as planned
             for (int32_t i : refused) pl->route[i] = 0, pl->early_zdrop[i] = 1;
             pl->band_ids.erase(std::remove_if(pl->band_ids.begin(), pl->band_ids.end(),
                                               [&](int32_t i) { return pl->route[i] != 3; }),
                                pl->band_ids.end());
             pl->refused = (int)refused.size();
-            set_error("Singletrack traceback of a pair exceeds the HBM traceback budget: pair reported "
-                      "as zdropped (allocation failure)");
+            set_error("a pair's traceback does not fit the HBM traceback budget (a Singletrack traceback, which "
+                      "cannot be recomputed in strip groups, or a single strip beyond it): pair reported as "
+                      "zdropped (allocation failure)");
         }
         pl->tb_cap = std::max(pl->tb_cap, pl->band.tb_cap);
         pl->tb_total += pl->band.tb_total;
@@ -521,6 +523,7 @@ static int plan_alloc(aw_ksw_plan_t *pl) {
         AW_CUDA(B->band_progress.ensure(sizeof(int32_t) * PROG_STRIDE * bp.strips.size()));
         AW_CUDA(B->band_bnd.ensure(sizeof(uint2) * (size_t)bp.bnd_cap + 256));
         AW_CUDA(B->band_queue.ensure(sizeof(int32_t) * 64 * bp.waves.size()));
+        AW_CUDA(B->band_groups.ensure(sizeof(BandGroupDev) * std::max<size_t>(bp.groups.size(), 1)));
     }
     AW_CUDA(B->h_pairs.ensure(sizeof(KswPair) * (size_t)std::max(n, 1)));
     AW_CUDA(B->h_order.ensure(sizeof(int32_t) * (pl->order.size() + pl->exact_ids.size() + 1)));
@@ -573,15 +576,17 @@ static int plan_upload(aw_ksw_plan_t *pl, const uint8_t *const *query, const uin
     if (!pl->band_ids.empty()) {
         const BandPlan &bp = pl->band;
         const size_t np = sizeof(BandPairDev) * bp.pairs.size(), ns = sizeof(BandStripDev) * bp.strips.size(),
-                     nu = sizeof(int2) * bp.units.size();
-        AW_CUDA(B->h_band.ensure(np + ns + nu));
+                     nu = sizeof(int2) * bp.units.size(), ng = sizeof(BandGroupDev) * bp.groups.size();
+        AW_CUDA(B->h_band.ensure(np + ns + nu + ng));
         uint8_t *h = B->h_band.as<uint8_t>();
         memcpy(h, bp.pairs.data(), np);
         memcpy(h + np, bp.strips.data(), ns);
         memcpy(h + np + ns, bp.units.data(), nu);
+        if (ng) memcpy(h + np + ns + nu, bp.groups.data(), ng);
         AW_CUDA(cudaMemcpyAsync(B->band_pairs.p, h, np, cudaMemcpyHostToDevice, B->st));
         AW_CUDA(cudaMemcpyAsync(B->band_strips.p, h + np, ns, cudaMemcpyHostToDevice, B->st));
         AW_CUDA(cudaMemcpyAsync(B->band_units.p, h + np + ns, nu, cudaMemcpyHostToDevice, B->st));
+        if (ng) AW_CUDA(cudaMemcpyAsync(B->band_groups.p, h + np + ns + nu, ng, cudaMemcpyHostToDevice, B->st));
     }
     pl->uploaded = true;
     return AW_OK;
@@ -681,6 +686,7 @@ static int plan_launch(aw_ksw_plan_t *pl) {
         D.walk = B->band_walk.as<BandWalkState>();
         D.progress = B->band_progress.as<int32_t>(), D.queue = B->band_queue.as<int32_t>();
         D.bnd = B->band_bnd.as<uint2>(), D.tb = B->tb.as<uint8_t>(), D.error = B->error.as<int32_t>();
+        D.groups = B->band_groups.as<BandGroupDev>();
         D.deadline = deadline;
         const int ctas = band_occupancy(P.flag) * B->sms;
         for (int k = 0; k < nbw; ++k) {
@@ -693,13 +699,11 @@ static int plan_launch(aw_ksw_plan_t *pl) {
                                        P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), P.mat, P.m, B->st));
             launches += 2;
             const BandWave &BW = pl->band.waves[k];
-            if (BW.ngroup > 0) {
+            if (BW.nround > 0) {
                 AW_CUDA(band_launch_groups(pl->band, k, D, B->qcodes.as<uint8_t>(), B->tcodes.as<uint8_t>(), pl->S,
                                            P.flag, B->out.as<KswOut>(), B->cig.as<uint32_t>(), P.mat, P.m, ctas,
                                            B->st));
-                int lasts = 0;
-                for (int gi = BW.group0; gi < BW.group0 + BW.ngroup; ++gi) lasts += pl->band.groups[gi].last;
-                launches += 3 * BW.ngroup + lasts;  // counters, strips, walk per group; tail per pair
+                launches += 3 * BW.nround;  // counters, strips, walks per round
             }
             AW_CUDA(record_timing(ev[2], B->st));
         }

@@ -678,12 +678,16 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
     if (lane == 0) A.out[P.idx] = o;
 }
 
-// One group of a recomputed pair: continue the ksw_backtrack walk through the group's
-// freshly stored traceback until it leaves the group on the left (or ends).
+// One group of a recomputed pair per block (a round's groups): continue the ksw_backtrack
+// walk through the group's freshly stored traceback until it leaves the group on the left
+// (or ends); in the pair's first group, close the walk (the leading gap, the reversal, the
+// CIGAR length).
 template <int NC>
-__global__ void __launch_bounds__(32) ksw_band_walk_kernel(BtArgs A, int slot, int col_lo) {
+__global__ void __launch_bounds__(32) ksw_band_round_walk_kernel(BtArgs A, const BandGroupDev *groups) {
     using Cache = TileCache<NC, 32, 64 / NC>;
     __shared__ typename Cache::Word tiles[2 * Cache::NW];
+    const BandGroupDev G = groups[blockIdx.x];
+    const int slot = G.slot, col_lo = G.col_lo;
     BandWalkState w = A.walk[slot];
     if (w.done) return;
     const BandPairDev P = A.pairs[slot];
@@ -713,30 +717,29 @@ __global__ void __launch_bounds__(32) ksw_band_walk_kernel(BtArgs A, int slot, i
     WarpCig cg{A.cig + P.cig_off, w.n, (uint32_t)w.op, w.len};
     int i = w.i, j = w.j, state = w.state;
     band_walk<NC>(i, j, state, col_lo, cg, cache, load, g);
+    if (G.last) {
+        if (i >= 0) cg.push(2, i + 1);
+        if (j >= 0) cg.push(1, j + 1);
+        const int n = cg.finish(!(A.flag & AW_EZ_REV_CIGAR));
+        if ((threadIdx.x & 31) == 0) {
+            A.out[P.idx].n_cigar = n;
+            A.walk[slot].done = 1;
+        }
+        return;
+    }
     if ((threadIdx.x & 31) == 0) {
         w.i = i, w.j = j, w.state = state, w.n = cg.n, w.op = (int)cg.op, w.len = cg.len;
         A.walk[slot] = w;
     }
 }
 
-// The end of a recomputed pair's walk: the leading gap, the reversal, the CIGAR length.
-__global__ void __launch_bounds__(32) ksw_band_walk_finish_kernel(BtArgs A, int slot) {
-    BandWalkState w = A.walk[slot];
-    if (w.done) return;
-    const BandPairDev P = A.pairs[slot];
-    WarpCig cg{A.cig + P.cig_off, w.n, (uint32_t)w.op, w.len};
-    if (w.i >= 0) cg.push(2, w.i + 1);
-    if (w.j >= 0) cg.push(1, w.j + 1);
-    const int n = cg.finish(!(A.flag & AW_EZ_REV_CIGAR));
-    if ((threadIdx.x & 31) == 0) A.out[P.idx].n_cigar = n;
-}
-
-// Progress counters of a group pass: the group's strips start from zero, the strip on its
-// left (not recomputed: its boundary column is stored from the first pass) counts as done.
-__global__ void band_group_progress_kernel(int32_t *progress, int s_first, int s_end, int left) {
-    const int k = s_first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < s_end) progress[PROG_STRIDE * k] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && left >= 0) progress[PROG_STRIDE * left] = INT_MAX / 2;
+// Progress counters of a round (one block per group): the group's strips start from zero, the
+// strip on its left (not recomputed: its boundary column is stored from the first pass) counts
+// as done.
+__global__ void band_round_progress_kernel(int32_t *progress, const BandGroupDev *groups) {
+    const BandGroupDev G = groups[blockIdx.x];
+    for (int k = G.s_first + (int)threadIdx.x; k < G.s_end; k += blockDim.x) progress[PROG_STRIDE * k] = 0;
+    if (threadIdx.x == 0 && G.left >= 0) progress[PROG_STRIDE * G.left] = INT_MAX / 2;
 }
 
 template <bool CIGAR, bool RIGHT, bool ST>
@@ -807,13 +810,10 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
     struct PairGeo {
         int32_t id, ww, rb;
         int64_t tb, bnd;
-        bool ckpt = false, refused = false;
+        bool ckpt = false, refused = false, notb = false;
         std::vector<BandStripDev> strips;
         std::vector<int64_t> start;  // estimated start step of each strip
         std::vector<int64_t> stb;    // traceback bytes of each strip
-        std::vector<std::pair<int, int>> groups;  // recomputed pairs: strip groups [s0, s1)
-        std::vector<int64_t> gtb;
-        int64_t gtb_max = 0;
     };
     std::vector<PairGeo> geo(ids.size());
     for (size_t a = 0; a < ids.size(); ++a) {
@@ -860,48 +860,45 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
         }
         G.tb = (G.tb + 255) / 256 * 256;
         const int64_t bnd_bytes = band_bnd_bytes(G.bnd);
-        if (G.tb + bnd_bytes > tb_budget) {
+        // Singletrack pairs keep their whole two-track traceback: the reconstruction probes
+        // arbitrarily far left in one gap search, so it cannot be split into strip groups.  A
+        // pair whose traceback and boundary columns exceed the budget is refused like an
+        // allocation failure of the reference (ksw2_extd2_avx.c:206-210: reset result,
+        // zdropped = 1).
+        if (G.rb < nd) {
+            // the band becomes empty before the end: the reference stops there with
+            // zdropped = 1 and no traceback (ksw2_extd2_sse.c:151-154), so the DP runs without
+            // storing one (the first pass of a recomputed pair, with nothing to recompute)
+            G.ckpt = G.notb = true;
+            G.tb = 0;
+        }
+        bool refuse = st && G.tb + bnd_bytes > tb_budget;
+        if (!st && G.tb + bnd_bytes > tb_budget) {
             // Traceback beyond the budget: the first pass stores only the strips' boundary
-            // columns; the walk then recomputes groups of strips, from the last group to the
-            // first, each from the stored column on its left.  Groups take at most half of
-            // the budget, so that the boundary columns of the pairs of a wave fit beside
-            // them.  The Singletrack reconstruction probes arbitrarily far left in one gap
-            // search, so it is not split this way: such a pair is refused like an allocation
-            // failure of the reference (ksw2_extd2_avx.c:206-210: reset result, zdropped = 1).
-            const int64_t gbudget = tb_budget / 2;
-            bool fits = !st && bnd_bytes <= tb_budget - gbudget;
-            for (int s = 0; fits && s < (int)G.strips.size(); ++s) fits = G.stb[s] <= gbudget;
-            if (!fits) {
-                if (!refused) return AW_E_NOMEM_INTERNAL;
-                G.refused = true;
-                refused->push_back(G.id);
-                continue;
+            // columns; then the traceback is recomputed in groups of strips, from the last group
+            // to the first, each from the stored column on its left, and the walk continues
+            // through each group as it is recomputed.  The groups are cut per wave (below).
+            for (int s = 0; s < (int)G.strips.size(); ++s) refuse |= G.stb[s] > tb_budget / 2;
+            if (!refuse) {
+                G.ckpt = true;
+                G.tb = 0;  // the first pass stores no traceback
             }
-            G.ckpt = true;
-            int s0 = 0;
-            int64_t acc = 0;
-            for (int s = 0; s < (int)G.strips.size(); ++s) {
-                if (acc + G.stb[s] > gbudget) {
-                    G.groups.push_back({s0, s});
-                    G.gtb.push_back(acc);
-                    G.gtb_max = std::max(G.gtb_max, acc);
-                    s0 = s, acc = 0;
-                }
-                G.strips[s].tb_off = acc;  // relative to the group's buffer
-                acc += G.stb[s];
-            }
-            G.groups.push_back({s0, (int)G.strips.size()});
-            G.gtb.push_back(acc);
-            G.gtb_max = std::max(G.gtb_max, acc);
-            G.tb = 0;  // the first pass stores no traceback
+        }
+        if (refuse) {
+            if (!refused) return AW_E_NOMEM_INTERNAL;
+            G.refused = true;
+            refused->push_back(G.id);
+            continue;
         }
         bp.tb_total += G.tb;
         bp.cells += band_cells(ql, tl, ww);
     }
-    // pairs largest first into the fewest waves under the budget (LPT multiway fit).  A
-    // wave holds its pairs' boundary columns for the whole wave, and its traceback arena
-    // serves first the pairs stored in full, then (after their walks) one group of a
-    // recomputed pair at a time: bnd + max(tb, largest group) <= budget.
+    // Pairs largest first into the fewest waves under the budget (LPT multiway fit).  A wave
+    // holds its pairs' boundary columns throughout; its traceback arena serves first the pairs
+    // stored in full, then (after their walks) the recompute rounds of its recomputed pairs,
+    // which take half of the budget: bnd + max(tb, half the budget if any pair is recomputed)
+    // <= budget, or one pair alone.
+    const int64_t gres = tb_budget / 2;
     std::vector<size_t> ord;
     for (size_t a = 0; a < ids.size(); ++a)
         if (!geo[a].refused) ord.push_back(a);
@@ -910,35 +907,40 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
         return cx != cy ? cx > cy : geo[x].id < geo[y].id;
     });
     std::vector<std::vector<size_t>> wv;
-    std::vector<int64_t> wtb, wbnd, wgtb;
-    auto foot = [&](int64_t tb, int64_t bnd, int64_t gtb) { return bnd + std::max(tb, gtb); };
+    std::vector<int64_t> wtb, wbnd;
+    std::vector<char> wck;
+    auto foot = [&](int64_t tb, int64_t bnd, bool ck) { return bnd + std::max(tb, ck ? gres : (int64_t)0); };
     for (size_t a : ord) {
         const PairGeo &G = geo[a];
         const int64_t pb = band_bnd_bytes(G.bnd);
         int best = -1;
         for (size_t k = 0; k < wv.size(); ++k) {
-            const int64_t f = foot(wtb[k] + G.tb, wbnd[k] + pb, std::max(wgtb[k], G.gtb_max));
-            if (f <= tb_budget && (best < 0 || foot(wtb[k], wbnd[k], wgtb[k]) < foot(wtb[best], wbnd[best], wgtb[best])))
+            const int64_t f = foot(wtb[k] + G.tb, wbnd[k] + pb, wck[k] || (G.ckpt && !G.notb));
+            if (f <= tb_budget && (best < 0 || foot(wtb[k], wbnd[k], wck[k]) < foot(wtb[best], wbnd[best], wck[best])))
                 best = (int)k;
         }
         if (best < 0) {
             wv.emplace_back();
-            wtb.push_back(0), wbnd.push_back(0), wgtb.push_back(0);
+            wtb.push_back(0), wbnd.push_back(0), wck.push_back(0);
             best = (int)wv.size() - 1;
         }
-        wtb[best] += G.tb, wbnd[best] += pb, wgtb[best] = std::max(wgtb[best], G.gtb_max);
+        wtb[best] += G.tb, wbnd[best] += pb, wck[best] |= (G.ckpt && !G.notb);
         wv[best].push_back(a);
     }
+    struct U {
+        int64_t start;
+        int slot, s;
+    };
+    auto by_start = [](const U &x, const U &y) {
+        return x.start != y.start ? x.start < y.start : (x.slot != y.slot ? x.slot < y.slot : x.s < y.s);
+    };
     for (size_t k = 0; k < wv.size(); ++k) {
         BandWave W;
         W.pair0 = (int)bp.pairs.size(), W.npair = (int)wv[k].size();
         W.unit0 = (int)bp.units.size(), W.strip0 = (int)bp.strips.size();
         int64_t tb = 0, bnd = 0;
-        struct U {
-            int64_t start;
-            int slot, s;
-        };
         std::vector<U> us;
+        std::vector<std::pair<int, size_t>> ck;  // (slot, geo index) of the recomputed pairs
         for (size_t a : wv[k]) {
             const PairGeo &G = geo[a];
             const KswPair &kp = pairs[G.id];
@@ -957,39 +959,81 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
                 bp.strips.push_back(sd);
                 us.push_back(U{G.start[s], slot, (int)s});
             }
+            if (G.ckpt && !G.notb) ck.push_back({slot, a});
             tb += G.tb;
             bnd += (G.bnd + 31) / 32 * 32;
         }
         // strips in estimated start order; a pair's strips keep their left-to-right order
-        std::stable_sort(us.begin(), us.end(), [](const U &x, const U &y) {
-            return x.start != y.start ? x.start < y.start : (x.slot != y.slot ? x.slot < y.slot : x.s < y.s);
-        });
+        std::stable_sort(us.begin(), us.end(), by_start);
         for (const U &x : us) bp.units.push_back(make_int2(x.slot, x.s));
         W.nunit = (int)us.size();
         W.nstrip = (int)bp.strips.size() - W.strip0;
         W.tb_bytes = tb, W.bnd_entries = bnd;
         bp.tb_cap = std::max(bp.tb_cap, tb);
         bp.bnd_cap = std::max(bp.bnd_cap, bnd);
-        // checkpoint groups of this wave's recomputed pairs, last group first
-        W.group0 = (int)bp.groups.size();
-        for (int slot = W.pair0; slot < W.pair0 + W.npair; ++slot) {
-            const BandPairDev &pd = bp.pairs[slot];
-            if (!pd.ckpt) continue;
-            const PairGeo &G = *std::find_if(geo.begin(), geo.end(), [&](const PairGeo &x) { return x.id == pd.idx; });
-            for (int gi = (int)G.groups.size() - 1; gi >= 0; --gi) {
-                BandGroup gr;
-                gr.slot = slot, gr.s0 = G.groups[gi].first, gr.s1 = G.groups[gi].second;
-                gr.unit0 = (int)bp.units.size();
-                for (int s = gr.s0; s < gr.s1; ++s) bp.units.push_back(make_int2(slot, s));
-                gr.nunit = gr.s1 - gr.s0;
-                gr.col_lo = gr.s0 * SW;
-                gr.last = gi == 0 ? 1 : 0;
-                gr.tb_bytes = G.gtb[gi];
-                bp.tb_cap = std::max(bp.tb_cap, G.gtb[gi]);
-                bp.groups.push_back(gr);
+        // Recompute rounds: each recomputed pair gets a share of the round budget in proportion
+        // to its whole traceback (so that all pairs need about as many rounds) and is cut into
+        // groups of consecutive strips within it (at least one strip); round r recomputes the
+        // r-th group from the right of every pair that has one, all together.
+        W.round0 = (int)bp.rounds.size();
+        std::vector<std::vector<std::pair<int, int>>> groups(ck.size());  // per pair: [s0, s1) right to left
+        std::vector<std::vector<int64_t>> gtb(ck.size());
+        double tb_all = 0;
+        for (size_t c = 0; c < ck.size(); ++c)
+            for (int64_t x : geo[ck[c].second].stb) tb_all += (double)x;
+        size_t nround = 0;
+        for (size_t c = 0; c < ck.size(); ++c) {
+            const PairGeo &G = geo[ck[c].second];
+            double tb_pair = 0;
+            for (int64_t x : G.stb) tb_pair += (double)x;
+            const int64_t share = std::max<int64_t>((int64_t)((double)gres * tb_pair / std::max(tb_all, 1.0)), 1);
+            int s1 = (int)G.strips.size();
+            while (s1 > 0) {
+                int s0 = s1 - 1;
+                int64_t acc = G.stb[s0];
+                while (s0 > 0 && acc + G.stb[s0 - 1] <= share) acc += G.stb[--s0];
+                groups[c].push_back({s0, s1});
+                gtb[c].push_back(acc);
+                s1 = s0;
             }
+            nround = std::max(nround, groups[c].size());
         }
-        W.ngroup = (int)bp.groups.size() - W.group0;
+        for (size_t r = 0; r < nround; ++r) {
+            BandRound R;
+            R.group0 = (int)bp.groups.size(), R.unit0 = (int)bp.units.size(), R.nstrip = 0;
+            int64_t off = 0;
+            std::vector<U> ru;
+            for (size_t c = 0; c < ck.size(); ++c) {
+                if (r >= groups[c].size()) continue;
+                const int slot = ck[c].first;
+                const PairGeo &G = geo[ck[c].second];
+                const BandPairDev &pd = bp.pairs[slot];
+                const int s0 = groups[c][r].first, s1 = groups[c][r].second;
+                BandGroupDev gd;
+                gd.slot = slot, gd.s_first = pd.strip0 + s0, gd.s_end = pd.strip0 + s1;
+                gd.left = s0 > 0 ? pd.strip0 + s0 - 1 : -1;
+                gd.col_lo = s0 * SW;
+                gd.last = r + 1 == groups[c].size() ? 1 : 0;
+                gd.pad0 = gd.pad1 = 0;
+                bp.groups.push_back(gd);
+                int64_t o = off;
+                for (int s = s0; s < s1; ++s) {
+                    bp.strips[pd.strip0 + s].tb_off = o;  // this round's arena
+                    o += G.stb[s];
+                    ru.push_back(U{G.start[s] - G.start[s0], slot, s});
+                }
+                off += gtb[c][r];
+                R.nstrip += s1 - s0;
+            }
+            std::stable_sort(ru.begin(), ru.end(), by_start);
+            for (const U &x : ru) bp.units.push_back(make_int2(x.slot, x.s));
+            R.ngroup = (int)bp.groups.size() - R.group0;
+            R.nunit = (int)ru.size();
+            R.tb_bytes = off;
+            bp.tb_cap = std::max(bp.tb_cap, off);
+            bp.rounds.push_back(R);
+        }
+        W.nround = (int)bp.rounds.size() - W.round0;
         bp.waves.push_back(W);
     }
     return 0;
@@ -1080,19 +1124,17 @@ cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, cons
     memset(b.mat, 0, sizeof(b.mat));
     memcpy(b.mat, mat, (size_t)m * m);
     b.m = m, b.flag = flag, b.block = bp.block;
-    for (int gi = W.group0; gi < W.group0 + W.ngroup; ++gi) {
-        const BandGroup &G = bp.groups[gi];
-        const BandPairDev &P = bp.pairs[G.slot];
-        const int sfirst = P.strip0 + G.s0, send = P.strip0 + G.s1;
-        band_group_progress_kernel<<<(G.nunit + 255) / 256, 256, 0, st>>>(D.progress, sfirst, send,
-                                                                          G.s0 > 0 ? sfirst - 1 : -1);
+    for (int ri = W.round0; ri < W.round0 + W.nround; ++ri) {
+        const BandRound &R = bp.rounds[ri];
+        const BandGroupDev *gd = D.groups + R.group0;
+        band_round_progress_kernel<<<R.ngroup, 256, 0, st>>>(D.progress, gd);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        // this group's counter of the work queue: the wave's slot, reused per group
+        // this round's counter of the work queue: the wave's slot, reused per round
         if ((e = cudaMemsetAsync(D.queue + 64 * k, 0, sizeof(int32_t), st)) != cudaSuccess) return e;
         BandArgs a;
         a.qcodes = qcodes, a.tcodes = tcodes;
-        a.pairs = D.pairs, a.strips = D.strips, a.units = D.units + G.unit0;
-        a.n_units = G.nunit;
+        a.pairs = D.pairs, a.strips = D.strips, a.units = D.units + R.unit0;
+        a.n_units = R.nunit;
         a.queue = D.queue + 64 * k, a.progress = D.progress, a.error = D.error;
         a.tb = D.tb, a.bnd = D.bnd, a.res = D.res;
         a.sc = S;
@@ -1101,13 +1143,9 @@ cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, cons
         a.store_ckpt = 1;
         a.deadline = D.deadline;
         if ((e = band_launch_units(bp, a, flag, ctas, st)) != cudaSuccess) return e;
-        if (bp.nc == 4) ksw_band_walk_kernel<4><<<1, 32, 0, st>>>(b, G.slot, G.col_lo);
-        else ksw_band_walk_kernel<8><<<1, 32, 0, st>>>(b, G.slot, G.col_lo);
+        if (bp.nc == 4) ksw_band_round_walk_kernel<4><<<R.ngroup, 32, 0, st>>>(b, gd);
+        else ksw_band_round_walk_kernel<8><<<R.ngroup, 32, 0, st>>>(b, gd);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (G.last) {
-            ksw_band_walk_finish_kernel<<<1, 32, 0, st>>>(b, G.slot);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        }
     }
     return cudaSuccess;
 }

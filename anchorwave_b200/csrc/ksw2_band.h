@@ -43,7 +43,7 @@ struct BandWave {
     int unit0, nunit;    // units [unit0, unit0 + nunit) of the unit table
     int strip0, nstrip;  // strip descriptors used by this wave
     int64_t tb_bytes, bnd_entries;
-    int group0, ngroup;  // checkpoint groups of this wave's recomputed pairs, in walk order
+    int round0, nround;  // recompute rounds of this wave's recomputed pairs, in walk order
 };
 
 // Walk state of a pair whose traceback is recomputed group by group (see band_plan_build).
@@ -53,20 +53,32 @@ struct BandWalkState {
     int32_t done, pad;     // 1: nothing (left) to walk
 };
 
-// A group of consecutive strips [s0, s1) of one recomputed pair: its traceback fits the
-// budget; the walk visits groups from the last to the first.
-struct BandGroup {
-    int slot;           // pair slot
-    int s0, s1;
-    int unit0, nunit;   // units of this group (its strips, left to right)
-    int col_lo;         // first target column of the group
-    int last;           // 1: the pair's first group (the walk ends here)
+// A group of consecutive strips of one recomputed pair (device layout): its strips run again
+// with their traceback stored, then the pair's walk continues through them.  The walk visits
+// a pair's groups from the last to the first.
+struct BandGroupDev {
+    int32_t slot;             // pair slot
+    int32_t s_first, s_end;   // strip descriptors [s_first, s_end) (global indices)
+    int32_t left;             // the strip on the group's left (its stored column is the input), or -1
+    int32_t col_lo;           // first target column of the group
+    int32_t last;             // 1: the pair's first group (the walk ends here)
+    int32_t pad0, pad1;
+};
+
+// One recompute round of a wave: one group of every recomputed pair that still has one, run
+// together (their strips in one launch, their walks in another); the groups of a round share
+// the traceback arena, each at its own offset.
+struct BandRound {
+    int group0, ngroup;  // groups [group0, group0 + ngroup) of the group table
+    int unit0, nunit;    // their strips, in estimated start order
+    int nstrip;          // strips to reset
     int64_t tb_bytes;
 };
 
 struct BandPlan {
     std::vector<BandPairDev> pairs;
-    std::vector<BandGroup> groups;
+    std::vector<BandGroupDev> groups;
+    std::vector<BandRound> rounds;
     std::vector<BandStripDev> strips;
     std::vector<int2> units;  // (pair slot, strip) in processing order
     std::vector<BandWave> waves;
@@ -106,6 +118,7 @@ struct BandDev {
     uint8_t *tb;
     int32_t *error;
     const unsigned long long *deadline = nullptr;  // the calling thread's deadline word, or null
+    const BandGroupDev *groups = nullptr;          // the group table of the recompute rounds
 };
 
 int band_occupancy(int flag);
@@ -117,8 +130,8 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
 cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
                                const uint8_t *tcodes, const KswScore &S, int flag, KswOut *out, uint32_t *cig,
                                const int8_t *mat, int m, cudaStream_t st);
-// Enqueues the group-by-group traceback of wave k's recomputed pairs: for each group,
-// its strips again with their traceback stored, then the walk through them.
+// Enqueues the recompute rounds of wave k's recomputed pairs: per round, the strips of one
+// group of every such pair again with their traceback stored, then the walks through them.
 cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, const uint8_t *qcodes,
                                const uint8_t *tcodes, const KswScore &S, int flag, KswOut *out, uint32_t *cig,
                                const int8_t *mat, int m, int ctas, cudaStream_t st);

@@ -192,11 +192,13 @@ using namespace aw;
 extern "C" {
 
 int aw_align_score_certified_batch(int n, const char *const *query, const int64_t *qlen, const char *const *reference,
-                                   const int64_t *rlen, int64_t initial_band_width, int64_t maximum_band_width,
-                                   int32_t mis, int32_t o1, int32_t e1, int32_t o2, int32_t e2,
-                                   double maximum_runtime_seconds, const int64_t *precomputed_optimal_scores,
-                                   aw_certified_result_t *out) {
-    if (n < 0 || (n > 0 && (!query || !qlen || !reference || !rlen || !out))) return AW_E_INVAL;
+                                   const int64_t *rlen, const int64_t *initial_band_width,
+                                   const int64_t *maximum_band_width, int32_t mis, int32_t o1, int32_t e1, int32_t o2,
+                                   int32_t e2, double maximum_runtime_seconds,
+                                   const int64_t *precomputed_optimal_scores, aw_certified_result_t *out) {
+    if (n < 0 || (n > 0 && (!query || !qlen || !reference || !rlen || !out || !initial_band_width ||
+                            !maximum_band_width)))
+        return AW_E_INVAL;
     for (int i = 0; i < n; ++i)
         if (qlen[i] < 0 || rlen[i] < 0 || qlen[i] > INT32_MAX / 2 || rlen[i] > INT32_MAX / 2) return AW_E_INVAL;
     std::vector<Cert> C(n);
@@ -214,7 +216,7 @@ int aw_align_score_certified_batch(int n, const char *const *query, const int64_
             const int64_t L = std::max(qlen[i], rlen[i]);
             r.score = r.optimal = std::max<int64_t>((int64_t)o1 + (int64_t)e1 * L, (int64_t)o2 + (int64_t)e2 * L);
             r.final_band = 0, r.attempts = 1, r.status = kCompleted;
-        } else if (initial_band_width < 0 || maximum_band_width < 0 || maximum_band_width < diff) {
+        } else if (initial_band_width[i] < 0 || maximum_band_width[i] < 0 || maximum_band_width[i] < diff) {
             r.status = kNotCertified;
         } else {
             todo.push_back(i);
@@ -246,8 +248,8 @@ int aw_align_score_certified_batch(int n, const char *const *query, const int64_
                 continue;
             }
             const int64_t diff = std::llabs(qlen[i] - rlen[i]);
-            const int64_t max_band = std::min<int64_t>(std::max(qlen[i], rlen[i]), maximum_band_width);
-            const int64_t requested = std::max<int64_t>(diff, std::max<int64_t>(1, initial_band_width));
+            const int64_t max_band = std::min<int64_t>(std::max(qlen[i], rlen[i]), maximum_band_width[i]);
+            const int64_t requested = std::max<int64_t>(diff, std::max<int64_t>(1, initial_band_width[i]));
             const int64_t doubled = requested * 2;
             int64_t band = std::min(max_band, std::max(requested, doubled));
             while (band >= diff && band <= max_band) {
@@ -316,12 +318,15 @@ void aw_certified_result_free(aw_certified_result_t *r) {
 }
 
 int aw_align_sliding_window_batch(int n, const char *const *query, const int64_t *qlen, const char *const *reference,
-                                  const int64_t *rlen, int64_t W, int32_t match, int32_t mis, int32_t o1, int32_t e1,
-                                  int32_t o2, int32_t e2, aw_window_result_t *out) {
-    if (n < 0 || (n > 0 && (!query || !qlen || !reference || !rlen || !out)) || W <= 0) return AW_E_INVAL;
-    if (W > 1073741824) {
-        set_error("aw_align_sliding_window_batch: the windows size is too large");
-        return AW_E_INVAL;
+                                  const int64_t *rlen, const int64_t *window, int32_t match, int32_t mis, int32_t o1,
+                                  int32_t e1, int32_t o2, int32_t e2, aw_window_result_t *out) {
+    if (n < 0 || (n > 0 && (!query || !qlen || !reference || !rlen || !out || !window))) return AW_E_INVAL;
+    for (int i = 0; i < n; ++i) {
+        if (window[i] <= 0) return AW_E_INVAL;
+        if (window[i] > 1073741824) {
+            set_error("aw_align_sliding_window_batch: the windows size is too large");
+            return AW_E_INVAL;
+        }
     }
     std::vector<std::string> Q(n), D(n), AQ(n), AD(n);
     std::vector<int64_t> qs(n, 1), ds(n, 1);
@@ -330,7 +335,7 @@ int aw_align_sliding_window_batch(int n, const char *const *query, const int64_t
         if (qlen[i] < 0 || rlen[i] < 0 || qlen[i] > INT32_MAX / 2 || rlen[i] > INT32_MAX / 2) return AW_E_INVAL;
         Q[i].assign(query[i] ? query[i] : "", (size_t)qlen[i]);
         D[i].assign(reference[i] ? reference[i] : "", (size_t)rlen[i]);
-        whole[i] = ((double)rlen[i] / (double)W) * ((double)qlen[i] / (double)W) <= 1.0;
+        whole[i] = ((double)rlen[i] / (double)window[i]) * ((double)qlen[i] / (double)window[i]) <= 1.0;
     }
     // the windows' penalties (:531-535)
     int wm, wo1, we1, wo2, we2;
@@ -359,6 +364,7 @@ int aw_align_sliding_window_batch(int n, const char *const *query, const int64_t
             for (int i = 0; i < n; ++i) {
                 if (whole[i] || !(ds[i] <= rlen[i] && qs[i] <= qlen[i])) continue;
                 // getSubsequence(seq, start, start + W): 1-based, inclusive, clamped at the end
+                const int64_t W = window[i];
                 const int64_t qe = std::min<int64_t>(qs[i] + W, qlen[i]), de = std::min<int64_t>(ds[i] + W, rlen[i]);
                 jobs.push_back(Job{i, Q[i].substr((size_t)qs[i] - 1, (size_t)(qe - qs[i] + 1)),
                                    D[i].substr((size_t)ds[i] - 1, (size_t)(de - ds[i] + 1)), -1});

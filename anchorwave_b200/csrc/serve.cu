@@ -2,9 +2,10 @@
 // that stands in for AnchorWave's CPU alignment thread pool
 // (src/service/AnchorTaskExecutor.h:54-160, ParallelGapBatchScheduler.h:39-280).
 //
-//   * aw_serve_submit() enqueues one interval as the anchor stage emits it, with
-//     the engine the caller's selector chose for it (KSW2 full/banded, KSW2
-//     Singletrack, WFA, WFA Singletrack);
+//   * aw_serve_submit() / aw_serve_submit_route() enqueue one interval as the anchor
+//     stage emits it, with the engine the caller's selector chose for it (KSW2
+//     full/banded, KSW2 Singletrack, WFA in its four memory modes, score-certified KSW2,
+//     sliding-window KSW2) and that engine's parameters;
 //   * `slots` worker threads each own their CUDA streams and pooled device
 //     buffers (the thread-local pools of the batch entries); requests wait in one
 //     FIFO per engine/parameter class, and an idle worker takes the class whose
@@ -48,7 +49,8 @@ double now_s() {
 
 struct Req {
     uint64_t id;
-    int method, band;
+    int method, band, band_max;
+    int64_t window;
     std::string q, t;  // ASCII
     int64_t pred;
     double t_submit;
@@ -67,6 +69,16 @@ struct Res {
 
 int64_t predict_bytes(const Req &rq) {
     const int64_t ql = (int64_t)rq.q.size(), tl = (int64_t)rq.t.size();
+    if (rq.method == AW_ROUTE_KSW2_CERTIFIED) {
+        // the largest banded traceback of the certification (the score pass keeps none)
+        const int64_t n = std::min(std::min(ql, tl), (int64_t)std::max(rq.band, rq.band_max) + 1);
+        return (ql + tl) * ((n + 63) / 64 + 1) * 64;
+    }
+    if (rq.method == AW_ROUTE_SLIDING_WINDOW) {
+        // one window's full traceback at a time
+        const int64_t w = std::max<int64_t>(1, std::min<int64_t>(rq.window + 1, std::max(ql, tl)));
+        return ksw_full_tb_bytes((int)std::min<int64_t>(w, ql), (int)std::min<int64_t>(w, tl));
+    }
     if (rq.method >= AW_ROUTE_WFA) {
         // wavefront retention grows with the alignment score; a length-based proxy (the
         // piggyback modes keep a ring of recent scores and about 1.6 bytes of blocks per cell)
@@ -155,6 +167,60 @@ int64_t wfa_pool_share(const aw_server *S, int method) {
     return worker_share(S) * pct / 100;
 }
 
+// Gapped rows -> a KSW2-style CIGAR (M/I/D runs), malloc'd into ez.
+void rows_to_cigar(const char *q, const char *d, int64_t n, ksw_extz_t &ez) {
+    std::vector<uint32_t> cg;
+    int64_t i = 0;
+    while (i < n) {
+        const uint32_t op = q[i] == '-' ? 2u : d[i] == '-' ? 1u : 0u;
+        int64_t j = i + 1;
+        while (j < n && (q[j] == '-' ? 2u : d[j] == '-' ? 1u : 0u) == op) ++j;
+        cg.push_back((uint32_t)(j - i) << 4 | op);
+        i = j;
+    }
+    ez.n_cigar = ez.m_cigar = (int)cg.size();
+    ez.cigar = cg.empty() ? nullptr : (uint32_t *)malloc(sizeof(uint32_t) * cg.size());
+    if (ez.cigar) memcpy(ez.cigar, cg.data(), sizeof(uint32_t) * cg.size());
+}
+
+// The rescue routes: the batch entries of rescue.cu with the server's scoring in
+// AnchorWave's form (mismatch = the matrix's off-diagonal score, gap penalties negative).
+void run_rescue_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out) {
+    const aw_serve_config_t &C = S->cfg;
+    const int n = (int)batch.size();
+    const int mis = C.mat[1], o1 = -C.q, e1 = -C.e, o2 = -C.q2, e2 = -C.e2;
+    std::vector<const char *> qp(n), dp(n);
+    std::vector<int64_t> ql(n), dl(n), b0(n), b1(n), win(n);
+    for (int i = 0; i < n; ++i) {
+        qp[i] = batch[i].q.data(), dp[i] = batch[i].t.data();
+        ql[i] = (int64_t)batch[i].q.size(), dl[i] = (int64_t)batch[i].t.size();
+        b0[i] = batch[i].band, b1[i] = batch[i].band_max, win[i] = batch[i].window;
+    }
+    if (batch[0].method == AW_ROUTE_KSW2_CERTIFIED) {
+        std::vector<aw_certified_result_t> r(n);
+        const int rc = aw_align_score_certified_batch(n, qp.data(), ql.data(), dp.data(), dl.data(), b0.data(),
+                                                      b1.data(), mis, o1, e1, o2, e2, 0.0, nullptr, r.data());
+        for (int i = 0; i < n; ++i) {
+            out[i].r.status = rc ? rc : r[i].status;
+            out[i].r.ez.score = (int)r[i].score;
+            if (r[i].alignment_len > 0) rows_to_cigar(r[i].alignment_q, r[i].alignment_d, r[i].alignment_len, out[i].r.ez);
+            else if (r[i].best_effort_len > 0)
+                rows_to_cigar(r[i].best_effort_q, r[i].best_effort_d, r[i].best_effort_len, out[i].r.ez);
+            aw_certified_result_free(&r[i]);
+        }
+    } else {
+        std::vector<aw_window_result_t> r(n);
+        const int rc = aw_align_sliding_window_batch(n, qp.data(), ql.data(), dp.data(), dl.data(), win.data(), 0, mis,
+                                                     o1, e1, o2, e2, r.data());
+        for (int i = 0; i < n; ++i) {
+            out[i].r.status = rc;
+            out[i].r.ez.score = (int)r[i].score;
+            if (r[i].alignment_len > 0) rows_to_cigar(r[i].alignment_q, r[i].alignment_d, r[i].alignment_len, out[i].r.ez);
+            aw_window_result_free(&r[i]);
+        }
+    }
+}
+
 void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wavefront_aligner_gpu_t **al) {
     const aw_serve_config_t &C = S->cfg;
     const int n = (int)batch.size();
@@ -165,7 +231,9 @@ void run_batch(aw_server *S, std::vector<Req> &batch, std::vector<Res> &out, wav
         out[i].r.method = batch[i].method;
     }
     const int method = batch[0].method;
-    if (method == AW_ROUTE_KSW2 || method == AW_ROUTE_KSW2_SINGLETRACK) {
+    if (method == AW_ROUTE_KSW2_CERTIFIED || method == AW_ROUTE_SLIDING_WINDOW) {
+        run_rescue_batch(S, batch, out);
+    } else if (method == AW_ROUTE_KSW2 || method == AW_ROUTE_KSW2_SINGLETRACK) {
         std::vector<std::vector<uint8_t>> qs(n), ts(n);
         bool generic = false;
         for (int i = 0; i < n; ++i) generic |= encode(batch[i].q, qs[i]), generic |= encode(batch[i].t, ts[i]);
@@ -303,9 +371,23 @@ aw_server_t *aw_serve_open(const aw_serve_config_t *cfg) {
 
 int aw_serve_submit(aw_server_t *S, uint64_t id, int method, int band, const char *query, int qlen,
                     const char *target, int tlen) {
-    if (!S || qlen < 0 || tlen < 0 || method < AW_ROUTE_KSW2 || method > AW_ROUTE_WFA_LOW) return AW_E_INVAL;
+    aw_serve_route_t rt;
+    rt.method = method, rt.band = band, rt.band_max = -1, rt.window = 0;
+    return aw_serve_submit_route(S, id, &rt, query, qlen, target, tlen);
+}
+
+int aw_serve_submit_route(aw_server_t *S, uint64_t id, const aw_serve_route_t *route, const char *query, int qlen,
+                          const char *target, int tlen) {
+    if (!S || !route || qlen < 0 || tlen < 0 || route->method < AW_ROUTE_KSW2 ||
+        route->method > AW_ROUTE_SLIDING_WINDOW)
+        return AW_E_INVAL;
+    const int method = route->method;
+    if (method == AW_ROUTE_SLIDING_WINDOW && route->window <= 0) {
+        set_error("aw_serve_submit_route: the sliding-window route needs window > 0");
+        return AW_E_INVAL;
+    }
     Req r;
-    r.id = id, r.method = method, r.band = band;
+    r.id = id, r.method = method, r.band = route->band, r.band_max = route->band_max, r.window = route->window;
     r.q.assign(query ? query : "", (size_t)qlen);
     r.t.assign(target ? target : "", (size_t)tlen);
     r.pred = predict_bytes(r);

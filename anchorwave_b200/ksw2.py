@@ -466,7 +466,7 @@ def _text(ptr, n) -> str:
     return C.string_at(ptr, n).decode() if ptr and n > 0 else ""
 
 
-def align_score_certified_ksw2_batch(pairs, initial_band_width: int, maximum_band_width: int,
+def align_score_certified_ksw2_batch(pairs, initial_band_width, maximum_band_width,
                                      mismatching_penalty: int, open1: int, extend1: int, open2: int, extend2: int,
                                      maximum_runtime_seconds: float = 0.0,
                                      precomputed_optimal_scores=None) -> List[CertifiedResult]:
@@ -485,9 +485,11 @@ def align_score_certified_ksw2_batch(pairs, initial_band_width: int, maximum_ban
     pre = None
     if precomputed_optimal_scores is not None:
         pre = np.ascontiguousarray(np.asarray(precomputed_optimal_scores, dtype=np.int64))
+    ib = np.broadcast_to(np.asarray(initial_band_width, dtype=np.int64), (n,)).copy()
+    mb = np.broadcast_to(np.asarray(maximum_band_width, dtype=np.int64), (n,)).copy()
     out = (CertResultC * n)()
-    rc = lib.aw_align_score_certified_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, int(initial_band_width),
-                                            int(maximum_band_width), mismatching_penalty, open1, extend1, open2,
+    rc = lib.aw_align_score_certified_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, ib.ctypes.data,
+                                            mb.ctypes.data, mismatching_penalty, open1, extend1, open2,
                                             extend2, float(maximum_runtime_seconds or 0.0),
                                             pre.ctypes.data if pre is not None else None, out)
     res = []
@@ -516,7 +518,7 @@ def align_score_certified_ksw2(dna_q: str, dna_d: str, initial_band_width: int, 
 
 # ---- sliding-window semiglobal alignment (alignSlidingWindow.cpp:457-590) ----------------
 
-def align_sliding_window_batch(pairs, sliding_window_size: int, matching_score: int, mismatching_penalty: int,
+def align_sliding_window_batch(pairs, sliding_window_size, matching_score: int, mismatching_penalty: int,
                                open1: int, extend1: int, open2: int, extend2: int) -> List[Tuple[int, str, str]]:
     """alignSlidingWindow (alignSlidingWindow.cpp:457-590) for many intervals, through
     aw_align_sliding_window_batch: an interval whose (len_d / W) * (len_q / W) <= 1 gets one
@@ -525,15 +527,16 @@ def align_sliding_window_batch(pairs, sliding_window_size: int, matching_score: 
     window of every interval still advancing runs in one batched call.  Returns (score of the
     whole alignment under the two-piece objective, aligned query, aligned reference) per
     interval, as a call of its own would."""
-    if int(sliding_window_size) > 1073741824:
-        raise ValueError("the windows size is too large")
     n = len(pairs)
     if n == 0:
         return []
+    win = np.broadcast_to(np.asarray(sliding_window_size, dtype=np.int64), (n,)).copy()
+    if int(win.max()) > 1073741824:
+        raise ValueError("the windows size is too large")
     qp, ql, qb = _seq_arrays([p[0] for p in pairs])
     rp, rl, rb = _seq_arrays([p[1] for p in pairs])
     out = (WindowResultC * n)()
-    rc = lib.aw_align_sliding_window_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, int(sliding_window_size),
+    rc = lib.aw_align_sliding_window_batch(n, qp, ql.ctypes.data, rp, rl.ctypes.data, win.ctypes.data,
                                            matching_score, mismatching_penalty, open1, extend1, open2, extend2, out)
     res = []
     for o in out:

@@ -12,7 +12,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from ._lib import AwError, ServeConfig, ServeResult, ServeStats, last_error, lib
+from ._lib import AwError, ServeConfig, ServeResult, ServeRoute, ServeStats, last_error, lib
 
 ROUTE_KSW2 = 0
 ROUTE_KSW2_SINGLETRACK = 1
@@ -20,6 +20,9 @@ ROUTE_WFA = 2
 ROUTE_WFA_SINGLETRACK = 3
 ROUTE_WFA_MEDIUM = 4
 ROUTE_WFA_LOW = 5
+ROUTE_KSW2_CERTIFIED = 6
+ROUTE_SLIDING_WINDOW = 7
+KSW2_ROUTES = (ROUTE_KSW2, ROUTE_KSW2_SINGLETRACK, ROUTE_KSW2_CERTIFIED, ROUTE_SLIDING_WINDOW)
 
 
 @dataclass
@@ -28,7 +31,8 @@ class ServedAlignment:
     method: int
     status: int
     latency_s: float
-    ksw: Optional[tuple] = None      # ksw_extz_t key (fields + CIGAR), KSW2 routes
+    ksw: Optional[tuple] = None      # ksw_extz_t key (fields + CIGAR), KSW2 routes (the rescue routes:
+                                     # their rows as a CIGAR and the re-scored score)
     wfa: Optional[tuple] = None      # (status, score, ops), WFA routes
 
 
@@ -46,10 +50,15 @@ class AlignmentServer:
         if not self.h:
             raise AwError(f"aw_serve_open failed: {last_error()}")
 
-    def submit(self, rid: int, method: int, query: bytes, target: bytes, band: int = -1):
-        rc = lib.aw_serve_submit(self.h, rid, method, band, query, len(query), target, len(target))
+    def submit(self, rid: int, method: int, query: bytes, target: bytes, band: int = -1, band_max: int = -1,
+               window: int = 0):
+        """Enqueue one interval with its engine and that engine's parameters (band: KSW2 band,
+        or score-certified KSW2's initial band; band_max: its largest band; window: the
+        sliding-window width)."""
+        rt = ServeRoute(method, band, band_max, window)
+        rc = lib.aw_serve_submit_route(self.h, rid, C.byref(rt), query, len(query), target, len(target))
         if rc != 0:
-            raise AwError(f"aw_serve_submit failed ({rc})")
+            raise AwError(f"aw_serve_submit_route failed ({rc}): {last_error()}")
 
     def poll(self, max_results: int = 1024, wait_ms: int = 0) -> List[ServedAlignment]:
         buf = (ServeResult * max_results)()
@@ -58,7 +67,7 @@ class AlignmentServer:
         for i in range(n):
             r = buf[i]
             item = ServedAlignment(int(r.id), int(r.method), int(r.status), float(r.latency_s))
-            if r.method in (ROUTE_KSW2, ROUTE_KSW2_SINGLETRACK):
+            if r.method in KSW2_ROUTES:
                 ez = r.ez
                 # one copy of the CIGAR words (indexing a ctypes pointer word by word costs
                 # more than the alignment itself for long intervals)

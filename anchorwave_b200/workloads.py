@@ -198,6 +198,17 @@ def band_cells(qlen: int, tlen: int, w: int) -> int:
     return int((en - st + 1).sum())
 
 
+def band_reaches_end(qlen: int, tlen: int, w: int) -> bool:
+    """True when no anti-diagonal's band is empty (ksw2_extd2_sse.c:151-154); otherwise the
+    reference stops at the first empty one and reports zdropped = 1 with no CIGAR."""
+    if w < 0 or w > max(qlen, tlen):
+        return True
+    r = np.arange(qlen + tlen - 1, dtype=np.int64)
+    st = np.maximum(np.maximum(0, r - qlen + 1), (r - w + 1) >> 1)
+    en = np.minimum(np.minimum(tlen - 1, r), (r + w) >> 1)
+    return bool((st <= en).all())
+
+
 @dataclass
 class Request:
     id: int

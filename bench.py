@@ -24,8 +24,9 @@ and the CIGARs.
     per cell / DP-phase CUDA-event time) is set against the packed-field peak measured live
     by aw_int16x2_peak_ops() (the 32-bit peak, aw_int32_peak_ops(), is reported beside it);
     the traceback store stream is reported against HBM bandwidth.
-  * serving: a 20,000-request trace through the continuous-batching server (saturated and at
-    80% offered load with p50/p99 latency).
+  * serving: a 20,000-request trace (lengths to 500 kb) routed by AnchorWave's own selector,
+    through the continuous-batching server under a 150 GB HBM budget (saturated and at 80%
+    offered load with p50/p99 latency), beside the plain per-call GPU path on a sample.
   * long_banded: 64 pairs of 100 kb-1 Mb, w = 10%, banded and Singletrack (one execution
     each), every CIGAR checked and re-scored, beside the reference's CPU code on the pairs
     whose host traceback fits a safe share of the host memory.
@@ -274,64 +275,141 @@ def run_reference_arm(args):
 
 # Serving configuration: two workers (each with half of the device budget for its pooled
 # traceback arena and wavefront pools) and micro-batches of up to 1,024 requests gave the
-# best saturated rate and 70%-load latency on the trace (more workers split the budget into
-# smaller arenas, so the long banded class runs in more waves).
+# best saturated rate and latency on the trace (more workers split the budget into smaller
+# arenas, so the long banded class runs in more waves).
 SERVE_SLOTS, SERVE_BATCH = 2, 1024
 # offered load of the latency run, as a fraction of the saturated request rate
 SERVE_LOAD = 0.8
+# the HBM budget of the serving workload (traceback arenas and wavefront pools)
+SERVE_HBM_BUDGET = 150 * 10**9
 
 
-def serving_measurement(nreq: int, rank: int):
-    """Serving trace (lengths log-normal, median 2 kb, sigma 1, clipped to 50 bp-50 kb here;
-    low-divergence intervals up to 10 kb on WFA, > 20 kb banded KSW2, the rest full KSW2; 10%
-    with repeat structure) through the
-    continuous-batching server: saturated throughput with all requests queued at once, then
-    p50/p99 latency with Poisson arrivals at 80% of that rate."""
+def plain_route_call(rt, q: bytes, t: bytes, mat, aligners):
+    """One interval through the single-call form of its routed engine (the plain per-call GPU
+    path): ksw_extd2_gpu / ksw_extd2_singletrack_gpu, wavefront_align_gpu, or the rescue
+    procedures on one interval.  Returns a comparable result."""
+    from anchorwave_b200 import ksw2, wfa
+    pen = (-4, -4, -2, -24, -1)
+    if rt.method in (0, 1):
+        qc, f1 = ksw2.encode(q)
+        tc, f2 = ksw2.encode(t)
+        fn = ksw2.ksw_extd2_singletrack if rt.method == 1 else ksw2.ksw_extd2
+        r = fn(qc, tc, mat, 4, 2, 24, 1, w=rt.band, flag=f1 | f2)
+        return (r.score, tuple(r.cigar))
+    if rt.method in (2, 3, 4, 5):
+        al = aligners.get(rt.method)
+        if al is None:
+            al = aligners[rt.method] = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=rt.method == 3,
+                                                      memory_mode=max(0, rt.method - 3))
+        st = al.align(t, q)
+        ops, score = al.cigar() if st == 0 else ("", 0)
+        return (st, score, ops)
+    if rt.method == 6:
+        r = ksw2.align_score_certified_ksw2(q.decode(), t.decode(), rt.band, rt.band_max, *pen)
+        return (r.status, r.score)
+    return ksw2.align_sliding_window(q.decode(), t.decode(), rt.window, 0, *pen)[0]
+
+
+def serving_measurement(nreq: int, rank: int, plain_sample: int = 400):
+    """Serving trace (lengths log-normal, median 2 kb, sigma 1, clipped to 50 bp-500 kb;
+    divergence and indels as the batched workload; 10% with repeat structure).  Every request
+    is routed by AnchorWave's own selector (the routing front end: makeAlignmentSelectionPlan
+    and the executor's first choice on an idle system) before it is submitted, then the
+    continuous-batching server runs the trace under a 150 GB HBM budget: saturated
+    throughput with all requests queued at once, then p50/p99 latency with Poisson arrivals
+    at 80% of that rate.  Beside it, the plain per-call GPU path (each interval through the
+    single-call form of its routed engine) on a seeded sample of the same trace, whose results
+    must equal the served ones."""
+    import collections
+
     import numpy as np
 
     from anchorwave_b200 import ksw2, serve
     from anchorwave_b200 import workloads as W
-    reqs = W.serving_trace(nreq, seed=4 + rank, lmax=50_000)
+    try:
+        from anchorwave_b200 import route
+    except ImportError as e:
+        return {"unavailable": f"routing front end missing: {e}"}
+    reqs = W.serving_trace(nreq, seed=4 + rank, lmax=500_000)
+    t0 = time.perf_counter()
+    routes = route.route_intervals([(r.query, r.target) for r in reqs])
+    route_s = time.perf_counter() - t0
+    mix = collections.Counter(rt.candidate for rt in routes)
     cells = sum(len(r.query) * len(r.target) for r in reqs)
+    mat = ksw2.anchorwave_matrix(-4)
 
-    def run(rate):
+    def run(rate, keep=None):
         rng = np.random.default_rng(99)
-        with serve.AlignmentServer(ksw2.anchorwave_matrix(-4), 4, 2, 24, 1, slots=SERVE_SLOTS,
-                                   max_batch=SERVE_BATCH) as srv:
+        kept = {}
+        with serve.AlignmentServer(mat, 4, 2, 24, 1, slots=SERVE_SLOTS, max_batch=SERVE_BATCH,
+                                   hbm_budget=SERVE_HBM_BUDGET) as srv:
             t0 = time.perf_counter()
 
             def producer():
                 nxt = t0
-                for r in reqs:
+                for r, rt in zip(reqs, routes):
                     if rate:
                         nxt += rng.exponential(1.0 / rate)
                         d = nxt - time.perf_counter()
                         if d > 0:
                             time.sleep(d)
-                    srv.submit(r.id, r.method, r.query, r.target, r.band)
+                    srv.submit(r.id, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max,
+                               window=rt.window)
 
             th = threading.Thread(target=producer)
             th.start()
             got = 0
             while got < len(reqs):
-                got += len(srv.poll(4096, wait_ms=20))
+                batch = srv.poll(4096, wait_ms=20)
+                got += len(batch)
+                if keep is not None:
+                    for g in batch:
+                        if g.id in keep:
+                            kept[g.id] = g
             th.join()
             dt = time.perf_counter() - t0
             st = srv.stats()
-        return dt, st
+        return dt, st, kept
 
-    dt_sat, st_sat = run(None)
+    rng = np.random.default_rng(2024)
+    sample = sorted(rng.choice(len(reqs), size=min(plain_sample, len(reqs)), replace=False).tolist())
+    dt_sat, st_sat, served = run(None, keep=set(sample))
     sat = len(reqs) / dt_sat
-    dt, st = run(SERVE_LOAD * sat)
-    return {"requests": len(reqs), "cells": cells, "saturated_requests_per_s": sat,
-            "saturated_gcups": cells / dt_sat / 1e9,
+    dt, st, _ = run(SERVE_LOAD * sat)
+    # plain per-call GPU path on the sample, and its results against the served ones
+    aligners = {}
+    plain_s, same = 0.0, True
+    for i in sample:
+        r, rt = reqs[i], routes[i]
+        t1 = time.perf_counter()
+        res = plain_route_call(rt, r.query, r.target, mat, aligners)
+        plain_s += time.perf_counter() - t1
+        g = served[i]
+        if rt.method in (0, 1):
+            same &= (g.ksw[8], g.ksw[12]) == res
+        elif rt.method in (2, 3, 4, 5):
+            same &= g.wfa == res
+        elif rt.method == 6:
+            same &= g.ksw[8] == res[1]
+        else:
+            same &= g.ksw[8] == res
+    for al in aligners.values():
+        al.close()
+    plain_pps = len(sample) / plain_s
+    return {"requests": len(reqs), "cells": cells, "routing": dict(mix), "routing_s": route_s,
+            "routed_by": "AnchorWave's makeAlignmentSelectionPlan (compiled unchanged) + the executor's first "
+                         "choice on an idle system",
+            "saturated_requests_per_s": sat, "saturated_gcups": cells / dt_sat / 1e9,
             "saturated_server_requests_per_s": len(reqs) / st_sat["elapsed_s"] if st_sat["elapsed_s"] else None,
             "offered_requests_per_s": SERVE_LOAD * sat, "load": SERVE_LOAD,
             "requests_per_s": len(reqs) / dt, "gcups": cells / dt / 1e9,
             "latency_ms_p50": 1e3 * st["latency_p50_s"], "latency_ms_p99": 1e3 * st["latency_p99_s"],
             "micro_batches": st["micro_batches"], "slots": SERVE_SLOTS, "max_batch": SERVE_BATCH,
-            "trace": "log-normal lengths (median 2 kb, sigma 1) clipped to 50 bp-50 kb, WFA for d<=5% "
-                     "and <=10 kb, >20 kb banded (w=10%), 10% repeat-rich; Poisson arrivals at 80% of saturation; "
+            "hbm_budget": SERVE_HBM_BUDGET,
+            "plain_per_call": {"sample": len(sample), "requests_per_s": plain_pps,
+                               "served_vs_plain": sat / plain_pps, "results_identical_to_served": bool(same)},
+            "trace": "log-normal lengths (median 2 kb, sigma 1) clipped to 50 bp-500 kb, divergence U(1%,15%), 10% "
+                     "repeat-rich; routed by AnchorWave's selector; Poisson arrivals at 80% of saturation; "
                      "cells = sum of qlen*tlen"}
 
 
@@ -479,6 +557,7 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
     ps = W.long_banded_set(npairs, seed=3 + rank, lmin=lmin, lmax=lmax, long_max=long_max)
     mat = ksw2.anchorwave_matrix(-4)
     pair_cells = [W.band_cells(len(q), len(t), w) for q, t, w in zip(ps.queries, ps.targets, ps.band)]
+    reach = [W.band_reaches_end(len(q), len(t), w) for q, t, w in zip(ps.queries, ps.targets, ps.band)]
     bcells = sum(pair_cells)
     out = {"workload": ps.name, "pairs": len(ps), "band_cells": bcells,
            "shape": f"target U({lmin // 1000} kb, {lmax // 1000} kb), 30% repeats, 3% substitutions, "
@@ -498,17 +577,23 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
         res = plan.download()
         plan.close()
         results[name] = res
-        refused = [i for i, r in enumerate(res) if r.zdropped and r.n_cigar == 0]
+        # pairs whose band becomes empty before the end: zdropped, no CIGAR, as the reference
+        refused = [i for i, r in enumerate(res) if r.zdropped and r.n_cigar == 0 and reach[i]]
         ran = [i for i in range(len(ps)) if i not in set(refused)]
         rcells = sum(pair_cells[i] for i in ran)
         valid = rescored = 0
         for i in ran:
+            if not reach[i]:
+                continue
             ok, sc = cigar_check(res[i], ps.queries[i], ps.targets[i])
             valid += ok
             rescored += ok and sc == res[i].score
         out[name] = {"ms": ms, "dp_ms": dp, "traceback_ms": bt, "gcups": rcells / (ms * 1e-3) / 1e9,
-                     "pairs_run": len(ran), "refused_over_budget": len(refused), "waves": st["waves"],
-                     "cigars_spanning_both": valid, "cigars_rescoring_to_score": rescored}
+                     "pairs_run": len(ran), "band_unreachable": len(ps) - sum(reach),
+                     "refused_over_budget": len(refused), "cigars_spanning_both": valid,
+                     # a restrictive band may report a frontier score that differs from its CIGAR's
+                     # score (the reference re-scores for that reason, alignSlidingWindow.cpp:872-876)
+                     "cigars_rescoring_to_score": rescored}
         ksw2.release_thread_buffers()
     if cpu:
         from concurrent.futures import ThreadPoolExecutor
@@ -803,13 +888,16 @@ def compact_summary(line):
                             "ref_p50_ms": get(p5, "cpu_reference", "latency_ms_p50"),
                             "ref_p99_ms": get(p5, "cpu_reference", "latency_ms_p99"),
                             "identical": get(p5, "cpu_reference", "results_identical")}
-    sv = line.get("serving")
-    if sv:
-        out["serving"] = {k: sv.get(k) for k in ("requests", "saturated_requests_per_s", "requests_per_s",
-                                                 "latency_ms_p50", "latency_ms_p99", "load")}
     par = {"batched_full": get(line, "cpu_baseline", "parity")}
     if par["batched_full"]:
         par["batched_full"] = {k: par["batched_full"][k] for k in ("pairs_checked", "identical")}
+    sv = line.get("serving")
+    if sv:
+        out["serving"] = {k: sv.get(k) for k in ("requests", "saturated_requests_per_s", "requests_per_s",
+                                                 "latency_ms_p50", "latency_ms_p99", "load", "routing")}
+        if sv.get("plain_per_call"):
+            out["serving"]["served_vs_plain"] = sv["plain_per_call"]["served_vs_plain"]
+            par["serving_vs_plain"] = sv["plain_per_call"]["results_identical_to_served"]
     lb = line.get("long_banded")
     if lb:
         out["long_banded"] = {"pairs": lb["pairs"], "band_cells": lb["band_cells"]}
@@ -817,9 +905,9 @@ def compact_summary(line):
             if nm in lb:
                 x = lb[nm]
                 out["long_banded"][nm] = {"gcups": x.get("gcups"), "s": x["ms"] / 1e3, "run": x["pairs_run"],
+                                          "unreachable": x["band_unreachable"],
                                           "refused": x["refused_over_budget"],
                                           "valid": x["cigars_spanning_both"],
-                                          "rescored": x["cigars_rescoring_to_score"],
                                           "vs_ref": x.get("vs_cpu_reference")}
                 par[f"long_{nm}"] = {"pairs_checked": get(x, "cpu_reference", "pairs"),
                                      "identical": get(x, "cpu_reference", "results_identical")}

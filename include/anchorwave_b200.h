@@ -152,14 +152,16 @@ typedef struct {
  * certified in one banded batch, until its re-scored alignment reaches the optimum; the
  * skipped smallest band runs only on failure.  Every interval gets the result a call of its
  * own would give (the selector's chained traceback, used when a selection plan is passed,
- * stays with the caller).  Sequences are ASCII; penalties AnchorWave's (negative);
- * maximum_runtime_seconds > 0 arms the calling thread's deadline (aw_ksw_set_deadline) for
- * the call; precomputed_optimal_scores (n values, or NULL) skips the score-only batch.
- * Returns AW_OK or a negative AW_E* code; out[i] is filled either way.
+ * stays with the caller).  Sequences are ASCII; initial_band_width / maximum_band_width hold
+ * interval i's bands (the selection plan's ksw2CertifiedInitialBandWidth and
+ * ksw2CertifiedMaximumBandWidth); penalties AnchorWave's (negative); maximum_runtime_seconds
+ * > 0 arms the calling thread's deadline (aw_ksw_set_deadline) for the call;
+ * precomputed_optimal_scores (n values, or NULL) skips the score-only batch.  Returns AW_OK
+ * or a negative AW_E* code; out[i] is filled either way.
  */
 int aw_align_score_certified_batch(int n, const char *const *query, const int64_t *qlen,
                                    const char *const *reference, const int64_t *rlen,
-                                   int64_t initial_band_width, int64_t maximum_band_width,
+                                   const int64_t *initial_band_width, const int64_t *maximum_band_width,
                                    int32_t mismatching_penalty, int32_t open1, int32_t extend1, int32_t open2,
                                    int32_t extend2, double maximum_runtime_seconds,
                                    const int64_t *precomputed_optimal_scores, aw_certified_result_t *out);
@@ -176,15 +178,16 @@ typedef struct {
 /*
  * alignSlidingWindow (src/myImportandFunction/alignSlidingWindow.cpp:457-590), the
  * approximate-tier fallback called from the executor at :2683, for n intervals at once: an
- * interval with (rlen/W)*(qlen/W) <= 1 gets one global alignment; the others advance window
- * by window (W+1 bases of each sequence, semiglobal KSW2 ending at the better of the last row
- * and the last column), the k-th window of every interval still advancing in one batched
- * call; trailing gaps close the alignment, which is re-scored with the two-piece objective.
- * Sequences ASCII, penalties negative.  Returns AW_OK or a negative AW_E* code (an endpoint
- * the traceback does not reconstruct is AW_E_INVAL, the reference's runtime_error).
+ * interval with (rlen/W)*(qlen/W) <= 1 gets one global alignment (W = window[i], e.g. the
+ * selection plan's slidingWindowWidth); the others advance window by window (W+1 bases of
+ * each sequence, semiglobal KSW2 ending at the better of the last row and the last column),
+ * the k-th window of every interval still advancing in one batched call; trailing gaps close
+ * the alignment, which is re-scored with the two-piece objective.  Sequences ASCII,
+ * penalties negative.  Returns AW_OK or a negative AW_E* code (an endpoint the traceback
+ * does not reconstruct is AW_E_INVAL, the reference's runtime_error).
  */
 int aw_align_sliding_window_batch(int n, const char *const *query, const int64_t *qlen,
-                                  const char *const *reference, const int64_t *rlen, int64_t sliding_window_size,
+                                  const char *const *reference, const int64_t *rlen, const int64_t *window,
                                   int32_t matching_score, int32_t mismatching_penalty, int32_t open1,
                                   int32_t extend1, int32_t open2, int32_t extend2, aw_window_result_t *out);
 void aw_window_result_free(aw_window_result_t *result);
@@ -270,6 +273,19 @@ int64_t aw_sequence_summary_sketch_view(const uint64_t **hash, const uint32_t **
 #define AW_ROUTE_WFA_SINGLETRACK  3  /* gap-affine-2p WFA, Singletrack */
 #define AW_ROUTE_WFA_MEDIUM       4  /* gap-affine-2p WFA, medium memory (piggyback) */
 #define AW_ROUTE_WFA_LOW          5  /* gap-affine-2p WFA, low memory (piggyback) */
+#define AW_ROUTE_KSW2_CERTIFIED   6  /* score-certified KSW2 (aw_align_score_certified_batch) */
+#define AW_ROUTE_SLIDING_WINDOW   7  /* sliding-window semiglobal KSW2 (aw_align_sliding_window_batch) */
+
+/* A request's engine and its parameters, as the selection plan gives them
+ * (src/myImportandFunction/AlignmentAlgorithmSelector.h:196-242): band (KSW2 band width, -1
+ * = full; the initial band of score-certified KSW2), band_max (score-certified KSW2's largest
+ * band) and window (the sliding-window width). */
+typedef struct {
+    int method;
+    int band;
+    int band_max;
+    int64_t window;
+} aw_serve_route_t;
 
 typedef struct {
     int slots;            /* concurrent micro-batches (workers with their own streams) */
@@ -285,8 +301,12 @@ typedef struct {
 typedef struct {
     uint64_t id;
     int method;
-    int status;           /* 0 ok; WF status for WFA routes; AW_E* on failure */
-    ksw_extz_t ez;        /* KSW2 routes: ez.cigar malloc'd */
+    int status;           /* 0 ok; WF status for WFA routes; AW_E* on failure; for score-certified
+                             KSW2 the certification status (0 Completed, 1 TimeLimit,
+                             2 NotCertified, 3 Failed) */
+    ksw_extz_t ez;        /* KSW2 routes: ez.cigar malloc'd.  Score-certified and sliding-window
+                             routes: the rows as a CIGAR (M/I/D) and ez.score = their re-scored
+                             two-piece score (a failed certification: its best-effort rows) */
     int wfa_score;        /* WFA routes: -penalty */
     int n_ops;
     char *ops;            /* WFA routes: 'M','X','I','D' operations, malloc'd */
@@ -306,6 +326,10 @@ aw_server_t *aw_serve_open(const aw_serve_config_t *cfg);
 /* Enqueue one interval (ASCII sequences; ids consecutive from 0). Never blocks on the GPU. */
 int aw_serve_submit(aw_server_t *server, uint64_t id, int method, int band, const char *query,
                     int qlen, const char *target, int tlen);
+/* The same with every parameter of the route (required for AW_ROUTE_KSW2_CERTIFIED and
+ * AW_ROUTE_SLIDING_WINDOW; aw_serve_submit leaves band_max = -1 and window = 0). */
+int aw_serve_submit_route(aw_server_t *server, uint64_t id, const aw_serve_route_t *route, const char *query,
+                          int qlen, const char *target, int tlen);
 /* Up to max finished results, strictly in id order (waits up to wait_ms for the next one). */
 int aw_serve_poll(aw_server_t *server, aw_serve_result_t *out, int max, int wait_ms);
 int aw_serve_stats(aw_server_t *server, aw_serve_stats_t *stats);

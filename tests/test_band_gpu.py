@@ -165,3 +165,26 @@ def test_checkpointed_traceback(gpu, restatement, columns, flag):
     for q, t, w, r in zip(qs, ts, ws, res):
         o = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, w=w, flag=flag)
         assert r.key() == o.key(), (len(q), len(t), w)
+
+
+def test_singletrack_beyond_budget_refused_alone(gpu, restatement):
+    """A Singletrack pair whose two-track traceback exceeds the budget cannot be recomputed in
+    strip groups: it alone is reported as the reference's allocation failure (reset result,
+    zdropped = 1, no CIGAR); the other pairs of the batch are unaffected."""
+    qs, ts, ws = _pairs(7, 6, 300, 900, wfrac=(0.1, 0.3))
+    rng = np.random.default_rng(70)
+    big_t = W.random_dna(rng, 9000)
+    big_q = W.mutate(rng, big_t, 0.03, 0.005, 3.0)
+    qs.insert(2, big_q), ts.insert(2, big_t), ws.insert(2, 2000)
+    mat = oracle.anchorwave_matrix(-4)
+    try:
+        gpu.set_traceback_budget(4 << 20)  # the 9 kb pair needs ~40 MB of Singletrack traceback
+        res = gpu.ksw_extd2_batch(qs, ts, mat, 4, 2, 24, 1, w=ws, flag=ST)
+    finally:
+        gpu.set_traceback_budget(0)
+    big = res[2]
+    assert big.zdropped == 1 and big.n_cigar == 0 and big.score == oracle.KSW_NEG_INF
+    for i, (q, t, w, r) in enumerate(zip(qs, ts, ws, res)):
+        if i != 2:
+            assert r.key() == restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, w=w,
+                                                   flag=ST).key()

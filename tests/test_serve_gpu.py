@@ -105,3 +105,85 @@ def test_continuous_arrivals_and_small_budget(gpu):
     assert st["completed"] == len(reqs) and st["latency_p99_s"] >= st["latency_p50_s"] > 0
     for g, (rid, m, q, t, band) in list(zip(got, reqs))[::7]:
         assert (g.ksw if m in (0, 1) else g.wfa) == _standalone(gpu, wfa, m, q, t, band)
+
+
+def _rows_key(rows_q, rows_d, score):
+    """A rescue result as the server returns it: the rows as an M/I/D CIGAR and the score."""
+    cig, i, n = [], 0, len(rows_q)
+    while i < n:
+        op = 2 if rows_q[i] == "-" else 1 if rows_d[i] == "-" else 0
+        j = i + 1
+        while j < n and (2 if rows_q[j] == "-" else 1 if rows_d[j] == "-" else 0) == op:
+            j += 1
+        cig.append(((j - i) << 4) | op)
+        i = j
+    return score, tuple(cig)
+
+
+def _rescue_standalone(method, q, t, band, band_max, window):
+    from anchorwave_b200 import ksw2
+    pen = (-4, -4, -2, -24, -1)
+    if method == 6:
+        r = ksw2.align_score_certified_ksw2_batch([(q.decode(), t.decode())], band, band_max, *pen)[0]
+        status = {ksw2.CERT_COMPLETED: 0, ksw2.CERT_TIME_LIMIT: 1, ksw2.CERT_NOT_CERTIFIED: 2, ksw2.CERT_FAILED: 3}
+        rq, rd = ((r.alignment_q, r.alignment_d) if r.alignment_q else
+                  (r.best_effort_query_alignment, r.best_effort_reference_alignment))
+        return status[r.status], _rows_key(rq, rd, r.score)
+    s, rq, rd = ksw2.align_sliding_window_batch([(q.decode(), t.decode())], window, 0, *pen)[0]
+    return 0, _rows_key(rq, rd, s)
+
+
+def test_rescue_routes_alone_and_in_the_mix(gpu):
+    """Score-certified KSW2 and sliding-window requests (the selector's rescue outcomes) go
+    through the server beside the other engines; each result equals the standalone batch
+    entry's (status, rows as CIGAR, re-scored score)."""
+    from anchorwave_b200 import serve
+    rng = np.random.default_rng(41)
+    reqs = []
+    for i in range(36):
+        L = int(rng.integers(200, 2500))
+        q, t = W.divergent_pair(rng, L, 0.02, 0.12, 4.0)
+        if i % 4 == 0 and len(q) > 400:
+            at = int(rng.integers(0, len(q) - 300))
+            q = np.concatenate([q[:at], q[at + int(rng.integers(40, 250)):]])
+        method = [6, 7, 0, 6, 7, 2][i % 6]
+        band, band_max, window = (16, 600, 0) if method == 6 else (-1, -1, 300) if method == 7 else (-1, -1, 0)
+        reqs.append((i, method, W.to_ascii(q), W.to_ascii(t), band, band_max, window))
+    with serve.AlignmentServer(oracle.anchorwave_matrix(-4), *PEN, wfa_penalties=WPEN, slots=3,
+                               max_batch=5) as srv:
+        for rid, m, q, t, b, bm, w in reqs:
+            srv.submit(rid, m, q, t, band=b, band_max=bm, window=w)
+        got = _drain(srv, len(reqs))
+    assert [g.id for g in got] == list(range(len(reqs)))
+    for g, (rid, m, q, t, b, bm, w) in zip(got, reqs):
+        if m in (6, 7):
+            st, key = _rescue_standalone(m, q, t, b, bm, w)
+            assert g.status == st and (g.ksw[8], g.ksw[12]) == key, (rid, m)
+    assert {g.method for g in got} == {0, 2, 6, 7}
+
+
+def test_selector_routes_reproduced(gpu):
+    """Intervals routed by AnchorWave's own selector (the routing front end) are served with
+    exactly the chosen engine and parameters, and each result equals that engine's standalone
+    result."""
+    try:
+        from anchorwave_b200 import route
+    except ImportError as e:
+        pytest.skip(str(e))
+    from anchorwave_b200 import serve, wfa
+    reqs = W.serving_trace(48, seed=12, lmax=20_000)
+    routes = route.route_intervals([(r.query, r.target) for r in reqs])
+    with serve.AlignmentServer(oracle.anchorwave_matrix(-4), *PEN, wfa_penalties=WPEN, slots=2,
+                               max_batch=8) as srv:
+        for r, rt in zip(reqs, routes):
+            srv.submit(r.id, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max, window=rt.window)
+        got = _drain(srv, len(reqs))
+    assert [g.id for g in got] == [r.id for r in reqs]
+    for g, r, rt in zip(got, reqs, routes):
+        assert g.method == rt.method
+        if rt.method in (6, 7):
+            st, key = _rescue_standalone(rt.method, r.query, r.target, rt.band, rt.band_max, rt.window)
+            assert g.status == st and (g.ksw[8], g.ksw[12]) == key
+        else:
+            alone = _standalone(gpu, wfa, rt.method, r.query, r.target, rt.band)
+            assert (g.ksw if rt.method in (0, 1) else g.wfa) == alone, (r.id, rt)
