@@ -1,16 +1,23 @@
-"""Autotuner for the batched KSW2 path.
+"""Autotuner for the batched and served alignment paths.
 
-Two launch knobs decide how a batch maps onto the SMs (aw_set_tuning):
-  * large_warps: how many warps pipeline the strips of one large pair (1, 2, 4 or 8);
-  * large_tlen_threshold: the target length from which a pair counts as large.
-The tuner times a seeded sample of the caller's workload (same length distribution) under
-every candidate with CUDA events on the plan's stream, keeps the fastest, and installs it.
-Results are identical under every setting (tests/test_ksw2_gpu.py checks the knobs), so
-the choice only moves throughput.
+Knobs, each timed on a seeded sample of the caller's own workload (same length
+distribution), the fastest installed or returned:
+  * full-matrix strip kernel (aw_set_tuning): large_warps, how many warps pipeline the strips
+    of one large pair (2, 4 or 8), and large_tlen_threshold, the target length from which a
+    pair counts as large;
+  * banded strip kernel (aw_set_band_columns): target columns per lane (4: a shorter pipeline
+    lag between strips, for batches bound by their longest pair's chain; 8: less work per
+    cell, for batches bound by total work; 0 keeps the per-batch rule);
+  * serving loop: worker slots and the micro-batch size, chosen for the lowest p99 latency at
+    a fixed offered request rate among the settings that sustain it.
+Results are identical under every setting (tests/test_ksw2_gpu.py, tests/test_band_gpu.py and
+tests/test_autotune_gpu.py check the knobs), so the choice only moves throughput and latency.
 """
 from __future__ import annotations
 
 import itertools
+import threading
+import time
 from typing import Dict, List, Sequence, Tuple
 
 import numpy as np
@@ -19,14 +26,20 @@ from . import ksw2
 
 WARPS = (2, 4, 8)
 THRESHOLDS = (1024, 2048, 4096, 8192)
+BAND_COLUMNS = (4, 8)
+SERVE_SLOTS = (1, 2, 4)
+SERVE_BATCH = (256, 1024)
+
+
+def _sample(n: int, size: int, seed: int):
+    rng = np.random.default_rng(seed)
+    return rng.choice(n, size=min(size, n), replace=False) if n > size else np.arange(n)
 
 
 def tune(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray], mat, q, e, q2, e2, flag: int = 0,
          sample: int = 1024, reps: int = 2, seed: int = 0) -> Tuple[Tuple[int, int], List[Dict]]:
-    """Returns ((large_warps, threshold), trials) and installs the winner."""
-    n = len(queries)
-    rng = np.random.default_rng(seed)
-    idx = rng.choice(n, size=min(sample, n), replace=False) if n > sample else np.arange(n)
+    """Full-matrix kernel: returns ((large_warps, threshold), trials) and installs the winner."""
+    idx = _sample(len(queries), sample, seed)
     qs = [queries[i] for i in idx]
     ts = [targets[i] for i in idx]
     cells = sum(len(a) * len(b) for a, b in zip(qs, ts))
@@ -44,3 +57,70 @@ def tune(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray], mat, q, e
             best = (ms, warps, thr)
     ksw2.set_tuning(best[1], best[2])
     return (best[1], best[2]), trials
+
+
+def tune_band(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray], bands: Sequence[int], mat, q, e, q2,
+              e2, flag: int = 0, sample: int = 8, reps: int = 1, seed: int = 0) -> Tuple[int, List[Dict]]:
+    """Banded kernel: times the sample under 4 and 8 columns per lane and under the per-batch
+    rule (0); returns (columns, trials) and installs the winner."""
+    idx = _sample(len(queries), sample, seed)
+    qs = [queries[i] for i in idx]
+    ts = [targets[i] for i in idx]
+    ws = [int(bands[i]) for i in idx]
+    trials = []
+    best = None
+    for cols in (0,) + BAND_COLUMNS:
+        ksw2.set_band_columns(cols)
+        plan = ksw2.KswPlan(qs, ts, mat, q, e, q2, e2, w=ws, flag=flag)
+        plan.upload()
+        plan.execute()  # warm-up
+        ms = min(plan.execute() for _ in range(reps))
+        plan.close()
+        trials.append({"columns": cols, "ms": ms})
+        if best is None or ms < best[0]:
+            best = (ms, cols)
+    ksw2.release_thread_buffers()
+    ksw2.set_band_columns(best[1])
+    return best[1], trials
+
+
+def tune_serving(requests, routes, mat, q, e, q2, e2, rate: float, sample: int = 3000, hbm_budget: int = 0,
+                 seed: int = 0) -> Tuple[Tuple[int, int], List[Dict]]:
+    """Serving loop: every (slots, max_batch) serves a seeded sample of the routed trace with
+    Poisson arrivals at `rate` requests/s; the setting with the lowest p99 latency among those
+    that complete within 10% of the offered rate wins (else the highest throughput).
+    Returns ((slots, max_batch), trials)."""
+    from . import serve
+    idx = sorted(_sample(len(requests), sample, seed).tolist())
+    reqs = [requests[i] for i in idx]
+    rts = [routes[i] for i in idx]
+    trials = []
+    for slots, batch in itertools.product(SERVE_SLOTS, SERVE_BATCH):
+        rng = np.random.default_rng(seed + 1)
+        with serve.AlignmentServer(mat, q, e, q2, e2, slots=slots, max_batch=batch, hbm_budget=hbm_budget) as srv:
+            t0 = time.perf_counter()
+
+            def producer():
+                nxt = t0
+                for k, (r, rt) in enumerate(zip(reqs, rts)):
+                    nxt += rng.exponential(1.0 / rate)
+                    d = nxt - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    srv.submit(k, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max,
+                               window=rt.window)
+
+            th = threading.Thread(target=producer)
+            th.start()
+            got = 0
+            while got < len(reqs):
+                got += len(srv.poll(4096, wait_ms=20))
+            th.join()
+            dt = time.perf_counter() - t0
+            st = srv.stats()
+        trials.append({"slots": slots, "max_batch": batch, "requests_per_s": len(reqs) / dt,
+                       "p50_ms": 1e3 * st["latency_p50_s"], "p99_ms": 1e3 * st["latency_p99_s"]})
+    ksw2.release_thread_buffers()
+    keep = [t for t in trials if t["requests_per_s"] >= 0.9 * rate]
+    best = min(keep, key=lambda t: t["p99_ms"]) if keep else max(trials, key=lambda t: t["requests_per_s"])
+    return (best["slots"], best["max_batch"]), trials

@@ -878,7 +878,7 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             // columns; then the traceback is recomputed in groups of strips, from the last group
             // to the first, each from the stored column on its left, and the walk continues
             // through each group as it is recomputed.  The groups are cut per wave (below).
-            for (int s = 0; s < (int)G.strips.size(); ++s) refuse |= G.stb[s] > tb_budget / 2;
+            for (int s = 0; s < (int)G.strips.size(); ++s) refuse |= G.stb[s] > tb_budget;
             if (!refuse) {
                 G.ckpt = true;
                 G.tb = 0;  // the first pass stores no traceback

@@ -187,6 +187,74 @@ struct OpsWriter {
     }
 };
 
+// Extends four diagonals of one lane at once (wavefront/wavefront_extend.c:86-121): o[u] is the
+// offset on diagonal k0 + 32u (WF_NULL: nothing to extend) and becomes the offset after the run
+// of equal bases.  2-bit words (32 bases per XOR) for ACGT-only pairs; otherwise 8 bytes per
+// XOR up to the sentinels after each sequence.  The four loads of a round are in flight
+// together.
+__device__ __forceinline__ void extend4(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
+                                        const uint8_t *txt, int k0, int32_t (&o)[4]) {
+    const int plen = PR.plen, tlen = PR.tlen;
+    int64_t v[4], h[4];
+    bool run[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int k = k0 + 32 * u;
+        run[u] = o[u] != WF_NULL;
+        v[u] = (int64_t)o[u] - k, h[u] = o[u];
+    }
+    bool any = run[0] || run[1] || run[2] || run[3];
+    if (PR.packed) {
+        // 32 bases per XOR; the run ends at the first differing base or at the end of either
+        // sequence (the sentinels of the byte path)
+        int64_t rem[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            rem[u] = run[u] ? min((int64_t)plen - v[u], (int64_t)tlen - h[u]) : 0;
+            if (rem[u] <= 0) run[u] = false;
+        }
+        any = run[0] || run[1] || run[2] || run[3];
+        while (any) {
+            uint64_t x[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                x[u] = run[u] ? (load32b(A.ppat, PR.poff + v[u]) ^ load32b(A.ptxt, PR.toff + h[u])) : 0;
+            any = false;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (!run[u]) continue;
+                int64_t nb = x[u] ? (int64_t)((__ffsll((long long)x[u]) - 1) >> 1) : 32;
+                const bool stop = x[u] != 0 || nb >= rem[u];
+                if (nb > rem[u]) nb = rem[u];
+                v[u] += nb, h[u] += nb, rem[u] -= nb;
+                if (stop || rem[u] == 0) run[u] = false;
+                else any = true;
+            }
+        }
+    }
+    while (any) {
+        uint64_t x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = run[u] ? (load8(pat, v[u]) ^ load8(txt, h[u])) : 0;
+        any = false;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (!run[u]) continue;
+            if (x[u]) {
+                const int nb = (__ffsll((long long)x[u]) - 1) >> 3;
+                v[u] += nb, h[u] += nb;
+                run[u] = false;
+            } else {
+                v[u] += 8, h[u] += 8;
+                any = true;
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (o[u] != WF_NULL) o[u] = (int32_t)h[u];
+}
+
 template <bool PIG>
 __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
     const int lane = threadIdx.x & 31;
@@ -250,80 +318,35 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         __syncwarp();
         const int k_end = tlen - plen;
         int s = 0, num_null = 0;
+        bool fused_reached = false;  // the compute step's extension reached the end (this lane)
         const int smax = PR.ctab_cap * HDR_CHUNK - 1;
         while (status == 0) {
-            // ---- extend M[s] and check the end
+            // ---- extend M[s] and check the end.  Outside the piggyback modes the compute step
+            // below extends M[s] as it computes it (fused), so here only M[0] is extended.
             {
                 const CompHdr m = HR.get(A, ctab, s, s)->c[CM];
                 bool reached = false;
                 if (m.lo <= m.hi) {
-                    int32_t *d = (int32_t *)(A.pool + m.off);
-                    // four diagonals per lane at a time, so their loads overlap
-                    for (int k0 = m.lo + lane; k0 <= m.hi; k0 += 128) {
-                        int32_t o[4];
-                        int64_t v[4], h[4];
-                        bool run[4];
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int k = k0 + 32 * u;
-                            o[u] = k <= m.hi ? d[k - m.base] : WF_NULL;
-                            run[u] = o[u] != WF_NULL;
-                            v[u] = (int64_t)o[u] - k, h[u] = o[u];
-                        }
-                        bool any = run[0] || run[1] || run[2] || run[3];
-                        if (PR.packed) {
-                            // 32 bases per XOR; the run ends at the first differing base or
-                            // at the end of either sequence (the sentinels of the byte path)
-                            int64_t rem[4];
+                    if (PIG || s == 0) {
+                        int32_t *d = (int32_t *)(A.pool + m.off);
+                        for (int k0 = m.lo + lane; k0 <= m.hi; k0 += 128) {
+                            int32_t o[4];
 #pragma unroll
                             for (int u = 0; u < 4; ++u) {
-                                rem[u] = run[u] ? min((int64_t)plen - v[u], (int64_t)tlen - h[u]) : 0;
-                                if (rem[u] <= 0) run[u] = false;
+                                const int k = k0 + 32 * u;
+                                o[u] = k <= m.hi ? d[k - m.base] : WF_NULL;
                             }
-                            any = run[0] || run[1] || run[2] || run[3];
-                            while (any) {
-                                uint64_t x[4];
-#pragma unroll
-                                for (int u = 0; u < 4; ++u)
-                                    x[u] = run[u] ? (load32b(A.ppat, PR.poff + v[u]) ^ load32b(A.ptxt, PR.toff + h[u])) : 0;
-                                any = false;
-#pragma unroll
-                                for (int u = 0; u < 4; ++u) {
-                                    if (!run[u]) continue;
-                                    int64_t nb = x[u] ? (int64_t)((__ffsll((long long)x[u]) - 1) >> 1) : 32;
-                                    const bool stop = x[u] != 0 || nb >= rem[u];
-                                    if (nb > rem[u]) nb = rem[u];
-                                    v[u] += nb, h[u] += nb, rem[u] -= nb;
-                                    if (stop || rem[u] == 0) run[u] = false;
-                                    else any = true;
-                                }
-                            }
-                        }
-                        while (any) {
-                            uint64_t x[4];
-#pragma unroll
-                            for (int u = 0; u < 4; ++u) x[u] = run[u] ? (load8(pat, v[u]) ^ load8(txt, h[u])) : 0;
-                            any = false;
+                            extend4(A, PR, pat, txt, k0, o);
 #pragma unroll
                             for (int u = 0; u < 4; ++u) {
-                                if (!run[u]) continue;
-                                if (x[u]) {
-                                    const int nb = (__ffsll((long long)x[u]) - 1) >> 3;
-                                    v[u] += nb, h[u] += nb;
-                                    run[u] = false;
-                                } else {
-                                    v[u] += 8, h[u] += 8;
-                                    any = true;
-                                }
+                                const int k = k0 + 32 * u;
+                                if (k <= m.hi && o[u] != WF_NULL) d[k - m.base] = o[u];
+                                // end-to-end check on the lane that holds diagonal tlen-plen
+                                if (k == k_end && o[u] != WF_NULL && o[u] >= tlen) reached = true;
                             }
                         }
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int k = k0 + 32 * u;
-                            if (k <= m.hi && o[u] != WF_NULL) d[k - m.base] = (int32_t)h[u];
-                            // end-to-end check on the lane that holds diagonal tlen-plen
-                            if (k == k_end && o[u] != WF_NULL && h[u] >= tlen) reached = true;
-                        }
+                    } else {
+                        reached = fused_reached;
                     }
                     if (__any_sync(0xffffffffu, reached)) {
                         end_score = s;
@@ -370,9 +393,11 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                 }
                 __syncwarp();
                 ++num_null;
+                fused_reached = false;
                 continue;
             }
             num_null = 0;
+            fused_reached = false;
             // limits (null inputs contribute lo=1, hi=-1)
             int lo = m_misms.lo, hi = m_misms.hi;
             lo = min(lo, m_open1.lo - 1), hi = max(hi, m_open1.hi + 1);
@@ -526,12 +551,22 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                         del2[u] = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
                         misms[u] = getv(A, m_misms, k) + 1;
                     }
+                    // M[s] of these diagonals, then its extension (the extend step of the next
+                    // iteration, fused: the offsets never round-trip through memory unextended)
+                    int32_t mo[4];
+    #pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + 32 * u;
+                        const int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
+                        mo[u] = (k <= hi && in_matrix(best, k, plen, tlen)) ? best : WF_NULL;
+                    }
+                    extend4(A, PR, pat, txt, k0, mo);
     #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int k = k0 + 32 * u;
                         if (k > hi) break;
-                        int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
-                        if (!in_matrix(best, k, plen, tlen)) best = WF_NULL;
+                        const int32_t best = mo[u];
+                        if (k == k_end && best != WF_NULL && best >= tlen) fused_reached = true;
                         oM[k - lo] = best;
                         if (oI1) oI1[k - lo] = ins1[u];
                         if (oD1) oD1[k - lo] = del1[u];

@@ -26,6 +26,16 @@ KSW2_ROUTES = (ROUTE_KSW2, ROUTE_KSW2_SINGLETRACK, ROUTE_KSW2_CERTIFIED, ROUTE_S
 
 
 @dataclass
+class ServeRouteSpec:
+    """A request's engine and parameters (aw_serve_route_t), as the routing front end returns
+    them (anchorwave_b200.route.Route has the same fields)."""
+    method: int
+    band: int = -1
+    band_max: int = -1
+    window: int = 0
+
+
+@dataclass
 class ServedAlignment:
     id: int
     method: int

@@ -310,7 +310,7 @@ def plain_route_call(rt, q: bytes, t: bytes, mat, aligners):
     return ksw2.align_sliding_window(q.decode(), t.decode(), rt.window, 0, *pen)[0]
 
 
-def serving_measurement(nreq: int, rank: int, plain_sample: int = 400):
+def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 400):
     """Serving trace (lengths log-normal, median 2 kb, sigma 1, clipped to 50 bp-500 kb;
     divergence and indels as the batched workload; 10% with repeat structure).  Every request
     is routed by AnchorWave's own selector (the routing front end: makeAlignmentSelectionPlan
@@ -338,10 +338,12 @@ def serving_measurement(nreq: int, rank: int, plain_sample: int = 400):
     cells = sum(len(r.query) * len(r.target) for r in reqs)
     mat = ksw2.anchorwave_matrix(-4)
 
+    cfg = {"slots": SERVE_SLOTS, "max_batch": SERVE_BATCH}
+
     def run(rate, keep=None):
         rng = np.random.default_rng(99)
         kept = {}
-        with serve.AlignmentServer(mat, 4, 2, 24, 1, slots=SERVE_SLOTS, max_batch=SERVE_BATCH,
+        with serve.AlignmentServer(mat, 4, 2, 24, 1, slots=cfg["slots"], max_batch=cfg["max_batch"],
                                    hbm_budget=SERVE_HBM_BUDGET) as srv:
             t0 = time.perf_counter()
 
@@ -373,6 +375,18 @@ def serving_measurement(nreq: int, rank: int, plain_sample: int = 400):
 
     rng = np.random.default_rng(2024)
     sample = sorted(rng.choice(len(reqs), size=min(plain_sample, len(reqs)), replace=False).tolist())
+    # the autotuner picks the worker slots and the micro-batch size for the lowest p99 at 80% of
+    # the saturated rate of the default setting, on a 3,000-request sample of the trace
+    from anchorwave_b200 import autotune
+    dt0, _, _ = run(None)
+    t_tune = time.perf_counter()
+    (cfg["slots"], cfg["max_batch"]), trials = autotune.tune_serving(
+        reqs, routes, mat, 4, 2, 24, 1, rate=SERVE_LOAD * len(reqs) / dt0, sample=3000, hbm_budget=SERVE_HBM_BUDGET)
+    if tuning is not None:
+        tuning["serving"] = {"slots": cfg["slots"], "max_batch": cfg["max_batch"], "sample_requests": 3000,
+                             "seconds": time.perf_counter() - t_tune,
+                             "trials": [{k: (round(v, 1) if isinstance(v, float) else v) for k, v in t.items()}
+                                        for t in trials]}
     dt_sat, st_sat, served = run(None, keep=set(sample))
     sat = len(reqs) / dt_sat
     dt, st, _ = run(SERVE_LOAD * sat)
@@ -404,7 +418,7 @@ def serving_measurement(nreq: int, rank: int, plain_sample: int = 400):
             "offered_requests_per_s": SERVE_LOAD * sat, "load": SERVE_LOAD,
             "requests_per_s": len(reqs) / dt, "gcups": cells / dt / 1e9,
             "latency_ms_p50": 1e3 * st["latency_p50_s"], "latency_ms_p99": 1e3 * st["latency_p99_s"],
-            "micro_batches": st["micro_batches"], "slots": SERVE_SLOTS, "max_batch": SERVE_BATCH,
+            "micro_batches": st["micro_batches"], "slots": cfg["slots"], "max_batch": cfg["max_batch"],
             "hbm_budget": SERVE_HBM_BUDGET,
             "plain_per_call": {"sample": len(sample), "requests_per_s": plain_pps,
                                "served_vs_plain": sat / plain_pps, "results_identical_to_served": bool(same)},
@@ -541,7 +555,7 @@ def cigar_check(res, q, t, mis=4, o1=4, e1=2, o2=24, e2=1):
 
 
 def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 100_000, lmax: int = 1_000_000,
-                            long_max: int = 50_000):
+                            long_max: int = 50_000, tuning=None):
     """The long-interval banded and Singletrack workload (target length U(lmin, lmax), 30% of
     the query replaced by repeat structure, 3% substitutions, 5-20 long indels of U(1,
     long_max), w = 10% of the shorter length): one execution of the whole set per traceback,
@@ -567,6 +581,18 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
     warm.upload()
     warm.execute()
     warm.close()
+    # the autotuner picks the banded kernel's columns per lane (4, 8, or the per-batch rule) on
+    # the four smallest pairs of this workload that reach the end of the band, score-only (the DP
+    # pass the setting affects)
+    from anchorwave_b200 import autotune
+    t_tune = time.perf_counter()
+    reachable = sorted((i for i in range(len(ps)) if reach[i]), key=lambda i: pair_cells[i])
+    pick = reachable[:4]
+    cols, trials = autotune.tune_band([ps.queries[i] for i in pick], [ps.targets[i] for i in pick],
+                                      [ps.band[i] for i in pick], mat, 4, 2, 24, 1, flag=0x01, sample=4, reps=1)
+    if tuning is not None:
+        tuning["band_kernel"] = {"columns_per_lane": cols, "trials_ms": {str(t["columns"]): t["ms"] for t in trials},
+                                 "seconds": time.perf_counter() - t_tune, "sample_pairs": len(pick)}
     results = {}
     for name, flag in (("banded", 0), ("singletrack", 0x1000)):
         plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1, w=ps.band, flag=flag)
@@ -595,6 +621,7 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
                      # score (the reference re-scores for that reason, alignSlidingWindow.cpp:872-876)
                      "cigars_rescoring_to_score": rescored}
         ksw2.release_thread_buffers()
+    ksw2.set_band_columns(0)
     if cpu:
         from concurrent.futures import ThreadPoolExecutor
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -727,6 +754,13 @@ def main():
     cells = ps.cells()
     n = len(ps)
 
+    # the autotuner picks the strip kernel's warps per large pair and the large-pair threshold
+    # on a seeded 1,024-pair sample of this workload, before anything is timed
+    from anchorwave_b200 import autotune
+    t_tune = time.perf_counter()
+    (tuned_warps, tuned_thr), _ = autotune.tune(ps.queries, ps.targets, mat, 4, 2, 24, 1, sample=1024, reps=1)
+    tuning = {"full_kernel": {"large_warps": tuned_warps, "large_tlen_threshold": tuned_thr,
+                              "seconds": time.perf_counter() - t_tune, "sample_pairs": min(1024, n)}}
     plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1)
     plan.upload()
     st = plan.stats()
@@ -800,9 +834,10 @@ def main():
     # the batch calls above keep ~100 GB of traceback arena pooled on this thread; give it
     # back before the other workloads size their own device pools
     ksw2.release_thread_buffers()
-    serving = serving_measurement(args.serve_requests, rank) if args.serve_requests > 0 else None
+    serving = serving_measurement(args.serve_requests, rank, tuning) if args.serve_requests > 0 else None
     long_banded = None if args.no_long_banded else long_banded_measurement(
-        rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max, args.long_banded_indel)
+        rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max, args.long_banded_indel,
+        tuning)
     wfa_res = (wfa_measurement(args.wfa_pairs, rank, cpu_on, args.wfa_pool_gb) if args.wfa_pairs > 0 else None)
     summary_res = (None if args.no_selector_summary else selector_summary_measurement(ps, rank, cpu_on))
 
@@ -823,6 +858,7 @@ def main():
         "pairs_per_s": pairs_per_s,
         "config": run_config(ps, world),
         "plan": {"waves": st["waves"], "traceback_bytes": st["tb_bytes"]},
+        "tuning": tuning,
         "latency_ms": {"batch_step_p50": float(np.percentile(step_ms, 50)),
                        "batch_step_p99": float(np.percentile(step_ms, 99)),
                        "serving_p50": serving["latency_ms_p50"] if serving else None,
@@ -923,6 +959,10 @@ def compact_summary(line):
     if ss:
         out["selector_pass"] = {"bases_per_s": ss.get("e2e_bases_per_s"), "vs_ref": ss.get("vs_cpu_reference")}
         par["selector_pass"] = get(ss, "cpu_reference", "summaries_identical")
+    tn = line.get("tuning") or {}
+    out["tuning"] = {"full": [get(tn, "full_kernel", "large_warps"), get(tn, "full_kernel", "large_tlen_threshold")],
+                     "band_columns": get(tn, "band_kernel", "columns_per_lane"),
+                     "serve": [get(tn, "serving", "slots"), get(tn, "serving", "max_batch")]}
     out["parity"] = par
     return sig(out)
 
