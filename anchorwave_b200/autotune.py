@@ -108,7 +108,7 @@ def tune_serving(requests, routes, mat, q, e, q2, e2, rate: float, sample: int =
                     if d > 0:
                         time.sleep(d)
                     srv.submit(k, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max,
-                               window=rt.window)
+                               window=rt.window, predicted_bytes=rt.predicted_bytes)
 
             th = threading.Thread(target=producer)
             th.start()
@@ -119,7 +119,8 @@ def tune_serving(requests, routes, mat, q, e, q2, e2, rate: float, sample: int =
             dt = time.perf_counter() - t0
             st = srv.stats()
         trials.append({"slots": slots, "max_batch": batch, "requests_per_s": len(reqs) / dt,
-                       "p50_ms": 1e3 * st["latency_p50_s"], "p99_ms": 1e3 * st["latency_p99_s"]})
+                       "p50_ms": 1e3 * st["latency_p50_s"], "p99_ms": 1e3 * st["latency_p99_s"],
+                       "seconds": dt})
     ksw2.release_thread_buffers()
     keep = [t for t in trials if t["requests_per_s"] >= 0.9 * rate]
     best = min(keep, key=lambda t: t["p99_ms"]) if keep else max(trials, key=lambda t: t["requests_per_s"])

@@ -18,6 +18,7 @@
 #include "../../include/anchorwave_b200.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cstdio>
@@ -66,6 +67,9 @@ static cudaError_t record_timing(cudaEvent_t e, cudaStream_t st) {
 static int64_t g_tb_budget = 0;           // 0 = 60% of free memory
 static thread_local int64_t tls_tb_budget = 0;  // per-thread override (serving workers)
 static thread_local bool tls_all_large = false;  // single-pair calls: every pair gets a warp group
+// full-matrix pairs on the critical path go to the banded kernel at full width
+// (aw_set_full_pair_routing)
+static std::atomic<bool> g_band_full_pairs{true};
 static int g_large_warps = 8;
 static int g_large_tlen = 4096;
 static int g_band_nc = 0;  // banded kernel columns per lane: 0 = chosen per plan, 4 or 8
@@ -396,6 +400,27 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
         pl->cells += (int64_t)ql * tl;
     }
     pl->qbytes = qb, pl->tbytes = tbt, pl->cig_words = cw;
+    // A full-matrix pair that would be the batch's critical path goes to the banded strip
+    // kernel at full width instead (w >= max(qlen, tlen) is the reference's full mode, so the
+    // results are the same): the strip kernel pipelines one pair's strips over a group of
+    // 8 warps of one CTA, ceil(strips / 8) sweeps of its rows, while the banded kernel
+    // pipelines them across CTAs, one strip per warp.  Estimates (seconds): strip-kernel
+    // chain ceil(ceil(tlen/512)/8) * (qlen + 600) * 0.35e-6 against the batch's work at
+    // 1e12 cells/s, and the banded kernel's chain (tlen/256 strips * 64 lane-steps * 2e-6, plus
+    // the rows) and the pair's work at 2e11 cells/s.
+    if (g_band_full_pairs.load()) {
+        double work = 0.0;
+        for (int i = 0; i < n; ++i)
+            if (pl->route[i] == 1) work += (double)pl->qlen[i] * pl->tlen[i];
+        const double batch_s = work / 1e12;
+        for (int i = 0; i < n; ++i) {
+            if (pl->route[i] != 1 || !band_path_ok(P, pl->qlen[i], pl->tlen[i])) continue;
+            const double ql = pl->qlen[i], tl = pl->tlen[i];
+            const double k1 = std::ceil(std::ceil(tl / KSW_STRIP) / 8.0) * (ql + 600.0) * 0.35e-6;
+            const double k2 = std::ceil(tl / 256.0) * 64.0 * 2e-6 + ql * 0.3e-6 + ql * tl / 2e11;
+            if (k1 > 1.5 * std::max(batch_s, k2)) pl->route[i] = 3;
+        }
+    }
     // strip-kernel pairs: largest first, packed into traceback waves
     std::vector<int32_t> strip;
     for (int i = 0; i < n; ++i)
@@ -824,6 +849,8 @@ void aw_ksw_set_deadline(double seconds) {
 }
 
 void aw_ksw_set_stop_antidiagonal(int interval, int antidiagonal) { set_exact_stop(interval, antidiagonal); }
+
+void aw_set_full_pair_routing(int enabled) { g_band_full_pairs.store(enabled != 0); }
 
 void aw_set_band_columns(int columns) {
     std::lock_guard<std::mutex> lk(g_cfg_mu);

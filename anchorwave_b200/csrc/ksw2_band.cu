@@ -859,12 +859,6 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             G.start.push_back(T);
         }
         G.tb = (G.tb + 255) / 256 * 256;
-        const int64_t bnd_bytes = band_bnd_bytes(G.bnd);
-        // Singletrack pairs keep their whole two-track traceback: the reconstruction probes
-        // arbitrarily far left in one gap search, so it cannot be split into strip groups.  A
-        // pair whose traceback and boundary columns exceed the budget is refused like an
-        // allocation failure of the reference (ksw2_extd2_avx.c:206-210: reset result,
-        // zdropped = 1).
         if (G.rb < nd) {
             // the band becomes empty before the end: the reference stops there with
             // zdropped = 1 and no traceback (ksw2_extd2_sse.c:151-154), so the DP runs without
@@ -872,13 +866,30 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             G.ckpt = G.notb = true;
             G.tb = 0;
         }
-        bool refuse = st && G.tb + bnd_bytes > tb_budget;
-        if (!st && G.tb + bnd_bytes > tb_budget) {
+    }
+    // The budget is split once between the boundary-column arena and the traceback arena
+    // (both are sized for their largest wave): the boundary columns get what the whole batch
+    // needs, up to a third of the budget; the traceback arena the rest.  A wave's boundary
+    // columns and its tracebacks stored in full must fit their arenas; the recompute rounds of
+    // its recomputed pairs use the whole traceback arena after the wave's other walks.
+    int64_t bnd_all = 0;
+    for (const PairGeo &G : geo) bnd_all += band_bnd_bytes(G.bnd);
+    const int64_t cap_bnd = std::min(bnd_all, tb_budget / 3);
+    const int64_t cap_tb = std::max<int64_t>(tb_budget - cap_bnd, 1);
+    const int64_t gres = cap_tb;
+    for (PairGeo &G : geo) {
+        if (G.notb) continue;
+        // Singletrack pairs keep their whole two-track traceback: the reconstruction probes
+        // arbitrarily far left in one gap search, so it cannot be split into strip groups.  A
+        // pair whose traceback does not fit is refused like an allocation failure of the
+        // reference (ksw2_extd2_avx.c:206-210: reset result, zdropped = 1).
+        bool refuse = st && G.tb > cap_tb;
+        if (!st && G.tb > cap_tb) {
             // Traceback beyond the budget: the first pass stores only the strips' boundary
             // columns; then the traceback is recomputed in groups of strips, from the last group
             // to the first, each from the stored column on its left, and the walk continues
             // through each group as it is recomputed.  The groups are cut per wave (below).
-            for (int s = 0; s < (int)G.strips.size(); ++s) refuse |= G.stb[s] > tb_budget;
+            for (int s = 0; s < (int)G.strips.size(); ++s) refuse |= G.stb[s] > cap_tb;
             if (!refuse) {
                 G.ckpt = true;
                 G.tb = 0;  // the first pass stores no traceback
@@ -888,17 +899,15 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
             if (!refused) return AW_E_NOMEM_INTERNAL;
             G.refused = true;
             refused->push_back(G.id);
-            continue;
         }
-        bp.tb_total += G.tb;
-        bp.cells += band_cells(ql, tl, ww);
     }
-    // Pairs largest first into the fewest waves under the budget (LPT multiway fit).  A wave
-    // holds its pairs' boundary columns throughout; its traceback arena serves first the pairs
-    // stored in full, then (after their walks) the recompute rounds of its recomputed pairs,
-    // which take half of the budget: bnd + max(tb, half the budget if any pair is recomputed)
-    // <= budget, or one pair alone.
-    const int64_t gres = tb_budget / 2;
+    for (const PairGeo &G : geo) {
+        if (G.refused) continue;
+        bp.tb_total += G.tb;
+        bp.cells += band_cells(qlen[G.id], tlen[G.id], G.ww);
+    }
+    // Pairs largest first into the fewest waves whose boundary columns and tracebacks stored in
+    // full fit their arenas (LPT multiway fit), or one pair alone.
     std::vector<size_t> ord;
     for (size_t a = 0; a < ids.size(); ++a)
         if (!geo[a].refused) ord.push_back(a);
@@ -908,23 +917,21 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
     });
     std::vector<std::vector<size_t>> wv;
     std::vector<int64_t> wtb, wbnd;
-    std::vector<char> wck;
-    auto foot = [&](int64_t tb, int64_t bnd, bool ck) { return bnd + std::max(tb, ck ? gres : (int64_t)0); };
     for (size_t a : ord) {
         const PairGeo &G = geo[a];
         const int64_t pb = band_bnd_bytes(G.bnd);
         int best = -1;
         for (size_t k = 0; k < wv.size(); ++k) {
-            const int64_t f = foot(wtb[k] + G.tb, wbnd[k] + pb, wck[k] || (G.ckpt && !G.notb));
-            if (f <= tb_budget && (best < 0 || foot(wtb[k], wbnd[k], wck[k]) < foot(wtb[best], wbnd[best], wck[best])))
+            if (wtb[k] + G.tb <= cap_tb && wbnd[k] + pb <= cap_bnd &&
+                (best < 0 || wbnd[k] * cap_tb + wtb[k] * cap_bnd < wbnd[best] * cap_tb + wtb[best] * cap_bnd))
                 best = (int)k;
         }
         if (best < 0) {
             wv.emplace_back();
-            wtb.push_back(0), wbnd.push_back(0), wck.push_back(0);
+            wtb.push_back(0), wbnd.push_back(0);
             best = (int)wv.size() - 1;
         }
-        wtb[best] += G.tb, wbnd[best] += pb, wck[best] |= (G.ckpt && !G.notb);
+        wtb[best] += G.tb, wbnd[best] += pb;
         wv[best].push_back(a);
     }
     struct U {

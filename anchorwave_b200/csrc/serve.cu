@@ -132,6 +132,19 @@ struct aw_server {
 
 namespace {
 
+// Device memory of one worker: its share of the budget, split between the KSW2 traceback
+// arena (50%, reserved when the worker starts) and the wavefront pools of the four WFA
+// engines (allocated when an engine first runs; high memory 16%, Singletrack 26% -- the
+// engine AnchorWave's selector picks most, for intervals up to tens of kb -- medium and low
+// 4% each as they keep a ring and packed-CIGAR blocks), so that the pooled allocations of
+// all workers stay inside the budget whatever mix of engines each worker sees.
+int64_t worker_share(const aw_server *S) { return S->cfg.hbm_budget / std::max(1, S->cfg.slots); }
+int64_t ksw_tb_share(const aw_server *S) { return worker_share(S) * 5 / 10; }
+int64_t wfa_pool_share(const aw_server *S, int method) {
+    const int pct = method == AW_ROUTE_WFA ? 16 : method == AW_ROUTE_WFA_SINGLETRACK ? 26 : 4;
+    return worker_share(S) * pct / 100;
+}
+
 // Pops one micro-batch: the requests of the class whose head waited longest, oldest
 // first, while they fit the batch size and the budget.
 bool take_batch(aw_server *S, std::vector<Req> &batch) {
@@ -142,9 +155,14 @@ bool take_batch(aw_server *S, std::vector<Req> &batch) {
         if (!kv.second.empty() && (!q || kv.second.front().id < q->front().id)) q = &kv.second;
     const int64_t budget = S->cfg.hbm_budget;
     if (S->inflight_bytes > 0 && S->inflight_bytes + q->front().pred > budget) return false;
+    // a WFA micro-batch shares one wavefront pool: its predicted bytes stay within that pool,
+    // so that large alignments are not started together only to exhaust it and retry
+    const int method = q->front().method;
+    const int64_t pool = method >= AW_ROUTE_WFA && method <= AW_ROUTE_WFA_LOW ? wfa_pool_share(S, method) : INT64_MAX;
     int64_t bytes = 0;
     while (!q->empty() && (int)batch.size() < S->cfg.max_batch) {
         if (!batch.empty() && S->inflight_bytes + bytes + q->front().pred > budget) break;
+        if (!batch.empty() && bytes + q->front().pred > pool) break;
         bytes += q->front().pred;
         batch.push_back(std::move(q->front()));
         q->pop_front();
@@ -154,18 +172,6 @@ bool take_batch(aw_server *S, std::vector<Req> &batch) {
     return true;
 }
 
-// Device memory of one worker: its share of the budget, split between the KSW2 traceback
-// arena (60%, reserved when the worker starts) and the wavefront pools of the four WFA
-// engines (allocated when an engine first runs; high memory 20%, Singletrack 12% as it
-// keeps M only, medium and low 4% each as they keep a ring and packed-CIGAR blocks), so
-// that the pooled allocations of all workers stay inside the budget whatever mix of
-// engines each worker sees.
-int64_t worker_share(const aw_server *S) { return S->cfg.hbm_budget / std::max(1, S->cfg.slots); }
-int64_t ksw_tb_share(const aw_server *S) { return worker_share(S) * 6 / 10; }
-int64_t wfa_pool_share(const aw_server *S, int method) {
-    const int pct = method == AW_ROUTE_WFA ? 20 : method == AW_ROUTE_WFA_SINGLETRACK ? 12 : 4;
-    return worker_share(S) * pct / 100;
-}
 
 // Gapped rows -> a KSW2-style CIGAR (M/I/D runs), malloc'd into ez.
 void rows_to_cigar(const char *q, const char *d, int64_t n, ksw_extz_t &ez) {
@@ -372,7 +378,7 @@ aw_server_t *aw_serve_open(const aw_serve_config_t *cfg) {
 int aw_serve_submit(aw_server_t *S, uint64_t id, int method, int band, const char *query, int qlen,
                     const char *target, int tlen) {
     aw_serve_route_t rt;
-    rt.method = method, rt.band = band, rt.band_max = -1, rt.window = 0;
+    rt.method = method, rt.band = band, rt.band_max = -1, rt.window = 0, rt.predicted_bytes = 0;
     return aw_serve_submit_route(S, id, &rt, query, qlen, target, tlen);
 }
 
@@ -391,6 +397,10 @@ int aw_serve_submit_route(aw_server_t *S, uint64_t id, const aw_serve_route_t *r
     r.q.assign(query ? query : "", (size_t)qlen);
     r.t.assign(target ? target : "", (size_t)tlen);
     r.pred = predict_bytes(r);
+    // the selector's memory estimate of a WFA alignment (its score model) replaces the
+    // length-based proxy; KSW2 tracebacks are sized exactly by the server itself
+    if (method >= AW_ROUTE_WFA && method <= AW_ROUTE_WFA_LOW && route->predicted_bytes > 0)
+        r.pred = route->predicted_bytes;
     r.generic = 0;
     if (method <= AW_ROUTE_KSW2_SINGLETRACK) {
         std::vector<uint8_t> tmp;

@@ -33,6 +33,8 @@
 #include "aw_internal.h"
 #include "wfa_internal.h"
 
+#include <cooperative_groups.h>
+
 namespace aw {
 namespace {
 
@@ -187,41 +189,49 @@ struct OpsWriter {
     }
 };
 
-// Extends four diagonals of one lane at once (wavefront/wavefront_extend.c:86-121): o[u] is the
-// offset on diagonal k0 + 32u (WF_NULL: nothing to extend) and becomes the offset after the run
+// Extends N diagonals of one lane at once (wavefront/wavefront_extend.c:86-121): o[u] is the
+// offset on diagonal k0 + stride*u (WF_NULL: nothing to extend) and becomes the offset after the run
 // of equal bases.  2-bit words (32 bases per XOR) for ACGT-only pairs; otherwise 8 bytes per
-// XOR up to the sentinels after each sequence.  The four loads of a round are in flight
-// together.
-__device__ __forceinline__ void extend4(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
-                                        const uint8_t *txt, int k0, int32_t (&o)[4]) {
-    const int plen = PR.plen, tlen = PR.tlen;
-    int64_t v[4], h[4];
-    bool run[4];
+// XOR up to the sentinels after each sequence.  The N loads of a round are in flight together.
+template <int N>
+__device__ __forceinline__ bool any_of(const bool (&r)[N]) {
+    bool a = false;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int k = k0 + 32 * u;
+    for (int u = 0; u < N; ++u) a |= r[u];
+    return a;
+}
+
+template <int N>
+__device__ __forceinline__ void extend_n(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
+                                         const uint8_t *txt, int k0, int stride, int32_t (&o)[N]) {
+    const int plen = PR.plen, tlen = PR.tlen;
+    int64_t v[N], h[N];
+    bool run[N];
+#pragma unroll
+    for (int u = 0; u < N; ++u) {
+        const int k = k0 + stride * u;
         run[u] = o[u] != WF_NULL;
         v[u] = (int64_t)o[u] - k, h[u] = o[u];
     }
-    bool any = run[0] || run[1] || run[2] || run[3];
+    bool any = any_of(run);
     if (PR.packed) {
         // 32 bases per XOR; the run ends at the first differing base or at the end of either
         // sequence (the sentinels of the byte path)
-        int64_t rem[4];
+        int64_t rem[N];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < N; ++u) {
             rem[u] = run[u] ? min((int64_t)plen - v[u], (int64_t)tlen - h[u]) : 0;
             if (rem[u] <= 0) run[u] = false;
         }
-        any = run[0] || run[1] || run[2] || run[3];
+        any = any_of(run);
         while (any) {
-            uint64_t x[4];
+            uint64_t x[N];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < N; ++u)
                 x[u] = run[u] ? (load32b(A.ppat, PR.poff + v[u]) ^ load32b(A.ptxt, PR.toff + h[u])) : 0;
             any = false;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < N; ++u) {
                 if (!run[u]) continue;
                 int64_t nb = x[u] ? (int64_t)((__ffsll((long long)x[u]) - 1) >> 1) : 32;
                 const bool stop = x[u] != 0 || nb >= rem[u];
@@ -233,12 +243,12 @@ __device__ __forceinline__ void extend4(const WfaArgs &A, const WfaPairDev &PR, 
         }
     }
     while (any) {
-        uint64_t x[4];
+        uint64_t x[N];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = run[u] ? (load8(pat, v[u]) ^ load8(txt, h[u])) : 0;
+        for (int u = 0; u < N; ++u) x[u] = run[u] ? (load8(pat, v[u]) ^ load8(txt, h[u])) : 0;
         any = false;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < N; ++u) {
             if (!run[u]) continue;
             if (x[u]) {
                 const int nb = (__ffsll((long long)x[u]) - 1) >> 3;
@@ -251,12 +261,214 @@ __device__ __forceinline__ void extend4(const WfaArgs &A, const WfaPairDev &PR, 
         }
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < N; ++u)
         if (o[u] != WF_NULL) o[u] = (int32_t)h[u];
 }
 
+// The result of one pair (one thread): the backtrace of a pair that reached the end
+// (status 0), the CIGAR operations reversed into forward order, and the output record.
 template <bool PIG>
-__global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
+__device__ void finish_pair(const WfaArgs &A, const WfaPairDev &PR, int idx, const uint8_t *pat, const uint8_t *txt,
+                            const int64_t *ctab, const HdrRing &HR, int status, int end_score, int s, int64_t used) {
+    const WfaPen P = A.pen;
+    const int plen = PR.plen, tlen = PR.tlen;
+    const int k_end = tlen - plen;
+    WfaOutDev o;
+    o.status = status, o.score = 0, o.n_ops = 0, o.final_s = s;
+    o.mem_bytes = used;
+    if (status == 0) {
+        OpsWriter w{A.ops + PR.ops_off, 0, plen + tlen + 8, true};
+        if constexpr (PIG) {
+            // reverse the links from the end cell in place, then unpack the blocks
+            // oldest first: before every operation taken in M the run of matches
+            // is re-extended; the mismatch that closes a gap is dropped
+            const CompHdr m = HR.get(A, ctab, end_score, end_score)->c[CM];
+            const uint32_t *md = (const uint32_t *)(A.pool + m.off) + (k_end - m.base);
+            const uint32_t pc_end = md[m.pad];
+            uint32_t cur = md[2 * m.pad], prv = BT_NULL;
+            uint2 *blk = (uint2 *)A.pool;
+            const int64_t lim = 2 * ((int64_t)plen + tlen) + 64;
+            int64_t steps = 0;
+            bool ok = true;
+            while (cur != BT_NULL) {
+                if (++steps > lim) { ok = false; break; }
+                const uint32_t nxt = blk[cur].y;
+                blk[cur].y = prv;
+                prv = cur, cur = nxt;
+            }
+            int64_t v = 0, h = 0;
+            bool in_m = true;
+            cur = prv;
+            for (bool last = false; ok && !last;) {
+                uint32_t pc;
+                if (cur != BT_NULL) pc = blk[cur].x, cur = blk[cur].y;
+                else pc = pc_end, last = true;
+                const int len = pc ? 16 - (__clz(pc) >> 1) : 0;
+                for (int j = len - 1; j >= 0; --j) {
+                    if (in_m) {
+                        const int64_t nm = lcp1(A, PR, pat, txt, v, h);
+                        w.put('M', (int)nm);
+                        v += nm, h += nm;
+                    }
+                    const uint32_t op = (pc >> (2 * j)) & 3u;
+                    if (!in_m && op == 2u) {
+                        in_m = true;
+                        continue;
+                    }
+                    w.put(op == 1u ? 'D' : op == 2u ? 'X' : 'I', 1);
+                    v += (op == 1u || op == 2u), h += (op == 2u || op == 3u);
+                    in_m = op == 2u;
+                    if (op == 0u || v > plen || h > tlen) { ok = false; break; }
+                }
+            }
+            if (ok) {
+                const int64_t nm = min((int64_t)plen - v, (int64_t)tlen - h);
+                w.put('M', (int)nm);
+                v += nm, h += nm;
+                w.put('I', (int)(tlen - h));
+                w.put('D', (int)(plen - v));
+            } else {
+                o.status = WFA_UNATTAINABLE;
+            }
+        } else if (!A.singletrack) {
+            enum { BM = 9, BD2E = 8, BD2O = 7, BD1E = 6, BD1O = 5, BI2E = 4, BI2O = 3, BI1E = 2, BI1O = 1 };
+            int mt = CM, sc = end_score, k = k_end;
+            int32_t off = tlen;
+            int v = off - k, h = off;
+            const int64_t NEG = pb(WF_NULL, 0);
+            while (v > 0 && h > 0 && sc > 0) {
+                const int smm = sc - P.x, sg1 = sc - P.o1 - P.e1, sg2 = sc - P.o2 - P.e2, sx1 = sc - P.e1,
+                          sx2 = sc - P.e2;
+                auto G = [&](int scr, int comp, int kk, int add, int t) -> int64_t {
+                    if (scr < 0) return NEG;
+                    const CompHdr hh = hdr_ptr(A, ctab, scr)->c[comp];
+                    return pb(getv(A, hh, kk) + add, t);
+                };
+                int64_t mall;
+                const int64_t i1o = (mt == CM || mt == CI1) ? G(sg1, CM, k - 1, 1, BI1O) : NEG;
+                const int64_t i1e = (mt == CM || mt == CI1) ? G(sx1, CI1, k - 1, 1, BI1E) : NEG;
+                const int64_t d1o = (mt == CM || mt == CD1) ? G(sg1, CM, k + 1, 0, BD1O) : NEG;
+                const int64_t d1e = (mt == CM || mt == CD1) ? G(sx1, CD1, k + 1, 0, BD1E) : NEG;
+                const int64_t i2o = (mt == CM || mt == CI2) ? G(sg2, CM, k - 1, 1, BI2O) : NEG;
+                const int64_t i2e = (mt == CM || mt == CI2) ? G(sx2, CI2, k - 1, 1, BI2E) : NEG;
+                const int64_t d2o = (mt == CM || mt == CD2) ? G(sg2, CM, k + 1, 0, BD2O) : NEG;
+                const int64_t d2e = (mt == CM || mt == CD2) ? G(sx2, CD2, k + 1, 0, BD2E) : NEG;
+                if (mt == CM) {
+                    const int64_t misms = G(smm, CM, k, 1, BM);
+                    mall = max(misms, max(max(max(i1o, i1e), max(i2o, i2e)), max(max(d1o, d1e), max(d2o, d2e))));
+                } else if (mt == CI1) mall = max(i1o, i1e);
+                else if (mt == CI2) mall = max(i2o, i2e);
+                else if (mt == CD1) mall = max(d1o, d1e);
+                else mall = max(d2o, d2e);
+                if (mall < 0) break;
+                if (mt == CM) {
+                    const int mo = (int)(mall >> 4);
+                    w.put('M', off - mo);
+                    off = mo;
+                    v = off - k, h = off;
+                    if (v <= 0 || h <= 0) break;
+                }
+                const int bt = (int)(mall & 0xf);
+                switch (bt) {
+                case BM: sc = smm; mt = CM; break;
+                case BI1O: sc = sg1; mt = CM; break;
+                case BI1E: sc = sx1; mt = CI1; break;
+                case BI2O: sc = sg2; mt = CM; break;
+                case BI2E: sc = sx2; mt = CI2; break;
+                case BD1O: sc = sg1; mt = CM; break;
+                case BD1E: sc = sx1; mt = CD1; break;
+                case BD2O: sc = sg2; mt = CM; break;
+                default: sc = sx2; mt = CD2; break;
+                }
+                if (bt == BM) w.put('X', 1), --off;
+                else if (bt <= BI2E) w.put('I', 1), --k, --off;
+                else w.put('D', 1), ++k;
+                v = off - k, h = off;
+            }
+            if (mt == CM) {
+                if (v > 0 && h > 0) {
+                    const int nm = v < h ? v : h;
+                    w.put('M', nm);
+                    v -= nm, h -= nm;
+                }
+                w.put('D', v > 0 ? v : 0);
+                w.put('I', h > 0 ? h : 0);
+            }
+        } else {
+            int sc = end_score, k = k_end, gl = 0;
+            bool in_m = true, ok = true;
+            int32_t off = tlen, off_be = off;
+            const int64_t maxgap = (int64_t)plen + tlen;
+            while (sc != 0) {
+                if (sc < 0 || off < 0) { ok = false; break; }
+                if (in_m) {
+                    const int v = off - k, h = off;
+                    if (v < 0 || h < 0 || v > plen || h > tlen) { ok = false; break; }
+                    int nm = 0;
+                    while (nm < v && nm < h && pat[v - nm - 1] == txt[h - nm - 1]) ++nm;
+                    off_be = off - nm;
+                    const int ms = sc - P.x;
+                    bool took = false;
+                    if (ms >= 0) {
+                        const CompHdr mh = hdr_ptr(A, ctab, ms)->c[CM];
+                        if (mh.lo <= k && k <= mh.hi &&
+                            ((const int32_t *)(A.pool + mh.off))[k - mh.base] + 1 == off_be) {
+                            w.put('M', nm);
+                            w.put('X', 1);
+                            off = off_be - 1;
+                            sc = ms;
+                            took = true;
+                        }
+                    }
+                    if (!took) in_m = false, gl = 0;
+                    continue;
+                }
+                ++gl;
+                if ((int64_t)gl > maxgap) { ok = false; break; }
+                const int ki = k - gl, kd = k + gl;
+                for (int piece = 0; piece < 2; ++piece) {
+                    const int64_t isc = piece == 0 ? (int64_t)sc - P.o1 - (int64_t)gl * P.e1
+                                                   : (int64_t)sc - P.o2 - (int64_t)gl * P.e2;
+                    if (isc < 0 || isc > s) continue;
+                    const CompHdr ih = hdr_ptr(A, ctab, (int)isc)->c[CM];
+                    const int32_t *id = (const int32_t *)(A.pool + ih.off);
+                    if (ih.lo <= ki && ki <= ih.hi && id[ki - ih.base] + gl >= off_be &&
+                        id[ki - ih.base] + gl <= off) {
+                        w.put('M', off - (id[ki - ih.base] + gl));
+                        w.put('I', gl);
+                        k = ki, off = id[ki - ih.base], sc = (int)isc, in_m = true;
+                        break;
+                    }
+                    if (ih.lo <= kd && kd <= ih.hi && id[kd - ih.base] >= off_be && id[kd - ih.base] <= off) {
+                        w.put('M', off - id[kd - ih.base]);
+                        w.put('D', gl);
+                        k = kd, off = id[kd - ih.base], sc = (int)isc, in_m = true;
+                        break;
+                    }
+                }
+            }
+            if (ok && (!in_m || k != 0 || off < 0 || off > plen || off > tlen)) ok = false;
+            if (ok)
+                for (int i = 0; i < off; ++i)
+                    if (pat[i] != txt[i]) { ok = false; break; }
+            if (ok) w.put('M', off);
+            if (!ok) o.status = WFA_UNATTAINABLE;
+        }
+        if (!w.ok) o.status = WFA_OVERFLOW;
+        if (o.status == 0) {
+            for (int a = 0, b = PIG ? 0 : w.n - 1; a < b; ++a, --b) {
+                const char t = w.buf[a];
+                w.buf[a] = w.buf[b], w.buf[b] = t;
+            }
+            o.score = -end_score;
+            o.n_ops = w.n;
+        }
+    }
+    A.out[idx] = o;
+}
+
+template <bool PIG>
+__global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
     const int lane = threadIdx.x & 31;
     const WfaPen P = A.pen;
     extern __shared__ ScoreHdr hring_all[];
@@ -266,6 +478,7 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         if (lane == 0) pi = atomicAdd(A.queue, 1);
         pi = __shfl_sync(0xffffffffu, pi, 0);
         if (pi >= A.n) break;
+        if (lane == 0) atomicAdd(A.queue + 1, 1);  // pairs running on warps
         const int idx = A.order[pi];
         const WfaPairDev PR = A.pairs[idx];
         const int plen = PR.plen, tlen = PR.tlen;
@@ -321,13 +534,13 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         bool fused_reached = false;  // the compute step's extension reached the end (this lane)
         const int smax = PR.ctab_cap * HDR_CHUNK - 1;
         while (status == 0) {
-            // ---- extend M[s] and check the end.  Outside the piggyback modes the compute step
-            // below extends M[s] as it computes it (fused), so here only M[0] is extended.
+            // ---- extend M[s] and check the end.  The compute step below extends M[s] as it
+            // computes it (fused), so here only M[0] is extended.
             {
                 const CompHdr m = HR.get(A, ctab, s, s)->c[CM];
                 bool reached = false;
                 if (m.lo <= m.hi) {
-                    if (PIG || s == 0) {
+                    if (s == 0) {
                         int32_t *d = (int32_t *)(A.pool + m.off);
                         for (int k0 = m.lo + lane; k0 <= m.hi; k0 += 128) {
                             int32_t o[4];
@@ -336,7 +549,7 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                                 const int k = k0 + 32 * u;
                                 o[u] = k <= m.hi ? d[k - m.base] : WF_NULL;
                             }
-                            extend4(A, PR, pat, txt, k0, o);
+                            extend_n<4>(A, PR, pat, txt, k0, 32, o);
 #pragma unroll
                             for (int u = 0; u < 4; ++u) {
                                 const int k = k0 + 32 * u;
@@ -408,6 +621,21 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
             lo = min(lo, d2.lo - 1), hi = max(hi, d2.hi - 1);
             const bool a_i1 = !n_o1 || !n_i1, a_d1 = !n_o1 || !n_d1, a_i2 = !n_o2 || !n_i2, a_d2 = !n_o2 || !n_d2;
             const int width = hi - lo + 1;
+            // a wavefront wider than a warp's share: the cluster kernel re-runs the pair.  Above
+            // wide_width always; above wide_width_tail once every pair has started and at most
+            // wide_tail_pairs still run on warps (the batch's tail, whose idle SMs the cluster
+            // kernel puts to work)
+            if (!PIG && A.wide_width > 0 && width > A.wide_width_tail) {
+                int drained = 0;
+                if (lane == 0)
+                    drained = *(volatile int32_t *)A.queue >= A.n &&
+                              *(volatile int32_t *)(A.queue + 1) <= A.wide_tail_pairs;
+                drained = __shfl_sync(0xffffffffu, drained, 0);
+                if (width > A.wide_width || drained) {
+                    status = WFA_WIDE;
+                    break;
+                }
+            }
             CompHdr out[5];
             for (int c = 0; c < 5; ++c) out[c] = NUL;
             const bool alloc_c[5] = {true, a_i1, a_d1, a_i2, a_d2};
@@ -488,6 +716,21 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                                                                 : C[u][CI1];
                         C[u][CM] = Cell{in_matrix(best, k, plen, tlen) ? best : WF_NULL, (src.pc << 2) | 2u, src.pv};
                     }
+                    // the extension of M[s] (fused, as outside the piggyback modes): matches are
+                    // not recorded in the packed CIGAR; the traceback re-extends them
+                    {
+                        int32_t mo[PIG_U];
+#pragma unroll
+                        for (int u = 0; u < PIG_U; ++u) mo[u] = k0 + 32 * u <= hi ? C[u][CM].o : WF_NULL;
+                        extend_n<PIG_U>(A, PR, pat, txt, k0, 32, mo);
+#pragma unroll
+                        for (int u = 0; u < PIG_U; ++u) {
+                            const int k = k0 + 32 * u;
+                            if (k > hi) continue;
+                            C[u][CM].o = mo[u];
+                            if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) fused_reached = true;
+                        }
+                    }
                     // cells whose packed CIGAR holds 15 operations move it into a block,
                     // taken from the lane's reserved run; lanes whose run is short reserve
                     // LANE_BLOCKS more in one warp allocation
@@ -551,31 +794,35 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
                         del2[u] = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
                         misms[u] = getv(A, m_misms, k) + 1;
                     }
-                    // M[s] of these diagonals, then its extension (the extend step of the next
-                    // iteration, fused: the offsets never round-trip through memory unextended)
+                    // the gap components are final: store them (and their trimmed ends) first, so
+                    // that only M stays live across its extension
                     int32_t mo[4];
     #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int k = k0 + 32 * u;
                         const int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
                         mo[u] = (k <= hi && in_matrix(best, k, plen, tlen)) ? best : WF_NULL;
-                    }
-                    extend4(A, PR, pat, txt, k0, mo);
-    #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int k = k0 + 32 * u;
-                        if (k > hi) break;
-                        const int32_t best = mo[u];
-                        if (k == k_end && best != WF_NULL && best >= tlen) fused_reached = true;
-                        oM[k - lo] = best;
+                        if (k > hi) continue;
                         if (oI1) oI1[k - lo] = ins1[u];
                         if (oD1) oD1[k - lo] = del1[u];
                         if (oI2) oI2[k - lo] = ins2[u];
                         if (oD2) oD2[k - lo] = del2[u];
-                        const int32_t vals[5] = {best, ins1[u], del1[u], ins2[u], del2[u]};
+                        const int32_t vals[4] = {ins1[u], del1[u], ins2[u], del2[u]};
     #pragma unroll
-                        for (int c = 0; c < 5; ++c)
-                            if (in_matrix(vals[c], k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
+                        for (int c = 0; c < 4; ++c)
+                            if (in_matrix(vals[c], k, plen, tlen))
+                                kmin[c + 1] = min(kmin[c + 1], k), kmax[c + 1] = max(kmax[c + 1], k);
+                        if (mo[u] != WF_NULL) kmin[CM] = min(kmin[CM], k), kmax[CM] = max(kmax[CM], k);
+                    }
+                    // then M[s], extended (the extend step of the next iteration, fused: the
+                    // offsets never round-trip through memory unextended)
+                    extend_n<4>(A, PR, pat, txt, k0, 32, mo);
+    #pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + 32 * u;
+                        if (k > hi) break;
+                        if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) fused_reached = true;
+                        oM[k - lo] = mo[u];
                     }
                 }
             }
@@ -598,200 +845,405 @@ __global__ void __launch_bounds__(128) wfa_kernel(WfaArgs A, int rs) {
         }
         // ---- backtrace (lane 0)
         if (lane == 0) {
-            WfaOutDev o;
-            o.status = status, o.score = 0, o.n_ops = 0, o.final_s = s;
-            o.mem_bytes = al.used;
-            if (status == 0) {
-                OpsWriter w{A.ops + PR.ops_off, 0, plen + tlen + 8, true};
-                if constexpr (PIG) {
-                    // reverse the links from the end cell in place, then unpack the blocks
-                    // oldest first: before every operation taken in M the run of matches
-                    // is re-extended; the mismatch that closes a gap is dropped
-                    const CompHdr m = HR.get(A, ctab, end_score, end_score)->c[CM];
-                    const uint32_t *md = (const uint32_t *)(A.pool + m.off) + (k_end - m.base);
-                    const uint32_t pc_end = md[m.pad];
-                    uint32_t cur = md[2 * m.pad], prv = BT_NULL;
-                    uint2 *blk = (uint2 *)A.pool;
-                    const int64_t lim = 2 * ((int64_t)plen + tlen) + 64;
-                    int64_t steps = 0;
-                    bool ok = true;
-                    while (cur != BT_NULL) {
-                        if (++steps > lim) { ok = false; break; }
-                        const uint32_t nxt = blk[cur].y;
-                        blk[cur].y = prv;
-                        prv = cur, cur = nxt;
-                    }
-                    int64_t v = 0, h = 0;
-                    bool in_m = true;
-                    cur = prv;
-                    for (bool last = false; ok && !last;) {
-                        uint32_t pc;
-                        if (cur != BT_NULL) pc = blk[cur].x, cur = blk[cur].y;
-                        else pc = pc_end, last = true;
-                        const int len = pc ? 16 - (__clz(pc) >> 1) : 0;
-                        for (int j = len - 1; j >= 0; --j) {
-                            if (in_m) {
-                                const int64_t nm = lcp1(A, PR, pat, txt, v, h);
-                                w.put('M', (int)nm);
-                                v += nm, h += nm;
-                            }
-                            const uint32_t op = (pc >> (2 * j)) & 3u;
-                            if (!in_m && op == 2u) {
-                                in_m = true;
-                                continue;
-                            }
-                            w.put(op == 1u ? 'D' : op == 2u ? 'X' : 'I', 1);
-                            v += (op == 1u || op == 2u), h += (op == 2u || op == 3u);
-                            in_m = op == 2u;
-                            if (op == 0u || v > plen || h > tlen) { ok = false; break; }
-                        }
-                    }
-                    if (ok) {
-                        const int64_t nm = min((int64_t)plen - v, (int64_t)tlen - h);
-                        w.put('M', (int)nm);
-                        v += nm, h += nm;
-                        w.put('I', (int)(tlen - h));
-                        w.put('D', (int)(plen - v));
-                    } else {
-                        o.status = WFA_UNATTAINABLE;
-                    }
-                } else if (!A.singletrack) {
-                    enum { BM = 9, BD2E = 8, BD2O = 7, BD1E = 6, BD1O = 5, BI2E = 4, BI2O = 3, BI1E = 2, BI1O = 1 };
-                    int mt = CM, sc = end_score, k = k_end;
-                    int32_t off = tlen;
-                    int v = off - k, h = off;
-                    const int64_t NEG = pb(WF_NULL, 0);
-                    while (v > 0 && h > 0 && sc > 0) {
-                        const int smm = sc - P.x, sg1 = sc - P.o1 - P.e1, sg2 = sc - P.o2 - P.e2, sx1 = sc - P.e1,
-                                  sx2 = sc - P.e2;
-                        auto G = [&](int scr, int comp, int kk, int add, int t) -> int64_t {
-                            if (scr < 0) return NEG;
-                            const CompHdr hh = hdr_ptr(A, ctab, scr)->c[comp];
-                            return pb(getv(A, hh, kk) + add, t);
-                        };
-                        int64_t mall;
-                        const int64_t i1o = (mt == CM || mt == CI1) ? G(sg1, CM, k - 1, 1, BI1O) : NEG;
-                        const int64_t i1e = (mt == CM || mt == CI1) ? G(sx1, CI1, k - 1, 1, BI1E) : NEG;
-                        const int64_t d1o = (mt == CM || mt == CD1) ? G(sg1, CM, k + 1, 0, BD1O) : NEG;
-                        const int64_t d1e = (mt == CM || mt == CD1) ? G(sx1, CD1, k + 1, 0, BD1E) : NEG;
-                        const int64_t i2o = (mt == CM || mt == CI2) ? G(sg2, CM, k - 1, 1, BI2O) : NEG;
-                        const int64_t i2e = (mt == CM || mt == CI2) ? G(sx2, CI2, k - 1, 1, BI2E) : NEG;
-                        const int64_t d2o = (mt == CM || mt == CD2) ? G(sg2, CM, k + 1, 0, BD2O) : NEG;
-                        const int64_t d2e = (mt == CM || mt == CD2) ? G(sx2, CD2, k + 1, 0, BD2E) : NEG;
-                        if (mt == CM) {
-                            const int64_t misms = G(smm, CM, k, 1, BM);
-                            mall = max(misms, max(max(max(i1o, i1e), max(i2o, i2e)), max(max(d1o, d1e), max(d2o, d2e))));
-                        } else if (mt == CI1) mall = max(i1o, i1e);
-                        else if (mt == CI2) mall = max(i2o, i2e);
-                        else if (mt == CD1) mall = max(d1o, d1e);
-                        else mall = max(d2o, d2e);
-                        if (mall < 0) break;
-                        if (mt == CM) {
-                            const int mo = (int)(mall >> 4);
-                            w.put('M', off - mo);
-                            off = mo;
-                            v = off - k, h = off;
-                            if (v <= 0 || h <= 0) break;
-                        }
-                        const int bt = (int)(mall & 0xf);
-                        switch (bt) {
-                        case BM: sc = smm; mt = CM; break;
-                        case BI1O: sc = sg1; mt = CM; break;
-                        case BI1E: sc = sx1; mt = CI1; break;
-                        case BI2O: sc = sg2; mt = CM; break;
-                        case BI2E: sc = sx2; mt = CI2; break;
-                        case BD1O: sc = sg1; mt = CM; break;
-                        case BD1E: sc = sx1; mt = CD1; break;
-                        case BD2O: sc = sg2; mt = CM; break;
-                        default: sc = sx2; mt = CD2; break;
-                        }
-                        if (bt == BM) w.put('X', 1), --off;
-                        else if (bt <= BI2E) w.put('I', 1), --k, --off;
-                        else w.put('D', 1), ++k;
-                        v = off - k, h = off;
-                    }
-                    if (mt == CM) {
-                        if (v > 0 && h > 0) {
-                            const int nm = v < h ? v : h;
-                            w.put('M', nm);
-                            v -= nm, h -= nm;
-                        }
-                        w.put('D', v > 0 ? v : 0);
-                        w.put('I', h > 0 ? h : 0);
-                    }
-                } else {
-                    int sc = end_score, k = k_end, gl = 0;
-                    bool in_m = true, ok = true;
-                    int32_t off = tlen, off_be = off;
-                    const int64_t maxgap = (int64_t)plen + tlen;
-                    while (sc != 0) {
-                        if (sc < 0 || off < 0) { ok = false; break; }
-                        if (in_m) {
-                            const int v = off - k, h = off;
-                            if (v < 0 || h < 0 || v > plen || h > tlen) { ok = false; break; }
-                            int nm = 0;
-                            while (nm < v && nm < h && pat[v - nm - 1] == txt[h - nm - 1]) ++nm;
-                            off_be = off - nm;
-                            const int ms = sc - P.x;
-                            bool took = false;
-                            if (ms >= 0) {
-                                const CompHdr mh = hdr_ptr(A, ctab, ms)->c[CM];
-                                if (mh.lo <= k && k <= mh.hi &&
-                                    ((const int32_t *)(A.pool + mh.off))[k - mh.base] + 1 == off_be) {
-                                    w.put('M', nm);
-                                    w.put('X', 1);
-                                    off = off_be - 1;
-                                    sc = ms;
-                                    took = true;
-                                }
-                            }
-                            if (!took) in_m = false, gl = 0;
-                            continue;
-                        }
-                        ++gl;
-                        if ((int64_t)gl > maxgap) { ok = false; break; }
-                        const int ki = k - gl, kd = k + gl;
-                        for (int piece = 0; piece < 2; ++piece) {
-                            const int64_t isc = piece == 0 ? (int64_t)sc - P.o1 - (int64_t)gl * P.e1
-                                                           : (int64_t)sc - P.o2 - (int64_t)gl * P.e2;
-                            if (isc < 0 || isc > s) continue;
-                            const CompHdr ih = hdr_ptr(A, ctab, (int)isc)->c[CM];
-                            const int32_t *id = (const int32_t *)(A.pool + ih.off);
-                            if (ih.lo <= ki && ki <= ih.hi && id[ki - ih.base] + gl >= off_be &&
-                                id[ki - ih.base] + gl <= off) {
-                                w.put('M', off - (id[ki - ih.base] + gl));
-                                w.put('I', gl);
-                                k = ki, off = id[ki - ih.base], sc = (int)isc, in_m = true;
-                                break;
-                            }
-                            if (ih.lo <= kd && kd <= ih.hi && id[kd - ih.base] >= off_be && id[kd - ih.base] <= off) {
-                                w.put('M', off - id[kd - ih.base]);
-                                w.put('D', gl);
-                                k = kd, off = id[kd - ih.base], sc = (int)isc, in_m = true;
-                                break;
-                            }
-                        }
-                    }
-                    if (ok && (!in_m || k != 0 || off < 0 || off > plen || off > tlen)) ok = false;
-                    if (ok)
-                        for (int i = 0; i < off; ++i)
-                            if (pat[i] != txt[i]) { ok = false; break; }
-                    if (ok) w.put('M', off);
-                    if (!ok) o.status = WFA_UNATTAINABLE;
-                }
-                if (!w.ok) o.status = WFA_OVERFLOW;
-                if (o.status == 0) {
-                    for (int a = 0, b = PIG ? 0 : w.n - 1; a < b; ++a, --b) {
-                        const char t = w.buf[a];
-                        w.buf[a] = w.buf[b], w.buf[b] = t;
-                    }
-                    o.score = -end_score;
-                    o.n_ops = w.n;
-                }
-            }
-            A.out[idx] = o;
+            finish_pair<PIG>(A, PR, idx, pat, txt, ctab, HR, status, end_score, s, al.used);
+            atomicSub(A.queue + 1, 1);
         }
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Cluster kernel for pairs whose wavefronts outgrow a warp (high memory: standard and
+// Singletrack).  One cluster of CL CTAs (WIDE_NT threads each) per pair, one cluster barrier
+// per score:
+//   1. every thread of the cluster computes and extends the diagonals lo + gtid + GT*u of the
+//      plan (gtid = rank * WIDE_NT + thread, GT = CL * WIDE_NT), and each warp folds its
+//      trimmed ends per component, and whether the end cell was reached, into its CTA's
+//      partials;
+//   2. cluster barrier;
+//   3. warp 0 of every CTA gathers all CTAs' partials through distributed shared memory,
+//      and its lane 0 (the CTA's planner) finishes the score's headers and plans the next
+//      score.  Every planner holds the same state (the headers of the last scores in a
+//      shared-memory ring, the pool position), so all plans agree without being exchanged.
+// Pool space is carved deterministically out of reserve chunks that thread 0 of the first
+// CTA (the leader) takes from the pool one score ahead of need and announces to every CTA
+// through distributed shared memory before the barrier; the leader alone writes the pool
+// copy of the headers and the chunk table that the backtrace reads.  The cell arithmetic,
+// the limits, the trimming and the backtrace are the warp kernel's; only the split of the
+// diagonals differs, so the results are identical.  Offsets written by other CTAs are read
+// through L2 (ld.global.cg), after the barrier's release/acquire.
+constexpr int WIDE_NT = 384;
+constexpr int WIDE_U = 4;
+constexpr int WIDE_CHUNKS = 8;  // reserve chunks a planner keeps track of (a ring)
+
+enum { WOP_COMPUTE = 0, WOP_DONE = 1, WOP_EXIT = 2 };
+
+struct WidePlan {
+    int op, lo, hi, mask;  // mask: components allocated at the planned score (bit c)
+    CompHdr in[7];         // M[s-x], M[s-o1-e1], I1[s-e1], D1[s-e1], M[s-o2-e2], I2[s-e2], D2[s-e2]
+    CompHdr out[5];
+};
+struct WidePart {
+    int kmin[5], kmax[5], reached, pad;
+};
+// A reserve chunk announced by the leader: for pair `tag`, the planners' chunk number `seq`
+// (off < 0: the pool is exhausted).
+struct WideAnn {
+    int tag, seq;
+    int64_t off, len;
+};
+
+// The planner's state (lane 0 of warp 0 in every CTA; identical in all of them).
+struct WidePlanner {
+    int pi, idx;  // queue position and pair
+    int s, num_null, status, end_score, smax, R, ring_cap;
+    int lo_all, hi_all;  // the union of the planned diagonal ranges so far
+    int64_t ring, hdr_off, ctab_off;
+    int64_t cur, end;    // carving position in the current chunk
+    int nchunks, cidx;   // chunks received, chunk being carved
+    bool exhausted;
+};
+
+__device__ __forceinline__ int32_t getv_l2(const WfaArgs &A, const CompHdr &h, int k) {
+    if (k < h.lo || k > h.hi) return WF_NULL;
+    return __ldcg((const int32_t *)(A.pool + h.off) + (k - h.base));
+}
+
+__device__ __forceinline__ void part_reset(WidePart &p) {
+    for (int c = 0; c < 5; ++c) p.kmin[c] = INT_MAX, p.kmax[c] = INT_MIN;
+    p.reached = 0;
+}
+
+// Reserve chunk size: large (few pool atomics), smaller in a small pool.
+__device__ __forceinline__ int64_t wide_chunk(const WfaArgs &A, int64_t need) {
+    const int64_t base = min((int64_t)64 << 20, max((int64_t)1 << 20, A.pool_bytes / 64));
+    return ((max(base, 2 * need) + 255) & ~(int64_t)255);
+}
+
+__global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int CL = (int)cl.num_blocks();
+    const int rank = (int)cl.block_rank();
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int GT = CL * WIDE_NT, gtid = rank * WIDE_NT + tid;
+    const bool planner = tid == 0;
+    const bool leader = rank == 0 && tid == 0;
+    const WfaPen P = A.pen;
+    __shared__ WidePlan plan;
+    __shared__ WidePart part[2];
+    __shared__ WideAnn ann[2];     // reserve chunks announced before the barrier of step it (it & 1)
+    __shared__ WideAnn pstart[2];  // the pair of the np-th pair start (np & 1): tag = queue position,
+                                   // seq = pair, off/len = its first chunk
+    __shared__ int64_t qoff[WIDE_CHUNKS], qlen[WIDE_CHUNKS];  // the planner's chunks
+    extern __shared__ ScoreHdr wring[];
+    const HdrRing HR{wring, rs};
+    if (tid < 2) {
+        part_reset(part[tid]);
+        ann[tid] = WideAnn{-1, -1, -1, 0};
+    }
+    const CompHdr NUL{1, -1, 0, 0, 0};
+    WidePlanner W{};
+    int64_t used = 0;  // the leader's pool bytes for the pair
+    int it = 0, np = 0;
+
+    // ---- planner helpers (lane 0 of warp 0)
+    auto carve = [&](int64_t bytes) -> int64_t {
+        bytes = (bytes + 15) & ~(int64_t)15;
+        while (W.cur + bytes > W.end) {
+            if (W.cidx + 1 >= W.nchunks) return -1;
+            ++W.cidx;
+            W.cur = qoff[W.cidx % WIDE_CHUNKS];
+            W.end = W.cur + qlen[W.cidx % WIDE_CHUNKS];
+            if (W.cur < 0) return -1;
+        }
+        const int64_t r = W.cur;
+        W.cur += bytes;
+        return r;
+    };
+    // bytes the next plan may carve: one header chunk and the stored components over the
+    // planned range widened by one diagonal per side
+    auto need_next = [&]() -> int64_t {
+        const int64_t w = (int64_t)(W.hi_all - W.lo_all) + 3;
+        return (int64_t)sizeof(ScoreHdr) * HDR_CHUNK + (A.singletrack ? 1 : 5) * (w * 4 + 16) + 64;
+    };
+    // the next plan's carves fit: in the current chunk's tail, or in one queued chunk (a
+    // carve that does not fit moves on to the next chunk)
+    auto reserve_ok = [&]() -> bool {
+        const int64_t need = need_next();
+        bool ok = W.end - W.cur >= need;
+        for (int j = W.cidx + 1; j < W.nchunks; ++j) ok |= qlen[j % WIDE_CHUNKS] >= need;
+        return ok;
+    };
+    auto set_hdr = [&](int sc, const CompHdr (&o)[5]) {
+        if (leader) {
+            ScoreHdr *OH = (ScoreHdr *)(A.pool + W.hdr_off) + (sc % HDR_CHUNK);
+            for (int c = 0; c < 5; ++c) OH->c[c] = o[c];
+        }
+        if (HR.rs)
+            for (int c = 0; c < 5; ++c) HR.ring[sc & (HR.rs - 1)].c[c] = o[c];
+    };
+    // plans the next score with a non-null input; op = DONE with W.status set if the pair stops
+    auto plan_next = [&]() {
+        for (;;) {
+            ++W.s;
+            const int s = W.s;
+            if (s > W.smax) {
+                W.status = WFA_OVERFLOW;
+                break;
+            }
+            if (s % HDR_CHUNK == 0) {
+                const int64_t hb = carve((int64_t)sizeof(ScoreHdr) * HDR_CHUNK);
+                if (hb < 0) {
+                    W.status = WFA_RETRY;
+                    break;
+                }
+                W.hdr_off = hb;
+                if (leader) A.ctab[W.ctab_off + s / HDR_CHUNK] = hb;
+            }
+            const int sm = s - P.x, so1 = s - P.o1 - P.e1, se1 = s - P.e1, so2 = s - P.o2 - P.e2, se2 = s - P.e2;
+            CompHdr in[7];
+            in[0] = sm >= 0 ? HR.ring[sm & (HR.rs - 1)].c[CM] : NUL;
+            in[1] = so1 >= 0 ? HR.ring[so1 & (HR.rs - 1)].c[CM] : NUL;
+            in[2] = se1 >= 0 ? HR.ring[se1 & (HR.rs - 1)].c[CI1] : NUL;
+            in[3] = se1 >= 0 ? HR.ring[se1 & (HR.rs - 1)].c[CD1] : NUL;
+            in[4] = so2 >= 0 ? HR.ring[so2 & (HR.rs - 1)].c[CM] : NUL;
+            in[5] = se2 >= 0 ? HR.ring[se2 & (HR.rs - 1)].c[CI2] : NUL;
+            in[6] = se2 >= 0 ? HR.ring[se2 & (HR.rs - 1)].c[CD2] : NUL;
+            bool isnull[7], all_null = true;
+            for (int j = 0; j < 7; ++j) isnull[j] = in[j].lo > in[j].hi, all_null &= isnull[j];
+            if (all_null) {
+                const CompHdr o[5] = {NUL, NUL, NUL, NUL, NUL};
+                set_hdr(s, o);
+                // the top of the next step: M[s] is empty
+                if (++W.num_null > A.max_score_scope) {
+                    W.status = -3;
+                    break;
+                }
+                continue;
+            }
+            W.num_null = 0;
+            int lo = in[0].lo, hi = in[0].hi;
+            lo = min(lo, in[1].lo - 1), hi = max(hi, in[1].hi + 1);
+            lo = min(lo, in[2].lo + 1), hi = max(hi, in[2].hi + 1);
+            lo = min(lo, in[3].lo - 1), hi = max(hi, in[3].hi - 1);
+            lo = min(lo, in[4].lo - 1), hi = max(hi, in[4].hi + 1);
+            lo = min(lo, in[5].lo + 1), hi = max(hi, in[5].hi + 1);
+            lo = min(lo, in[6].lo - 1), hi = max(hi, in[6].hi - 1);
+            W.lo_all = min(W.lo_all, lo), W.hi_all = max(W.hi_all, hi);
+            const bool alloc_c[5] = {true, !isnull[1] || !isnull[2], !isnull[1] || !isnull[3],
+                                     !isnull[4] || !isnull[5], !isnull[4] || !isnull[6]};
+            const int width = hi - lo + 1;
+            const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
+            int mask = 0;
+            for (int c = 0; c < 5; ++c) mask |= alloc_c[c] ? 1 << c : 0;
+            const int nstore = A.singletrack ? 1 : __popc(mask);
+            if (A.singletrack && width > W.ring_cap) {
+                W.status = WFA_OVERFLOW;
+                break;
+            }
+            const int64_t blk = carve(wb * nstore);
+            if (blk < 0) {
+                W.status = WFA_RETRY;
+                break;
+            }
+            int64_t o = blk;
+            for (int c = 0; c < 5; ++c) {
+                plan.out[c] = NUL;
+                if (!alloc_c[c]) continue;
+                int64_t place;
+                if (c == CM || !A.singletrack) place = o, o += wb;
+                else place = W.ring + ((int64_t)((s % W.R) * 4 + (c - 1)) * W.ring_cap) * 4;
+                plan.out[c] = CompHdr{lo, hi, lo, 0, place};
+            }
+            for (int j = 0; j < 7; ++j) plan.in[j] = in[j];
+            plan.op = WOP_COMPUTE, plan.lo = lo, plan.hi = hi, plan.mask = mask;
+            return;
+        }
+        plan.op = WOP_DONE;
+    };
+
+    for (;;) {
+        // ---- pair start: the leader takes the next pair and its first chunk
+        if (leader) {
+            WideAnn a{A.n, -1, -1, 0};
+            const int pi = atomicAdd(A.queue, 1);
+            if (pi < A.n) {
+                const int idx = A.order[pi];
+                const WfaPairDev PR = A.pairs[idx];
+                const int R = (P.e1 > P.e2 ? P.e1 : P.e2) + 1;
+                const int64_t ring_b = A.singletrack ? (int64_t)R * 4 * (PR.plen + PR.tlen + 8) * 4 + 16 : 0;
+                const int64_t len = wide_chunk(A, ring_b + (int64_t)sizeof(ScoreHdr) * HDR_CHUNK + 4096);
+                a = WideAnn{pi, idx, pool_grab(A, len), len};
+                used = a.off >= 0 ? len : 0;
+            }
+            for (int c = 0; c < CL; ++c) *cl.map_shared_rank(&pstart[np & 1], c) = a;
+        }
+        cl.sync();
+        if (planner) {
+            const WideAnn a = pstart[np & 1];
+            if (a.tag >= A.n) {
+                plan.op = WOP_EXIT;
+            } else {
+                const WfaPairDev PR = A.pairs[a.seq];
+                W = WidePlanner{};
+                W.pi = a.tag, W.idx = a.seq, W.ctab_off = PR.ctab_off;
+                W.smax = PR.ctab_cap * HDR_CHUNK - 1;
+                W.R = (P.e1 > P.e2 ? P.e1 : P.e2) + 1;
+                W.ring_cap = PR.plen + PR.tlen + 8;
+                W.end_score = -1, W.lo_all = 0, W.hi_all = 0;
+                W.ring = -1;
+                qoff[0] = a.off, qlen[0] = a.len;
+                W.nchunks = 1, W.cidx = 0, W.cur = a.off, W.end = a.off + a.len;
+                W.exhausted = a.off < 0;
+                if (a.off < 0) W.status = WFA_RETRY;
+                if (W.status == 0 && A.singletrack) {
+                    W.ring = carve((int64_t)W.R * 4 * W.ring_cap * 4);
+                    if (W.ring < 0) W.status = WFA_RETRY;
+                }
+                const int64_t h0 = W.status == 0 ? carve((int64_t)sizeof(ScoreHdr) * HDR_CHUNK) : -1;
+                const int64_t d0 = h0 >= 0 ? carve(16) : -1;
+                if (W.status == 0 && d0 < 0) W.status = WFA_RETRY;
+                if (W.status == 0) {
+                    // M[0] = {0} on diagonal 0, extended (every planner writes the same value)
+                    const int32_t o0 = (int32_t)lcp1(A, PR, A.pat + PR.poff, A.txt + PR.toff, 0, 0);
+                    W.hdr_off = h0;
+                    if (leader) A.ctab[PR.ctab_off] = h0;
+                    *(int32_t *)(A.pool + d0) = o0;
+                    const CompHdr o[5] = {CompHdr{0, 0, 0, 0, d0}, NUL, NUL, NUL, NUL};
+                    set_hdr(0, o);
+                    if (PR.tlen - PR.plen == 0 && o0 >= PR.tlen) W.end_score = 0;
+                }
+                if (W.status != 0 || W.end_score == 0) plan.op = WOP_DONE;
+                else plan_next();
+            }
+        }
+        __syncthreads();
+        ++np;
+        int op = plan.op;
+        if (op == WOP_EXIT) break;
+        const int pidx = pstart[(np - 1) & 1].seq;
+        const WfaPairDev PR = A.pairs[pidx];
+        const int plen = PR.plen, tlen = PR.tlen, k_end = tlen - plen;
+        const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
+        while (op == WOP_COMPUTE) {
+            // ---- 1. this thread's diagonals of the planned score
+            {
+                const int lo = plan.lo, hi = plan.hi, mask = plan.mask;
+                const CompHdr m_misms = plan.in[0], m_open1 = plan.in[1], i1 = plan.in[2], d1 = plan.in[3],
+                              m_open2 = plan.in[4], i2 = plan.in[5], d2 = plan.in[6];
+                int32_t *oM = (int32_t *)(A.pool + plan.out[CM].off);
+                int32_t *oI1 = (mask & 2) ? (int32_t *)(A.pool + plan.out[CI1].off) : nullptr;
+                int32_t *oD1 = (mask & 4) ? (int32_t *)(A.pool + plan.out[CD1].off) : nullptr;
+                int32_t *oI2 = (mask & 8) ? (int32_t *)(A.pool + plan.out[CI2].off) : nullptr;
+                int32_t *oD2 = (mask & 16) ? (int32_t *)(A.pool + plan.out[CD2].off) : nullptr;
+                int kmin[5], kmax[5];
+                bool reached = false;
+#pragma unroll
+                for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
+                for (int k0 = lo + gtid; k0 <= hi; k0 += GT * WIDE_U) {
+                    int32_t ins1[WIDE_U], ins2[WIDE_U], del1[WIDE_U], del2[WIDE_U], misms[WIDE_U];
+#pragma unroll
+                    for (int u = 0; u < WIDE_U; ++u) {
+                        const int k = k0 + GT * u;
+                        ins1[u] = max(getv_l2(A, m_open1, k - 1), getv_l2(A, i1, k - 1)) + 1;
+                        ins2[u] = max(getv_l2(A, m_open2, k - 1), getv_l2(A, i2, k - 1)) + 1;
+                        del1[u] = max(getv_l2(A, m_open1, k + 1), getv_l2(A, d1, k + 1));
+                        del2[u] = max(getv_l2(A, m_open2, k + 1), getv_l2(A, d2, k + 1));
+                        misms[u] = getv_l2(A, m_misms, k) + 1;
+                    }
+                    int32_t mo[WIDE_U];
+#pragma unroll
+                    for (int u = 0; u < WIDE_U; ++u) {
+                        const int k = k0 + GT * u;
+                        const int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
+                        mo[u] = (k <= hi && in_matrix(best, k, plen, tlen)) ? best : WF_NULL;
+                        if (k > hi) continue;
+                        if (oI1) oI1[k - lo] = ins1[u];
+                        if (oD1) oD1[k - lo] = del1[u];
+                        if (oI2) oI2[k - lo] = ins2[u];
+                        if (oD2) oD2[k - lo] = del2[u];
+                        const int32_t vals[4] = {ins1[u], del1[u], ins2[u], del2[u]};
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (in_matrix(vals[c], k, plen, tlen))
+                                kmin[c + 1] = min(kmin[c + 1], k), kmax[c + 1] = max(kmax[c + 1], k);
+                        if (mo[u] != WF_NULL) kmin[CM] = min(kmin[CM], k), kmax[CM] = max(kmax[CM], k);
+                    }
+                    extend_n<WIDE_U>(A, PR, pat, txt, k0, GT, mo);
+#pragma unroll
+                    for (int u = 0; u < WIDE_U; ++u) {
+                        const int k = k0 + GT * u;
+                        if (k > hi) break;
+                        if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) reached = true;
+                        oM[k - lo] = mo[u];
+                    }
+                }
+                WidePart &pp = part[it & 1];
+#pragma unroll
+                for (int c = 0; c < 5; ++c) {
+                    const int th = __reduce_max_sync(0xffffffffu, kmax[c]);
+                    const int tl = __reduce_min_sync(0xffffffffu, kmin[c]);
+                    if (lane == 0 && th != INT_MIN) atomicMax(&pp.kmax[c], th), atomicMin(&pp.kmin[c], tl);
+                }
+                if (__any_sync(0xffffffffu, reached) && lane == 0) pp.reached = 1;
+            }
+            // the leader reserves the next plan's space ahead of need
+            if (leader && !W.exhausted && W.nchunks - W.cidx < WIDE_CHUNKS - 1 && !reserve_ok()) {
+                const int64_t len = wide_chunk(A, need_next());
+                const int64_t off = pool_grab(A, len);
+                if (off >= 0) used += len;
+                const WideAnn a{W.pi, W.nchunks, off, off >= 0 ? len : 0};
+                for (int c = 0; c < CL; ++c) *cl.map_shared_rank(&ann[it & 1], c) = a;
+            }
+            cl.sync();
+            // ---- 3. gather, finish the score, plan the next one (warp 0 of every CTA)
+            if (tid < 32) {
+                int gmin[5], gmax[5], gr = 0;
+#pragma unroll
+                for (int c = 0; c < 5; ++c) gmin[c] = INT_MAX, gmax[c] = INT_MIN;
+                if (lane < CL) {
+                    const WidePart *rp = cl.map_shared_rank(&part[it & 1], lane);
+#pragma unroll
+                    for (int c = 0; c < 5; ++c) gmin[c] = rp->kmin[c], gmax[c] = rp->kmax[c];
+                    gr = rp->reached;
+                }
+#pragma unroll
+                for (int c = 0; c < 5; ++c)
+                    gmin[c] = __reduce_min_sync(0xffffffffu, gmin[c]), gmax[c] = __reduce_max_sync(0xffffffffu, gmax[c]);
+                gr = __any_sync(0xffffffffu, gr != 0);
+                if (planner) {
+                    part_reset(part[(it + 1) & 1]);
+                    const WideAnn a = ann[it & 1];
+                    if (a.tag == W.pi && a.seq == W.nchunks) {
+                        qoff[W.nchunks % WIDE_CHUNKS] = a.off, qlen[W.nchunks % WIDE_CHUNKS] = a.len;
+                        ++W.nchunks;
+                        if (a.off < 0) W.exhausted = true;
+                    }
+                    CompHdr out[5];
+                    for (int c = 0; c < 5; ++c) {
+                        out[c] = plan.out[c];
+                        if (!(plan.mask & (1 << c))) continue;
+                        // no diagonal in the matrix: the empty range [lo, lo-1] of the scan
+                        if (gmax[c] == INT_MIN) out[c].hi = out[c].lo - 1;
+                        else out[c].lo = gmin[c], out[c].hi = gmax[c];
+                    }
+                    set_hdr(W.s, out);
+                    if (gr) {
+                        W.end_score = W.s;
+                        plan.op = WOP_DONE;
+                    } else {
+                        plan_next();
+                    }
+                }
+            }
+            __syncthreads();
+            ++it;
+            op = plan.op;
+        }
+        // ---- backtrace (leader)
+        if (leader)
+            finish_pair<false>(A, PR, W.idx, pat, txt, A.ctab + PR.ctab_off, HR, W.status, W.end_score, W.s, used);
     }
 }
 
@@ -820,6 +1272,56 @@ static cudaError_t launch_wfa_t(const WfaArgs &a, int ctas, cudaStream_t st) {
 
 cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st) {
     return a.piggyback ? launch_wfa_t<true>(a, ctas, st) : launch_wfa_t<false>(a, ctas, st);
+}
+
+static cudaLaunchConfig_t wide_config(int ctas, int cl, size_t smem, cudaStream_t st, cudaLaunchAttribute *at) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3(WIDE_NT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Header ring of the cluster kernel's planners: the smallest power of two above the score
+// scope, 32..1024 (0: scope too large for the cluster kernel).
+static int wide_ring_size(int scope) {
+    int rs = 32;
+    while (rs <= scope && rs <= 1024) rs <<= 1;
+    return rs <= 1024 ? rs : 0;
+}
+
+cudaError_t launch_wfa_wide(const WfaArgs &a, int clusters, int cl, cudaStream_t st) {
+    const int rs = wide_ring_size(a.max_score_scope);
+    if (rs == 0) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)rs * sizeof(ScoreHdr);
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(wfa_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t cfg = wide_config(clusters * cl, cl, smem, st, at);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, wfa_wide_kernel, a, rs);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+int wfa_wide_clusters(int cl, int scope) {
+    const int rs = wide_ring_size(scope);
+    if (rs == 0) return 0;
+    const size_t smem = (size_t)rs * sizeof(ScoreHdr);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(wfa_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t cfg = wide_config(cl, cl, smem, 0, at);
+    int n = 0;
+    return cudaOccupancyMaxActiveClusters(&n, (void *)wfa_wide_kernel, &cfg) == cudaSuccess ? n : 0;
 }
 
 namespace {

@@ -9,6 +9,7 @@
 #include "../../include/anchorwave_b200.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -41,6 +42,12 @@ struct PinBuf {
 
 int64_t al8(int64_t v) { return (v + 7) & ~(int64_t)7; }
 
+// Wavefront width from which a warp hands its pair to the cluster kernel, and the CTAs of a
+// cluster (aw_set_wfa_wide).
+std::atomic<int> g_wide_width{8192};
+std::atomic<int> g_wide_tail{1024};
+std::atomic<int> g_wide_cluster{8};
+
 }  // namespace
 
 struct wavefront_aligner_gpu {
@@ -59,6 +66,7 @@ struct wavefront_aligner_gpu {
     int sms = 0;
     float last_ms = 0.f;
     int last_launches = 0;
+    int last_cluster_launches = 0, last_cluster_pairs = 0;
     ~wavefront_aligner_gpu() {
         d_pat.release(), d_txt.release(), d_pairs.release(), d_order.release(), d_pool.release();
         d_head.release(), d_ctab.release(), d_ops.release(), d_out.release(), d_queue.release();
@@ -162,56 +170,75 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     const int scope = std::max(A.gap_opening1 + A.gap_extension1, A.gap_opening2 + A.gap_extension2);
     W.max_score_scope = std::max(scope, A.mismatch) + 1;
     const int occ = std::max(1, wfa_occupancy(W.piggyback != 0));
+    // Pairs whose wavefront outgrows a warp (high memory only) stop with WFA_WIDE and run
+    // again, from score 0, on the cluster kernel once the warp phase is over.
+    const int cl = std::min(8, std::max(1, g_wide_cluster.load()));
+    const int wide_clusters = W.piggyback ? 0 : wfa_wide_clusters(cl, W.max_score_scope);
+    W.wide_width = wide_clusters > 0 ? std::max(0, g_wide_width.load()) : 0;
+    W.wide_width_tail = std::min(W.wide_width, std::max(0, g_wide_tail.load()));
+    W.wide_tail_pairs = std::max(1, wide_clusters);
     // Rounds: every round restarts the pool and runs up to `chunk` pending pairs, largest
     // first; pairs that found the pool exhausted stay pending.  A round that completes
     // nothing halves the chunk (the pairs in flight together share the pool), one that
     // completes all of its pairs doubles it again; a pair that cannot finish with the whole
     // pool to itself reports WF_STATUS_OOM (the reference's max-memory abort).
-    std::vector<int32_t> pending = order;
-    size_t chunk = pending.size();
+    std::vector<int32_t> wide;
+    al->last_cluster_launches = 0;
     float total_ms = 0.f;
     int launches = 0;
-    while (!pending.empty()) {
-        const size_t take = std::min(chunk, pending.size());
-        std::vector<int32_t> batch(pending.begin(), pending.begin() + (std::ptrdiff_t)take);
-        WCUDA(cudaMemcpyAsync(al->d_order.p, batch.data(), sizeof(int32_t) * batch.size(), cudaMemcpyHostToDevice,
-                              al->st));
-        WCUDA(cudaMemsetAsync(al->d_queue.p, 0, 4, al->st));
-        WCUDA(cudaMemsetAsync(al->d_head.p, 0, 8, al->st));
-        W.order = al->d_order.as<int32_t>();
-        W.n = (int32_t)batch.size();
-        const int ctas = std::min((W.n + 3) / 4, occ * al->sms);
-        WCUDA(cudaEventRecord(al->e0, al->st));
-        WCUDA(launch_wfa(W, ctas, al->st));
-        WCUDA(cudaEventRecord(al->e1, al->st));
-        ++launches;
-        WCUDA(cudaMemcpyAsync(al->outs.data(), al->d_out.p, sizeof(WfaOutDev) * (size_t)n, cudaMemcpyDeviceToHost,
-                              al->st));
-        WCUDA(cudaStreamSynchronize(al->st));
-        float ms = 0.f;
-        WCUDA(cudaEventElapsedTime(&ms, al->e0, al->e1));
-        total_ms += ms;
-        std::vector<int32_t> again;
-        for (int32_t i : batch)
-            if (al->outs[i].status == WFA_RETRY) again.push_back(i);
-        if (getenv("AW_VERBOSE"))
-            fprintf(stderr, "[aw_b200] WFA round %d: %zu pairs, %zu to retry, %.1f ms\n", launches, batch.size(),
-                    again.size(), ms);
-        const size_t done = batch.size() - again.size();
-        if (done == 0 && take == 1) {
-            al->outs[batch[0]].status = WFA_OOM;
-            again.clear();
-        } else if (done == 0) {
-            chunk = std::max<size_t>(1, take / 2);
-        } else if (again.empty() && take == chunk) {
-            chunk *= 2;
+    for (int phase = 0; phase < 2; ++phase) {
+        std::vector<int32_t> pending = phase == 0 ? order : wide;
+        size_t chunk = pending.size();
+        while (!pending.empty()) {
+            const size_t take = std::min(chunk, pending.size());
+            std::vector<int32_t> batch(pending.begin(), pending.begin() + (std::ptrdiff_t)take);
+            WCUDA(cudaMemcpyAsync(al->d_order.p, batch.data(), sizeof(int32_t) * batch.size(), cudaMemcpyHostToDevice,
+                                  al->st));
+            WCUDA(cudaMemsetAsync(al->d_queue.p, 0, 8, al->st));
+            WCUDA(cudaMemsetAsync(al->d_head.p, 0, 8, al->st));
+            W.order = al->d_order.as<int32_t>();
+            W.n = (int32_t)batch.size();
+            WCUDA(cudaEventRecord(al->e0, al->st));
+            if (phase == 0) {
+                WCUDA(launch_wfa(W, std::min((W.n + 3) / 4, occ * al->sms), al->st));
+            } else {
+                ++al->last_cluster_launches;
+                WCUDA(launch_wfa_wide(W, std::min(W.n, wide_clusters), cl, al->st));
+            }
+            WCUDA(cudaEventRecord(al->e1, al->st));
+            ++launches;
+            WCUDA(cudaMemcpyAsync(al->outs.data(), al->d_out.p, sizeof(WfaOutDev) * (size_t)n, cudaMemcpyDeviceToHost,
+                                  al->st));
+            WCUDA(cudaStreamSynchronize(al->st));
+            float ms = 0.f;
+            WCUDA(cudaEventElapsedTime(&ms, al->e0, al->e1));
+            total_ms += ms;
+            std::vector<int32_t> again;
+            size_t handed = 0;
+            for (int32_t i : batch) {
+                if (al->outs[i].status == WFA_RETRY) again.push_back(i);
+                if (al->outs[i].status == WFA_WIDE) wide.push_back(i), ++handed;
+            }
+            if (getenv("AW_VERBOSE"))
+                fprintf(stderr, "[aw_b200] WFA round %d (%s): %zu pairs, %zu to retry, %zu to the cluster kernel, %.1f ms\n",
+                        launches, phase ? "cluster" : "warp", batch.size(), again.size(), handed, ms);
+            const size_t done = batch.size() - again.size();
+            if (done == 0 && take == 1) {
+                al->outs[batch[0]].status = WFA_OOM;
+                again.clear();
+            } else if (done == 0) {
+                chunk = std::max<size_t>(1, take / 2);
+            } else if (again.empty() && take == chunk) {
+                chunk *= 2;
+            }
+            // the retried pairs first (still largest first), then those not yet run
+            again.insert(again.end(), pending.begin() + (std::ptrdiff_t)take, pending.end());
+            pending.swap(again);
         }
-        // the retried pairs first (still largest first), then those not yet run
-        again.insert(again.end(), pending.begin() + (std::ptrdiff_t)take, pending.end());
-        pending.swap(again);
     }
     al->last_ms = total_ms;
     al->last_launches = launches;
+    al->last_cluster_pairs = (int)wide.size();
     al->mem_pair_max = 0, al->mem_total = 0;
     for (int i = 0; i < n; ++i) {
         al->mem_pair_max = std::max<int64_t>(al->mem_pair_max, al->outs[i].mem_bytes);
@@ -266,6 +293,21 @@ wavefront_aligner_gpu_t *wavefront_aligner_new_gpu(const wavefront_gpu_attr_t *a
 }
 
 void wavefront_aligner_delete_gpu(wavefront_aligner_gpu_t *al) { delete al; }
+
+int wavefront_gpu_last_launches(const wavefront_aligner_gpu_t *al, int *launches, int *cluster_launches,
+                                int *cluster_pairs) {
+    if (!al) return AW_E_INVAL;
+    if (launches) *launches = al->last_launches;
+    if (cluster_launches) *cluster_launches = al->last_cluster_launches;
+    if (cluster_pairs) *cluster_pairs = al->last_cluster_pairs;
+    return AW_OK;
+}
+
+void aw_set_wfa_wide(int width, int tail_width, int cluster_ctas) {
+    if (width >= 0) g_wide_width.store(width);
+    if (tail_width >= 0) g_wide_tail.store(tail_width);
+    if (cluster_ctas > 0) g_wide_cluster.store(std::min(8, cluster_ctas));
+}
 
 int wavefront_align_gpu(wavefront_aligner_gpu_t *al, const char *pattern, int pattern_length, const char *text,
                         int text_length) {

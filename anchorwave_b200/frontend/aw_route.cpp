@@ -33,6 +33,8 @@ bool is_wfa(AlignmentCandidate c) {
 aw_serve_route_t route_of(AlignmentCandidate c, const anchorwave::AlignmentSelectionPlan &p) {
     aw_serve_route_t r;
     r.band = -1, r.band_max = -1, r.window = 0;
+    const anchorwave::AlgorithmCostEstimate *e = estimate_of(p, c);
+    r.predicted_bytes = e ? (int64_t)std::min<uint64_t>(e->memoryBytes, (uint64_t)INT64_MAX) : 0;
     switch (c) {
     case AlignmentCandidate::SingletrackWfa: r.method = AW_ROUTE_WFA_SINGLETRACK; break;
     case AlignmentCandidate::StandardWfa: r.method = AW_ROUTE_WFA; break;

@@ -24,7 +24,7 @@ extern "C" {
 #endif
 
 typedef struct {
-    aw_serve_route_t route;
+    aw_serve_route_t route;   /* route.predicted_bytes: the plan's memoryBytes of the candidate */
     int candidate;  /* anchorwave::AlignmentCandidate (AlignmentAlgorithmSelector.h:10-20) */
     int tier;       /* 1 exact, 2 approximate */
 } aw_route_choice_t;

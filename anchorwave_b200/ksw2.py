@@ -281,6 +281,11 @@ def set_band_columns(columns: int = 0):
     lib.aw_set_band_columns(int(columns))
 
 
+def set_full_pair_routing(enabled: bool = True):
+    """aw_set_full_pair_routing: critical-path full-matrix pairs on the banded kernel (default)."""
+    lib.aw_set_full_pair_routing(1 if enabled else 0)
+
+
 def set_tuning(large_warps: int = 0, large_tlen_threshold: int = 0):
     lib.aw_set_tuning(int(large_warps), int(large_tlen_threshold))
 

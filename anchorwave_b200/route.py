@@ -40,6 +40,7 @@ class Route:
     window: int
     candidate: str
     tier: int
+    predicted_bytes: int = 0
 
 
 def _load():
@@ -74,5 +75,5 @@ def route_intervals(pairs: Sequence[Tuple[bytes, bytes]], window_width: int = AN
                                 nthreads or os.cpu_count() or 1, out)
     if rc != 0:
         raise ValueError("aw_route_intervals: bad arguments")
-    return [Route(o.route.method, o.route.band, o.route.band_max, o.route.window, CANDIDATES[o.candidate], o.tier)
-            for o in out]
+    return [Route(o.route.method, o.route.band, o.route.band_max, o.route.window, CANDIDATES[o.candidate], o.tier,
+                  o.route.predicted_bytes) for o in out]

@@ -33,6 +33,7 @@ class ServeRouteSpec:
     band: int = -1
     band_max: int = -1
     window: int = 0
+    predicted_bytes: int = 0
 
 
 @dataclass
@@ -61,11 +62,12 @@ class AlignmentServer:
             raise AwError(f"aw_serve_open failed: {last_error()}")
 
     def submit(self, rid: int, method: int, query: bytes, target: bytes, band: int = -1, band_max: int = -1,
-               window: int = 0):
+               window: int = 0, predicted_bytes: int = 0):
         """Enqueue one interval with its engine and that engine's parameters (band: KSW2 band,
         or score-certified KSW2's initial band; band_max: its largest band; window: the
-        sliding-window width)."""
-        rt = ServeRoute(method, band, band_max, window)
+        sliding-window width; predicted_bytes: the selector's memory estimate, 0 = the
+        server's own)."""
+        rt = ServeRoute(method, band, band_max, window, int(predicted_bytes))
         rc = lib.aw_serve_submit_route(self.h, rid, C.byref(rt), query, len(query), target, len(target))
         if rc != 0:
             raise AwError(f"aw_serve_submit_route failed ({rc}): {last_error()}")

@@ -29,6 +29,14 @@ WAVEFRONT_MEMORY_MED = 1
 WAVEFRONT_MEMORY_LOW = 2
 
 
+def set_wide(width: int = -1, tail_width: int = -1, cluster_ctas: int = 0) -> None:
+    """aw_set_wfa_wide: wavefront width from which a high-memory pair leaves its warp for a
+    cluster of CTAs (0 = never), the lower width that applies once every pair of the call has
+    started, and the CTAs of a cluster (1..8).  Negative widths and cluster_ctas 0 keep the
+    setting.  Results are identical under every setting."""
+    lib.aw_set_wfa_wide(int(width), int(tail_width), int(cluster_ctas))
+
+
 def positive_penalty(p: int) -> int:
     """AnchorWave passes negative penalties; WFA takes their magnitude (WfaAlignment.cpp:298-302)."""
     return -p if p < 0 else p
@@ -115,6 +123,12 @@ class WfaAligner:
         tot = C.c_int64(0)
         lib.wavefront_gpu_memory(self.h, C.byref(mx), C.byref(tot))
         return mx.value, tot.value
+
+    def launches(self) -> Tuple[int, int, int]:
+        """The last call's kernel launches: (all, of which the cluster kernel's, pairs moved to it)."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        lib.wavefront_gpu_last_launches(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
 
     def close(self):
         if self.h:

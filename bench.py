@@ -330,10 +330,16 @@ def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 4
         from anchorwave_b200 import route
     except ImportError as e:
         return {"unavailable": f"routing front end missing: {e}"}
+    t_all = time.perf_counter()
+
+    def log(msg):
+        print(f"[bench serving +{time.perf_counter() - t_all:.1f}s] {msg}", file=sys.stderr, flush=True)
+
     reqs = W.serving_trace(nreq, seed=4 + rank, lmax=500_000)
     t0 = time.perf_counter()
     routes = route.route_intervals([(r.query, r.target) for r in reqs])
     route_s = time.perf_counter() - t0
+    log(f"{len(reqs)} requests generated and routed ({route_s:.1f} s)")
     mix = collections.Counter(rt.candidate for rt in routes)
     cells = sum(len(r.query) * len(r.target) for r in reqs)
     mat = ksw2.anchorwave_matrix(-4)
@@ -356,7 +362,7 @@ def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 4
                         if d > 0:
                             time.sleep(d)
                     srv.submit(r.id, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max,
-                               window=rt.window)
+                               window=rt.window, predicted_bytes=rt.predicted_bytes)
 
             th = threading.Thread(target=producer)
             th.start()
@@ -379,6 +385,7 @@ def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 4
     # the saturated rate of the default setting, on a 3,000-request sample of the trace
     from anchorwave_b200 import autotune
     dt0, _, _ = run(None)
+    log(f"default setting saturated: {dt0:.1f} s")
     t_tune = time.perf_counter()
     (cfg["slots"], cfg["max_batch"]), trials = autotune.tune_serving(
         reqs, routes, mat, 4, 2, 24, 1, rate=SERVE_LOAD * len(reqs) / dt0, sample=3000, hbm_budget=SERVE_HBM_BUDGET)
@@ -387,9 +394,12 @@ def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 4
                              "seconds": time.perf_counter() - t_tune,
                              "trials": [{k: (round(v, 1) if isinstance(v, float) else v) for k, v in t.items()}
                                         for t in trials]}
+    log(f"tuned: {cfg}")
     dt_sat, st_sat, served = run(None, keep=set(sample))
     sat = len(reqs) / dt_sat
+    log(f"saturated: {dt_sat:.1f} s")
     dt, st, _ = run(SERVE_LOAD * sat)
+    log(f"80% load: {dt:.1f} s")
     # plain per-call GPU path on the sample, and its results against the served ones
     aligners = {}
     plain_s, same = 0.0, True
@@ -397,7 +407,10 @@ def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 4
         r, rt = reqs[i], routes[i]
         t1 = time.perf_counter()
         res = plain_route_call(rt, r.query, r.target, mat, aligners)
-        plain_s += time.perf_counter() - t1
+        dt1 = time.perf_counter() - t1
+        plain_s += dt1
+        if dt1 > 1.0:
+            log(f"plain call {i}: {rt.candidate} {len(r.query)}x{len(r.target)} {dt1:.1f} s")
         g = served[i]
         if rt.method in (0, 1):
             same &= (g.ksw[8], g.ksw[12]) == res

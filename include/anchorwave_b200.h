@@ -232,6 +232,18 @@ int wavefront_align_batch_gpu(wavefront_aligner_gpu_t *aligner, int n, const cha
  * wavefronts and packed-CIGAR blocks; the reference's align_status.memory_used,
  * WfaAlignment.cpp:353-354): the largest single alignment and the sum over the call. */
 int wavefront_gpu_memory(const wavefront_aligner_gpu_t *aligner, int64_t *pair_max, int64_t *total);
+/* High memory (standard and Singletrack): a pair whose wavefront grows wider than `width`
+ * diagonals, or wider than `tail_width` once every pair of the call has started and no more
+ * pairs run on warps than clusters fit on the device (the call's tail), leaves its
+ * warp and runs again from score 0 on a cluster of `cluster_ctas` CTAs (1..8) that spreads
+ * each wavefront over all of their threads; results are identical.  width 0: every pair
+ * stays on one warp; a negative value or cluster_ctas <= 0 keeps that setting.  Defaults:
+ * 8192, 1024 and 8.  Process-wide.  No counterpart in the reference (tuning knob). */
+void aw_set_wfa_wide(int width, int tail_width, int cluster_ctas);
+/* Kernel launches of the last call (every round and phase) and, of them, the cluster
+ * kernel's, with the number of pairs that moved to it. */
+int wavefront_gpu_last_launches(const wavefront_aligner_gpu_t *aligner, int *launches, int *cluster_launches,
+                                int *cluster_pairs);
 
 /* ---- selector sequence summary ------------------------------------------------- */
 
@@ -279,12 +291,16 @@ int64_t aw_sequence_summary_sketch_view(const uint64_t **hash, const uint32_t **
 /* A request's engine and its parameters, as the selection plan gives them
  * (src/myImportandFunction/AlignmentAlgorithmSelector.h:196-242): band (KSW2 band width, -1
  * = full; the initial band of score-certified KSW2), band_max (score-certified KSW2's largest
- * band) and window (the sliding-window width). */
+ * band), window (the sliding-window width) and predicted_bytes (the plan's memoryBytes
+ * estimate of the engine, AlignmentAlgorithmSelector.h:87; 0 = the server's own estimate),
+ * which the server uses for admission and to keep a WFA micro-batch within its wavefront
+ * pool. */
 typedef struct {
     int method;
     int band;
     int band_max;
     int64_t window;
+    int64_t predicted_bytes;
 } aw_serve_route_t;
 
 typedef struct {
@@ -391,6 +407,11 @@ void aw_set_tuning(int large_warps, int large_tlen_threshold);
 /* Target columns per lane of the banded kernel (4 or 8; 0 = chosen per batch from
  * its work and its longest pair).  No counterpart in the reference (tuning knob). */
 void aw_set_band_columns(int columns);
+/* 1 (default): a full-matrix pair that would be its batch's critical path (a long interval
+ * alone or among short ones) runs on the banded kernel at full width, whose strip pipeline
+ * spans all SMs; 0: every full-matrix pair runs on the full-matrix strip kernel.  Results
+ * are identical either way.  No counterpart in the reference (tuning knob). */
+void aw_set_full_pair_routing(int enabled);
 /* Frees the device and pinned buffers that the calling thread's KSW2 calls keep pooled
  * between calls (they grow to the largest batch seen; the next call re-creates them).
  * No counterpart in the reference (its work arrays are per call). */

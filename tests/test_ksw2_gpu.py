@@ -215,3 +215,21 @@ def test_exact_kernel_generic_scores(gpu, restatement):
             o = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, w=w, zdrop=200,
                                       flag=flag | (oracle.KSW_EZ_SINGLETRACK if st else 0), block=64)
             assert g.key() == o.key(), (i, L, w, hex(flag), st)
+
+
+@pytest.mark.parametrize("flag", [0, 0x02, 0x01, 0x800])
+def test_long_full_pair_on_the_banded_kernel(gpu, restatement, flag):
+    """A long full-matrix pair alone (the batch's critical path) runs on the banded kernel at
+    full width; with the routing off it runs on the strip kernel.  Both give the oracle's
+    ksw_extz_t and CIGAR."""
+    rng = np.random.default_rng(60 + flag)
+    q, t = W.divergent_pair(rng, 24000, 0.03, 0.06, 4.0)
+    mat = oracle.anchorwave_matrix(-4)
+    exp = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, 4, 2, 24, 1, flag=flag).key()
+    try:
+        for on in (True, False):
+            gpu.set_full_pair_routing(on)
+            assert gpu.ksw_extd2(q, t, mat, 4, 2, 24, 1, flag=flag).key() == exp, on
+            assert gpu.ksw_extd2_batch([q], [t], mat, 4, 2, 24, 1, flag=flag)[0].key() == exp, on
+    finally:
+        gpu.set_full_pair_routing(True)

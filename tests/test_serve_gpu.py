@@ -176,7 +176,8 @@ def test_selector_routes_reproduced(gpu):
     with serve.AlignmentServer(oracle.anchorwave_matrix(-4), *PEN, wfa_penalties=WPEN, slots=2,
                                max_batch=8) as srv:
         for r, rt in zip(reqs, routes):
-            srv.submit(r.id, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max, window=rt.window)
+            srv.submit(r.id, rt.method, r.query, r.target, band=rt.band, band_max=rt.band_max, window=rt.window,
+                       predicted_bytes=rt.predicted_bytes)
         got = _drain(srv, len(reqs))
     assert [g.id for g in got] == [r.id for r in reqs]
     for g, r, rt in zip(got, reqs, routes):

@@ -255,3 +255,58 @@ def test_align_with_medium_and_low_wfa(gpu, restatement):
         o = restatement.wfa_align(ts.encode(), qs.encode(), 4, 4, 2, 24, 1, False, memory_mode=mode)
         assert st == 0 and score == o[1]
         assert aq.replace("-", "") == qs and ar.replace("-", "") == ts
+
+
+@pytest.mark.parametrize("singletrack", [False, True])
+def test_wfa_cluster_kernel_identical(gpu, reference, singletrack):
+    """Pairs whose wavefronts outgrow the width threshold leave their warp for the cluster
+    kernel.  With the threshold lowered so that most pairs move, under clusters of 1, 2 and 8
+    CTAs, and under the tail rule alone, every result equals the warp kernel's and the
+    compiled WFA2-lib's."""
+    wfa = _wfa()
+    rng = np.random.default_rng(123 + int(singletrack))
+    ps, ts = [], []
+    for i in range(60):
+        L = int(np.exp(rng.uniform(np.log(50), np.log(6000))))
+        q, t = W.divergent_pair(rng, L, 0.02, 0.2, 4.0)
+        if i % 5 == 0 and len(q) > 400:  # one long deletion
+            at = int(rng.integers(0, len(q) - 300))
+            q = np.concatenate([q[:at], q[at + int(rng.integers(50, 300)):]])
+        if i % 7 == 3:
+            q = q.copy()
+            q[rng.integers(0, len(q), 3)] = 4
+        ps.append(W.to_ascii(t))
+        ts.append(W.to_ascii(q))
+    al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=singletrack)
+    try:
+        wfa.set_wide(0)
+        warp, _ = al.align_batch(ps, ts)
+        assert al.launches()[1] == 0
+        for width, tail, cl in ((16, 16, 1), (64, 64, 2), (256, 256, 8), (16, 16, 8), (1 << 30, 16, 8)):
+            wfa.set_wide(width, tail, cl)
+            got, _ = al.align_batch(ps, ts)
+            n_all, n_cluster, moved = al.launches()
+            # the tail rule moves only the pairs still running once few remain on warps
+            assert n_cluster >= 1 and moved >= (20 if width < (1 << 30) else 1), (width, tail, cl, moved)
+            assert got == warp, (width, tail, cl)
+    finally:
+        wfa.set_wide(8192, 1024, 8)
+        al.close()
+    for i in range(0, 60, 3):
+        assert warp[i] == reference.wfa_align(ps[i], ts[i], 4, 4, 2, 24, 1, singletrack=singletrack), i
+
+
+def test_wfa_cluster_kernel_long_pair(gpu, reference):
+    """A 20 kb pair at 15% divergence (wavefronts of tens of thousands of diagonals, several
+    per thread of an 8-CTA cluster) under the default threshold, standard and Singletrack,
+    against the compiled WFA2-lib."""
+    wfa = _wfa()
+    rng = np.random.default_rng(5)
+    q, t = W.divergent_pair(rng, 20000, 0.15, 0.15, 4.0)
+    p_, t_ = W.to_ascii(t), W.to_ascii(q)
+    for stk in (False, True):
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=stk)
+        got, _ = al.align_batch([p_], [t_])
+        assert al.launches()[2] == 1
+        al.close()
+        assert got[0] == reference.wfa_align(p_, t_, 4, 4, 2, 24, 1, singletrack=stk), stk
