@@ -20,7 +20,8 @@
 // Singletrack keeps only M and recycles I/D through a ring of max(e1,e2)+1 slots,
 // then reconstructs the path from M (:587-762).
 // Medium and low memory (the piggyback modes, wavefront/wavefront_compute_affine2p.c:110-282)
-// keep only the last max_score_scope scores in a ring of slots; every cell carries the
+// keep only the scores the compute step still reads (M: the last max_score_scope; I1/D1:
+// the last e1+1; I2/D2: the last e2+1) in rings of slots; every cell carries the
 // packed CIGAR of its latest operations and a link to the block that holds the earlier
 // ones, and a cell whose packed CIGAR reaches 15 operations moves it into a new block
 // (wavefront/wavefront_backtrace_offload.c); the traceback follows the links from the end
@@ -61,7 +62,6 @@ struct Alloc {
 // operation, newest lowest (1 deletion, 2 mismatch or gap close, 3 insertion).
 constexpr uint32_t PC_ALMOST_FULL = 0x10000000u;  // 15 operations or more
 constexpr uint32_t BT_NULL = 0xFFFFFFFFu;          // no earlier block
-constexpr int PIG_ARRAYS = 15;                     // 5 components x (offsets, pcigar, link)
 constexpr int PIG_U = 2;                           // diagonals per lane in flight
 constexpr uint32_t LANE_BLOCKS = 32;               // blocks a lane reserves at a time
 
@@ -115,6 +115,22 @@ struct HdrRing {
 __device__ __forceinline__ int32_t getv(const WfaArgs &A, const CompHdr &h, int k) {
     if (k < h.lo || k > h.hi) return WF_NULL;
     return ((const int32_t *)(A.pool + h.off))[k - h.base];
+}
+
+// An input wavefront of the compute step: its range and the address of its diagonal 0 (the
+// header's base folded in), so that a lane holds four values per input instead of six.
+struct InHdr {
+    int lo, hi;
+    const int32_t *p;
+};
+__device__ __forceinline__ InHdr in_hdr(const WfaArgs &A, const CompHdr &h) {
+    return InHdr{h.lo, h.hi, (const int32_t *)(A.pool + h.off) - h.base};
+}
+__device__ __forceinline__ int32_t getv(const InHdr &h, int k) {
+    return (k < h.lo || k > h.hi) ? WF_NULL : h.p[k];
+}
+__device__ __forceinline__ int32_t getv_l2(const InHdr &h, int k) {
+    return (k < h.lo || k > h.hi) ? WF_NULL : __ldcg(h.p + k);
 }
 
 // A piggyback cell: offset, packed CIGAR, link.  In a ring slot the three arrays of a
@@ -204,65 +220,57 @@ __device__ __forceinline__ bool any_of(const bool (&r)[N]) {
 template <int N>
 __device__ __forceinline__ void extend_n(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
                                          const uint8_t *txt, int k0, int stride, int32_t (&o)[N]) {
+    // o[u] is the text position h; the pattern position is h - k
     const int plen = PR.plen, tlen = PR.tlen;
-    int64_t v[N], h[N];
     bool run[N];
 #pragma unroll
-    for (int u = 0; u < N; ++u) {
-        const int k = k0 + stride * u;
-        run[u] = o[u] != WF_NULL;
-        v[u] = (int64_t)o[u] - k, h[u] = o[u];
-    }
+    for (int u = 0; u < N; ++u) run[u] = o[u] != WF_NULL;
     bool any = any_of(run);
     if (PR.packed) {
         // 32 bases per XOR; the run ends at the first differing base or at the end of either
         // sequence (the sentinels of the byte path)
-        int64_t rem[N];
 #pragma unroll
-        for (int u = 0; u < N; ++u) {
-            rem[u] = run[u] ? min((int64_t)plen - v[u], (int64_t)tlen - h[u]) : 0;
-            if (rem[u] <= 0) run[u] = false;
-        }
+        for (int u = 0; u < N; ++u)
+            if (run[u] && min(plen - (o[u] - (k0 + stride * u)), tlen - o[u]) <= 0) run[u] = false;
         any = any_of(run);
         while (any) {
             uint64_t x[N];
 #pragma unroll
             for (int u = 0; u < N; ++u)
-                x[u] = run[u] ? (load32b(A.ppat, PR.poff + v[u]) ^ load32b(A.ptxt, PR.toff + h[u])) : 0;
+                x[u] = run[u] ? (load32b(A.ppat, PR.poff + (o[u] - (k0 + stride * u))) ^ load32b(A.ptxt, PR.toff + o[u]))
+                              : 0;
             any = false;
 #pragma unroll
             for (int u = 0; u < N; ++u) {
                 if (!run[u]) continue;
-                int64_t nb = x[u] ? (int64_t)((__ffsll((long long)x[u]) - 1) >> 1) : 32;
-                const bool stop = x[u] != 0 || nb >= rem[u];
-                if (nb > rem[u]) nb = rem[u];
-                v[u] += nb, h[u] += nb, rem[u] -= nb;
-                if (stop || rem[u] == 0) run[u] = false;
+                const int rem = min(plen - (o[u] - (k0 + stride * u)), tlen - o[u]);
+                int nb = x[u] ? (__ffsll((long long)x[u]) - 1) >> 1 : 32;
+                const bool stop = x[u] != 0 || nb >= rem;
+                if (nb > rem) nb = rem;
+                o[u] += nb;
+                if (stop || rem == nb) run[u] = false;
                 else any = true;
             }
         }
+        return;
     }
     while (any) {
         uint64_t x[N];
 #pragma unroll
-        for (int u = 0; u < N; ++u) x[u] = run[u] ? (load8(pat, v[u]) ^ load8(txt, h[u])) : 0;
+        for (int u = 0; u < N; ++u) x[u] = run[u] ? (load8(pat, o[u] - (k0 + stride * u)) ^ load8(txt, o[u])) : 0;
         any = false;
 #pragma unroll
         for (int u = 0; u < N; ++u) {
             if (!run[u]) continue;
             if (x[u]) {
-                const int nb = (__ffsll((long long)x[u]) - 1) >> 3;
-                v[u] += nb, h[u] += nb;
+                o[u] += (__ffsll((long long)x[u]) - 1) >> 3;
                 run[u] = false;
             } else {
-                v[u] += 8, h[u] += 8;
+                o[u] += 8;
                 any = true;
             }
         }
     }
-#pragma unroll
-    for (int u = 0; u < N; ++u)
-        if (o[u] != WF_NULL) o[u] = (int32_t)h[u];
 }
 
 // The result of one pair (one thread): the backtrace of a pair that reached the end
@@ -467,8 +475,18 @@ __device__ void finish_pair(const WfaArgs &A, const WfaPairDev &PR, int idx, con
     A.out[idx] = o;
 }
 
+// Build-time tuning of the warp kernel: CTAs per SM the registers are sized for (4 warps
+// each), and diagonals per lane in flight in the high-memory compute step.
+#ifndef AW_WFA_MINB
+#define AW_WFA_MINB 3
+#endif
+#ifndef AW_WFA_WARP_U
+#define AW_WFA_WARP_U 4
+#endif
+constexpr int WU = AW_WFA_WARP_U;
+
 template <bool PIG>
-__global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
+__global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs) {
     const int lane = threadIdx.x & 31;
     const WfaPen P = A.pen;
     extern __shared__ ScoreHdr hring_all[];
@@ -487,13 +505,21 @@ __global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
         Alloc al{0, 0, true, 0};
         uint32_t bnext = 0, bend = 0;  // this lane's reserved piggyback blocks
         int status = 0, end_score = -1;
-        // piggyback ring: SR slots x 15 arrays x rcap elements; grows by reallocation
-        const int SR = A.max_score_scope;
+        // piggyback rings, each slot three arrays (offsets, packed CIGARs, links) of rcap
+        // elements: M keeps its last SR scores, I1/D1 their last e1+1 and I2/D2 their last
+        // e2+1 (the only scores the compute step reads them from); grown by reallocation
+        const int SR = A.max_score_scope, R1 = P.e1 + 1, R2 = P.e2 + 1;
+        const int64_t ring_arrays = 3 * (int64_t)(SR + 2 * R1 + 2 * R2);
+        auto pig_slot = [&](int c, int sc) -> int64_t {  // first array of component c at score sc
+            if (c == CM) return (int64_t)(sc % SR) * 3;
+            if (c <= CD1) return 3 * (int64_t)(SR + (sc % R1) * 2 + (c - CI1));
+            return 3 * (int64_t)(SR + 2 * R1 + (sc % R2) * 2 + (c - CI2));
+        };
         int rcap = 0;
         int64_t rbase = -1;
         if constexpr (PIG) {
             rcap = 32;
-            rbase = warp_alloc(A, al, (int64_t)SR * PIG_ARRAYS * rcap * 4, lane);
+            rbase = warp_alloc(A, al, ring_arrays * rcap * 4, lane);
             if (rbase < 0) status = WFA_RETRY;
         }
         // Singletrack ring for I/D: R slots x 4 components x cap offsets
@@ -642,7 +668,7 @@ __global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
             if constexpr (PIG) {
                 if (width > rcap) {
                     const int nc = max(2 * rcap, (width + 3) & ~3);
-                    const int64_t nb = warp_alloc(A, al, (int64_t)SR * PIG_ARRAYS * nc * 4, lane);
+                    const int64_t nb = warp_alloc(A, al, ring_arrays * nc * 4, lane);
                     if (nb < 0) {
                         status = WFA_RETRY;
                         break;
@@ -651,7 +677,7 @@ __global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
                 }
                 for (int c = 0; c < 5; ++c)
                     if (alloc_c[c])
-                        out[c] = CompHdr{lo, hi, lo, rcap, rbase + ((int64_t)(s % SR) * PIG_ARRAYS + c * 3) * rcap * 4};
+                        out[c] = CompHdr{lo, hi, lo, rcap, rbase + pig_slot(c, s) * rcap * 4};
             } else {
                 const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
                 int nstore = 1;
@@ -782,23 +808,26 @@ __global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
                 }
                 if (status != 0) break;
             } else {
-                // four diagonals per lane at a time: all input loads before any output store
-                for (int k0 = lo + lane; k0 <= hi; k0 += 128) {
-                    int32_t ins1[4], ins2[4], del1[4], del2[4], misms[4];
+                // WU diagonals per lane at a time: all input loads before any output store
+                const InHdr h_mm = in_hdr(A, m_misms), h_o1 = in_hdr(A, m_open1), h_i1 = in_hdr(A, i1),
+                            h_d1 = in_hdr(A, d1), h_o2 = in_hdr(A, m_open2), h_i2 = in_hdr(A, i2),
+                            h_d2 = in_hdr(A, d2);
+                for (int k0 = lo + lane; k0 <= hi; k0 += 32 * WU) {
+                    int32_t ins1[WU], ins2[WU], del1[WU], del2[WU], misms[WU];
     #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
+                    for (int u = 0; u < WU; ++u) {
                         const int k = k0 + 32 * u;
-                        ins1[u] = max(getv(A, m_open1, k - 1), getv(A, i1, k - 1)) + 1;
-                        ins2[u] = max(getv(A, m_open2, k - 1), getv(A, i2, k - 1)) + 1;
-                        del1[u] = max(getv(A, m_open1, k + 1), getv(A, d1, k + 1));
-                        del2[u] = max(getv(A, m_open2, k + 1), getv(A, d2, k + 1));
-                        misms[u] = getv(A, m_misms, k) + 1;
+                        ins1[u] = max(getv(h_o1, k - 1), getv(h_i1, k - 1)) + 1;
+                        ins2[u] = max(getv(h_o2, k - 1), getv(h_i2, k - 1)) + 1;
+                        del1[u] = max(getv(h_o1, k + 1), getv(h_d1, k + 1));
+                        del2[u] = max(getv(h_o2, k + 1), getv(h_d2, k + 1));
+                        misms[u] = getv(h_mm, k) + 1;
                     }
                     // the gap components are final: store them (and their trimmed ends) first, so
                     // that only M stays live across its extension
-                    int32_t mo[4];
+                    int32_t mo[WU];
     #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
+                    for (int u = 0; u < WU; ++u) {
                         const int k = k0 + 32 * u;
                         const int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
                         mo[u] = (k <= hi && in_matrix(best, k, plen, tlen)) ? best : WF_NULL;
@@ -816,9 +845,9 @@ __global__ void __launch_bounds__(128, 3) wfa_kernel(WfaArgs A, int rs) {
                     }
                     // then M[s], extended (the extend step of the next iteration, fused: the
                     // offsets never round-trip through memory unextended)
-                    extend_n<4>(A, PR, pat, txt, k0, 32, mo);
+                    extend_n<WU>(A, PR, pat, txt, k0, 32, mo);
     #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
+                    for (int u = 0; u < WU; ++u) {
                         const int k = k0 + 32 * u;
                         if (k > hi) break;
                         if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) fused_reached = true;
@@ -903,11 +932,6 @@ struct WidePlanner {
     int nchunks, cidx;   // chunks received, chunk being carved
     bool exhausted;
 };
-
-__device__ __forceinline__ int32_t getv_l2(const WfaArgs &A, const CompHdr &h, int k) {
-    if (k < h.lo || k > h.hi) return WF_NULL;
-    return __ldcg((const int32_t *)(A.pool + h.off) + (k - h.base));
-}
 
 __device__ __forceinline__ void part_reset(WidePart &p) {
     for (int c = 0; c < 5; ++c) p.kmin[c] = INT_MAX, p.kmax[c] = INT_MIN;
@@ -1130,8 +1154,9 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
             // ---- 1. this thread's diagonals of the planned score
             {
                 const int lo = plan.lo, hi = plan.hi, mask = plan.mask;
-                const CompHdr m_misms = plan.in[0], m_open1 = plan.in[1], i1 = plan.in[2], d1 = plan.in[3],
-                              m_open2 = plan.in[4], i2 = plan.in[5], d2 = plan.in[6];
+                const InHdr m_misms = in_hdr(A, plan.in[0]), m_open1 = in_hdr(A, plan.in[1]), i1 = in_hdr(A, plan.in[2]),
+                            d1 = in_hdr(A, plan.in[3]), m_open2 = in_hdr(A, plan.in[4]), i2 = in_hdr(A, plan.in[5]),
+                            d2 = in_hdr(A, plan.in[6]);
                 int32_t *oM = (int32_t *)(A.pool + plan.out[CM].off);
                 int32_t *oI1 = (mask & 2) ? (int32_t *)(A.pool + plan.out[CI1].off) : nullptr;
                 int32_t *oD1 = (mask & 4) ? (int32_t *)(A.pool + plan.out[CD1].off) : nullptr;
@@ -1146,11 +1171,11 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
 #pragma unroll
                     for (int u = 0; u < WIDE_U; ++u) {
                         const int k = k0 + GT * u;
-                        ins1[u] = max(getv_l2(A, m_open1, k - 1), getv_l2(A, i1, k - 1)) + 1;
-                        ins2[u] = max(getv_l2(A, m_open2, k - 1), getv_l2(A, i2, k - 1)) + 1;
-                        del1[u] = max(getv_l2(A, m_open1, k + 1), getv_l2(A, d1, k + 1));
-                        del2[u] = max(getv_l2(A, m_open2, k + 1), getv_l2(A, d2, k + 1));
-                        misms[u] = getv_l2(A, m_misms, k) + 1;
+                        ins1[u] = max(getv_l2(m_open1, k - 1), getv_l2(i1, k - 1)) + 1;
+                        ins2[u] = max(getv_l2(m_open2, k - 1), getv_l2(i2, k - 1)) + 1;
+                        del1[u] = max(getv_l2(m_open1, k + 1), getv_l2(d1, k + 1));
+                        del2[u] = max(getv_l2(m_open2, k + 1), getv_l2(d2, k + 1));
+                        misms[u] = getv_l2(m_misms, k) + 1;
                     }
                     int32_t mo[WIDE_U];
 #pragma unroll
