@@ -27,7 +27,7 @@ EXPORTS = [
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
     "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_graph", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_set_full_pair_routing",
-    "aw_set_wfa_wide", "wavefront_gpu_last_launches", "aw_release_thread_buffers",
+    "aw_set_wfa_wide", "aw_set_wfa_long", "wavefront_gpu_last_launches", "aw_release_thread_buffers",
     "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
     "aw_int32_peak_ops", "aw_int16x2_peak_ops", "aw_ksw_extd2_device_noalloc", "aw_cigar_rows_batch",
     "wavefront_aligner_new_gpu", "wavefront_aligner_delete_gpu", "wavefront_align_gpu", "wavefront_gpu_cigar",
@@ -123,6 +123,8 @@ def _load(path: str = LIB_PATH):
     lib.aw_set_band_columns.restype = None
     lib.aw_set_wfa_wide.argtypes = [i32, i32, i32]
     lib.aw_set_wfa_wide.restype = None
+    lib.aw_set_wfa_long.argtypes = [i32]
+    lib.aw_set_wfa_long.restype = None
     lib.wavefront_gpu_last_launches.argtypes = [C.c_void_p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     lib.wavefront_gpu_last_launches.restype = i32
     lib.aw_set_full_pair_routing.argtypes = [i32]

@@ -475,6 +475,301 @@ __device__ void finish_pair(const WfaArgs &A, const WfaPairDev &PR, int idx, con
     A.out[idx] = o;
 }
 
+// ---------------------------------------------------------------------------------------
+// Plans and partials shared by the CTA-cooperative mode below and the cluster kernel: the
+// plan of one score (its range, inputs and outputs) and, per CTA, the trimmed ends of each
+// component and whether the end cell was reached.
+enum { WOP_COMPUTE = 0, WOP_DONE = 1, WOP_EXIT = 2 };
+
+struct WidePlan {
+    int op, lo, hi, mask;  // mask: components allocated at the planned score (bit c)
+    CompHdr in[7];         // M[s-x], M[s-o1-e1], I1[s-e1], D1[s-e1], M[s-o2-e2], I2[s-e2], D2[s-e2]
+    CompHdr out[5];
+};
+struct WidePart {
+    int kmin[5], kmax[5], reached, pad;
+};
+
+__device__ __forceinline__ void part_reset(WidePart &p) {
+    for (int c = 0; c < 5; ++c) p.kmin[c] = INT_MAX, p.kmax[c] = INT_MIN;
+    p.reached = 0;
+}
+
+// The input headers of score s from the header ring (null below score 0).
+__device__ __forceinline__ void plan_inputs(const WfaArgs &A, const int64_t *ctab, const HdrRing &HR, int s,
+                                            CompHdr (&in)[7]) {
+    const WfaPen P = A.pen;
+    const CompHdr NUL{1, -1, 0, 0, 0};
+    const int sm = s - P.x, so1 = s - P.o1 - P.e1, se1 = s - P.e1, so2 = s - P.o2 - P.e2, se2 = s - P.e2;
+    in[0] = sm >= 0 ? HR.get(A, ctab, sm, s)->c[CM] : NUL;
+    in[1] = so1 >= 0 ? HR.get(A, ctab, so1, s)->c[CM] : NUL;
+    in[2] = se1 >= 0 ? HR.get(A, ctab, se1, s)->c[CI1] : NUL;
+    in[3] = se1 >= 0 ? HR.get(A, ctab, se1, s)->c[CD1] : NUL;
+    in[4] = so2 >= 0 ? HR.get(A, ctab, so2, s)->c[CM] : NUL;
+    in[5] = se2 >= 0 ? HR.get(A, ctab, se2, s)->c[CI2] : NUL;
+    in[6] = se2 >= 0 ? HR.get(A, ctab, se2, s)->c[CD2] : NUL;
+}
+
+// The limits of the compute step over its inputs (null inputs contribute lo=1, hi=-1) and
+// which I/D outputs exist (one of their inputs exists).
+__device__ __forceinline__ void plan_limits(const CompHdr (&in)[7], int &lo, int &hi, int &mask) {
+    bool isnull[7];
+    for (int j = 0; j < 7; ++j) isnull[j] = in[j].lo > in[j].hi;
+    lo = in[0].lo, hi = in[0].hi;
+    lo = min(lo, in[1].lo - 1), hi = max(hi, in[1].hi + 1);
+    lo = min(lo, in[2].lo + 1), hi = max(hi, in[2].hi + 1);
+    lo = min(lo, in[3].lo - 1), hi = max(hi, in[3].hi - 1);
+    lo = min(lo, in[4].lo - 1), hi = max(hi, in[4].hi + 1);
+    lo = min(lo, in[5].lo + 1), hi = max(hi, in[5].hi + 1);
+    lo = min(lo, in[6].lo - 1), hi = max(hi, in[6].hi - 1);
+    mask = 1;
+    if (!isnull[1] || !isnull[2]) mask |= 1 << CI1;
+    if (!isnull[1] || !isnull[3]) mask |= 1 << CD1;
+    if (!isnull[4] || !isnull[5]) mask |= 1 << CI2;
+    if (!isnull[4] || !isnull[6]) mask |= 1 << CD2;
+}
+
+// One thread's diagonals lo + g0 + G*u of a planned score (high memory): the compute step,
+// the fused extension of M, the stores, and this thread's trimmed ends and end check, folded
+// per warp into the CTA's partials.  `ld_l2` reads the inputs through L2 (other CTAs wrote them).
+template <bool L2>
+__device__ __forceinline__ void plan_compute(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
+                                             const uint8_t *txt, const WidePlan &Q, int g0, int G, WidePart &pp) {
+    const int plen = PR.plen, tlen = PR.tlen, k_end = tlen - plen, lane = threadIdx.x & 31;
+    const int lo = Q.lo, hi = Q.hi, mask = Q.mask;
+    const InHdr m_misms = in_hdr(A, Q.in[0]), m_open1 = in_hdr(A, Q.in[1]), i1 = in_hdr(A, Q.in[2]),
+                d1 = in_hdr(A, Q.in[3]), m_open2 = in_hdr(A, Q.in[4]), i2 = in_hdr(A, Q.in[5]),
+                d2 = in_hdr(A, Q.in[6]);
+    int32_t *oM = (int32_t *)(A.pool + Q.out[CM].off);
+    int32_t *oI1 = (mask & 2) ? (int32_t *)(A.pool + Q.out[CI1].off) : nullptr;
+    int32_t *oD1 = (mask & 4) ? (int32_t *)(A.pool + Q.out[CD1].off) : nullptr;
+    int32_t *oI2 = (mask & 8) ? (int32_t *)(A.pool + Q.out[CI2].off) : nullptr;
+    int32_t *oD2 = (mask & 16) ? (int32_t *)(A.pool + Q.out[CD2].off) : nullptr;
+    int kmin[5], kmax[5];
+    bool reached = false;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
+    constexpr int U = 4;
+    for (int k0 = lo + g0; k0 <= hi; k0 += G * U) {
+        int32_t ins1[U], ins2[U], del1[U], del2[U], misms[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + G * u;
+            if constexpr (L2) {
+                ins1[u] = max(getv_l2(m_open1, k - 1), getv_l2(i1, k - 1)) + 1;
+                ins2[u] = max(getv_l2(m_open2, k - 1), getv_l2(i2, k - 1)) + 1;
+                del1[u] = max(getv_l2(m_open1, k + 1), getv_l2(d1, k + 1));
+                del2[u] = max(getv_l2(m_open2, k + 1), getv_l2(d2, k + 1));
+                misms[u] = getv_l2(m_misms, k) + 1;
+            } else {
+                ins1[u] = max(getv(m_open1, k - 1), getv(i1, k - 1)) + 1;
+                ins2[u] = max(getv(m_open2, k - 1), getv(i2, k - 1)) + 1;
+                del1[u] = max(getv(m_open1, k + 1), getv(d1, k + 1));
+                del2[u] = max(getv(m_open2, k + 1), getv(d2, k + 1));
+                misms[u] = getv(m_misms, k) + 1;
+            }
+        }
+        int32_t mo[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + G * u;
+            const int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
+            mo[u] = (k <= hi && in_matrix(best, k, plen, tlen)) ? best : WF_NULL;
+            if (k > hi) continue;
+            if (oI1) oI1[k - lo] = ins1[u];
+            if (oD1) oD1[k - lo] = del1[u];
+            if (oI2) oI2[k - lo] = ins2[u];
+            if (oD2) oD2[k - lo] = del2[u];
+            const int32_t vals[4] = {ins1[u], del1[u], ins2[u], del2[u]};
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (in_matrix(vals[c], k, plen, tlen)) kmin[c + 1] = min(kmin[c + 1], k), kmax[c + 1] = max(kmax[c + 1], k);
+            if (mo[u] != WF_NULL) kmin[CM] = min(kmin[CM], k), kmax[CM] = max(kmax[CM], k);
+        }
+        extend_n<U>(A, PR, pat, txt, k0, G, mo);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + G * u;
+            if (k > hi) break;
+            if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) reached = true;
+            oM[k - lo] = mo[u];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const int th = __reduce_max_sync(0xffffffffu, kmax[c]);
+        const int tl = __reduce_min_sync(0xffffffffu, kmin[c]);
+        if (lane == 0 && th != INT_MIN) atomicMax(&pp.kmax[c], th), atomicMin(&pp.kmin[c], tl);
+    }
+    if (__any_sync(0xffffffffu, reached) && lane == 0) pp.reached = 1;
+}
+
+// Thread-0 bump allocation for the CTA-cooperative mode.
+__device__ int64_t cta_alloc(const WfaArgs &A, Alloc &al, int64_t bytes) {
+    bytes = (bytes + 15) & ~(int64_t)15;
+    if (!al.ok) return -1;
+    if (al.cur + bytes > al.end) {
+        const int64_t sz = bytes > DATA_CHUNK ? bytes : DATA_CHUNK;
+        const int64_t b = pool_grab(A, sz);
+        if (b < 0) {
+            al.ok = false;
+            return -1;
+        }
+        al.cur = b, al.end = b + sz, al.used += sz;
+    }
+    const int64_t r = al.cur;
+    al.cur += bytes;
+    return r;
+}
+
+// CTA-cooperative mode (high memory): one long pair on all threads of a CTA.  Thread 0 plans
+// every score (the headers in the CTA's header ring and the pool, the allocations) and all
+// threads compute and extend the diagonals lo + tid + NT*u; two CTA barriers per score.  A
+// pair whose wavefront grows too wide stops with WFA_WIDE for the cluster kernel.  The cell arithmetic, the limits, the trimming and the backtrace are the warp's.
+__device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan &plan, WidePart &part) {
+    const int tid = threadIdx.x, NT = blockDim.x;
+    const WfaPen P = A.pen;
+    const WfaPairDev PR = A.pairs[idx];
+    const int plen = PR.plen, tlen = PR.tlen;
+    const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
+    int64_t *ctab = A.ctab + PR.ctab_off;
+    const CompHdr NUL{1, -1, 0, 0, 0};
+    // thread 0's state
+    int s = 0, num_null = 0, status = 0, end_score = -1;
+    const int smax = PR.ctab_cap * HDR_CHUNK - 1;
+    const int R = (P.e1 > P.e2 ? P.e1 : P.e2) + 1, ring_cap = plen + tlen + 8;
+    int64_t ring = -1;
+    Alloc al{0, 0, true, 0};
+    auto set_hdr = [&](int sc, const CompHdr (&o)[5]) {
+        ScoreHdr *OH = hdr_ptr(A, ctab, sc);
+        for (int c = 0; c < 5; ++c) OH->c[c] = o[c];
+        if (HR.rs)
+            for (int c = 0; c < 5; ++c) HR.ring[sc & (HR.rs - 1)].c[c] = o[c];
+    };
+    auto plan_next = [&]() {
+        for (;;) {
+            ++s;
+            if (s > smax) {
+                status = WFA_OVERFLOW;
+                break;
+            }
+            if (s % HDR_CHUNK == 0) {
+                const int64_t hb = cta_alloc(A, al, (int64_t)sizeof(ScoreHdr) * HDR_CHUNK);
+                if (hb < 0) {
+                    status = WFA_RETRY;
+                    break;
+                }
+                ctab[s / HDR_CHUNK] = hb;
+            }
+            CompHdr in[7];
+            plan_inputs(A, ctab, HR, s, in);
+            bool all_null = true;
+            for (int j = 0; j < 7; ++j) all_null &= in[j].lo > in[j].hi;
+            if (all_null) {
+                const CompHdr o[5] = {NUL, NUL, NUL, NUL, NUL};
+                set_hdr(s, o);
+                if (++num_null > A.max_score_scope) {  // the top of the next step: M[s] is empty
+                    status = -3;
+                    break;
+                }
+                continue;
+            }
+            num_null = 0;
+            int lo, hi, mask;
+            plan_limits(in, lo, hi, mask);
+            const int width = hi - lo + 1;
+            // a wavefront too wide for the CTA: the cluster kernel re-runs the pair (past
+            // wide_width_cta always; past wide_width_tail in the call's tail, checked every 32
+            // scores: every pair started and few still running)
+            if (A.wide_width_cta > 0 && width > A.wide_width_tail) {
+                bool wide = width > A.wide_width_cta;
+                if (!wide && (s & 31) == 0)
+                    wide = *(volatile int32_t *)(A.queue + 2) >= A.n_long && *(volatile int32_t *)A.queue >= A.n &&
+                           *(volatile int32_t *)(A.queue + 1) <= A.wide_tail_pairs;
+                if (wide) {
+                    status = WFA_WIDE;
+                    break;
+                }
+            }
+            if (A.singletrack && width > ring_cap) {
+                status = WFA_OVERFLOW;
+                break;
+            }
+            const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
+            const int64_t blk = cta_alloc(A, al, wb * (A.singletrack ? 1 : __popc(mask)));
+            if (blk < 0) {
+                status = WFA_RETRY;
+                break;
+            }
+            int64_t o = blk;
+            for (int c = 0; c < 5; ++c) {
+                plan.out[c] = NUL;
+                if (!(mask & (1 << c))) continue;
+                int64_t place;
+                if (c == CM || !A.singletrack) place = o, o += wb;
+                else place = ring + ((int64_t)((s % R) * 4 + (c - 1)) * ring_cap) * 4;
+                plan.out[c] = CompHdr{lo, hi, lo, 0, place};
+            }
+            for (int j = 0; j < 7; ++j) plan.in[j] = in[j];
+            plan.op = WOP_COMPUTE, plan.lo = lo, plan.hi = hi, plan.mask = mask;
+            return;
+        }
+        plan.op = WOP_DONE;
+    };
+    if (tid == 0) {
+        atomicAdd(A.queue + 1, 1);  // pairs running
+        part_reset(part);
+        if (A.singletrack) {
+            ring = cta_alloc(A, al, (int64_t)R * 4 * ring_cap * 4);
+            if (ring < 0) status = WFA_RETRY;
+        }
+        const int64_t h0 = status == 0 ? cta_alloc(A, al, (int64_t)sizeof(ScoreHdr) * HDR_CHUNK) : -1;
+        const int64_t d0 = h0 >= 0 ? cta_alloc(A, al, 16) : -1;
+        if (status == 0 && d0 < 0) status = WFA_RETRY;
+        if (status == 0) {
+            // M[0] = {0} on diagonal 0, extended
+            const int32_t o0 = (int32_t)lcp1(A, PR, pat, txt, 0, 0);
+            ctab[0] = h0;
+            *(int32_t *)(A.pool + d0) = o0;
+            const CompHdr o[5] = {CompHdr{0, 0, 0, 0, d0}, NUL, NUL, NUL, NUL};
+            set_hdr(0, o);
+            if (tlen - plen == 0 && o0 >= tlen) end_score = 0;
+        }
+        if (status != 0 || end_score == 0) plan.op = WOP_DONE;
+        else plan_next();
+    }
+    __syncthreads();
+    while (plan.op == WOP_COMPUTE) {
+        plan_compute<false>(A, PR, pat, txt, plan, tid, NT, part);
+        __syncthreads();
+        if (tid == 0) {
+            CompHdr out[5];
+            for (int c = 0; c < 5; ++c) {
+                out[c] = plan.out[c];
+                if (!(plan.mask & (1 << c))) continue;
+                // no diagonal in the matrix: the empty range [lo, lo-1] of the scan
+                if (part.kmax[c] == INT_MIN) out[c].hi = out[c].lo - 1;
+                else out[c].lo = part.kmin[c], out[c].hi = part.kmax[c];
+            }
+            const bool reached = part.reached != 0;
+            part_reset(part);
+            set_hdr(s, out);
+            if (reached) {
+                end_score = s;
+                plan.op = WOP_DONE;
+            } else {
+                plan_next();
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        finish_pair<false>(A, PR, idx, pat, txt, ctab, HR, status, end_score, s, al.used);
+        atomicSub(A.queue + 1, 1);
+    }
+    __syncthreads();
+}
+
 // Build-time tuning of the warp kernel: CTAs per SM the registers are sized for (4 warps
 // each), and diagonals per lane in flight in the high-memory compute step.
 #ifndef AW_WFA_MINB
@@ -490,6 +785,21 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
     const int lane = threadIdx.x & 31;
     const WfaPen P = A.pen;
     extern __shared__ ScoreHdr hring_all[];
+    if constexpr (!PIG) {
+        // the long pairs first, each on the whole CTA (warp 0's header ring serves the
+        // planner; the warps take their own rings afterwards)
+        __shared__ WidePlan cplan;
+        __shared__ WidePart cpart;
+        __shared__ int cpi;
+        for (;;) {
+            if (threadIdx.x == 0) cpi = A.n_long > 0 ? atomicAdd(A.queue + 2, 1) : A.n_long;
+            __syncthreads();
+            const int pi = cpi;
+            __syncthreads();
+            if (pi >= A.n_long) break;
+            cta_pair(A, A.order_long[pi], HdrRing{hring_all, rs}, cplan, cpart);
+        }
+    }
     const HdrRing HR{hring_all + (threadIdx.x >> 5) * rs, rs};
     for (;;) {
         int pi = 0;
@@ -905,16 +1215,6 @@ constexpr int WIDE_NT = 384;
 constexpr int WIDE_U = 4;
 constexpr int WIDE_CHUNKS = 8;  // reserve chunks a planner keeps track of (a ring)
 
-enum { WOP_COMPUTE = 0, WOP_DONE = 1, WOP_EXIT = 2 };
-
-struct WidePlan {
-    int op, lo, hi, mask;  // mask: components allocated at the planned score (bit c)
-    CompHdr in[7];         // M[s-x], M[s-o1-e1], I1[s-e1], D1[s-e1], M[s-o2-e2], I2[s-e2], D2[s-e2]
-    CompHdr out[5];
-};
-struct WidePart {
-    int kmin[5], kmax[5], reached, pad;
-};
 // A reserve chunk announced by the leader: for pair `tag`, the planners' chunk number `seq`
 // (off < 0: the pool is exhausted).
 struct WideAnn {
@@ -932,11 +1232,6 @@ struct WidePlanner {
     int nchunks, cidx;   // chunks received, chunk being carved
     bool exhausted;
 };
-
-__device__ __forceinline__ void part_reset(WidePart &p) {
-    for (int c = 0; c < 5; ++c) p.kmin[c] = INT_MAX, p.kmax[c] = INT_MIN;
-    p.reached = 0;
-}
 
 // Reserve chunk size: large (few pool atomics), smaller in a small pool.
 __device__ __forceinline__ int64_t wide_chunk(const WfaArgs &A, int64_t need) {
@@ -1025,17 +1320,10 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
                 W.hdr_off = hb;
                 if (leader) A.ctab[W.ctab_off + s / HDR_CHUNK] = hb;
             }
-            const int sm = s - P.x, so1 = s - P.o1 - P.e1, se1 = s - P.e1, so2 = s - P.o2 - P.e2, se2 = s - P.e2;
             CompHdr in[7];
-            in[0] = sm >= 0 ? HR.ring[sm & (HR.rs - 1)].c[CM] : NUL;
-            in[1] = so1 >= 0 ? HR.ring[so1 & (HR.rs - 1)].c[CM] : NUL;
-            in[2] = se1 >= 0 ? HR.ring[se1 & (HR.rs - 1)].c[CI1] : NUL;
-            in[3] = se1 >= 0 ? HR.ring[se1 & (HR.rs - 1)].c[CD1] : NUL;
-            in[4] = so2 >= 0 ? HR.ring[so2 & (HR.rs - 1)].c[CM] : NUL;
-            in[5] = se2 >= 0 ? HR.ring[se2 & (HR.rs - 1)].c[CI2] : NUL;
-            in[6] = se2 >= 0 ? HR.ring[se2 & (HR.rs - 1)].c[CD2] : NUL;
-            bool isnull[7], all_null = true;
-            for (int j = 0; j < 7; ++j) isnull[j] = in[j].lo > in[j].hi, all_null &= isnull[j];
+            plan_inputs(A, A.ctab + W.ctab_off, HR, s, in);
+            bool all_null = true;
+            for (int j = 0; j < 7; ++j) all_null &= in[j].lo > in[j].hi;
             if (all_null) {
                 const CompHdr o[5] = {NUL, NUL, NUL, NUL, NUL};
                 set_hdr(s, o);
@@ -1047,20 +1335,11 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
                 continue;
             }
             W.num_null = 0;
-            int lo = in[0].lo, hi = in[0].hi;
-            lo = min(lo, in[1].lo - 1), hi = max(hi, in[1].hi + 1);
-            lo = min(lo, in[2].lo + 1), hi = max(hi, in[2].hi + 1);
-            lo = min(lo, in[3].lo - 1), hi = max(hi, in[3].hi - 1);
-            lo = min(lo, in[4].lo - 1), hi = max(hi, in[4].hi + 1);
-            lo = min(lo, in[5].lo + 1), hi = max(hi, in[5].hi + 1);
-            lo = min(lo, in[6].lo - 1), hi = max(hi, in[6].hi - 1);
+            int lo, hi, mask;
+            plan_limits(in, lo, hi, mask);
             W.lo_all = min(W.lo_all, lo), W.hi_all = max(W.hi_all, hi);
-            const bool alloc_c[5] = {true, !isnull[1] || !isnull[2], !isnull[1] || !isnull[3],
-                                     !isnull[4] || !isnull[5], !isnull[4] || !isnull[6]};
             const int width = hi - lo + 1;
             const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
-            int mask = 0;
-            for (int c = 0; c < 5; ++c) mask |= alloc_c[c] ? 1 << c : 0;
             const int nstore = A.singletrack ? 1 : __popc(mask);
             if (A.singletrack && width > W.ring_cap) {
                 W.status = WFA_OVERFLOW;
@@ -1074,7 +1353,7 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
             int64_t o = blk;
             for (int c = 0; c < 5; ++c) {
                 plan.out[c] = NUL;
-                if (!alloc_c[c]) continue;
+                if (!(mask & (1 << c))) continue;
                 int64_t place;
                 if (c == CM || !A.singletrack) place = o, o += wb;
                 else place = W.ring + ((int64_t)((s % W.R) * 4 + (c - 1)) * W.ring_cap) * 4;
@@ -1152,67 +1431,7 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
         const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
         while (op == WOP_COMPUTE) {
             // ---- 1. this thread's diagonals of the planned score
-            {
-                const int lo = plan.lo, hi = plan.hi, mask = plan.mask;
-                const InHdr m_misms = in_hdr(A, plan.in[0]), m_open1 = in_hdr(A, plan.in[1]), i1 = in_hdr(A, plan.in[2]),
-                            d1 = in_hdr(A, plan.in[3]), m_open2 = in_hdr(A, plan.in[4]), i2 = in_hdr(A, plan.in[5]),
-                            d2 = in_hdr(A, plan.in[6]);
-                int32_t *oM = (int32_t *)(A.pool + plan.out[CM].off);
-                int32_t *oI1 = (mask & 2) ? (int32_t *)(A.pool + plan.out[CI1].off) : nullptr;
-                int32_t *oD1 = (mask & 4) ? (int32_t *)(A.pool + plan.out[CD1].off) : nullptr;
-                int32_t *oI2 = (mask & 8) ? (int32_t *)(A.pool + plan.out[CI2].off) : nullptr;
-                int32_t *oD2 = (mask & 16) ? (int32_t *)(A.pool + plan.out[CD2].off) : nullptr;
-                int kmin[5], kmax[5];
-                bool reached = false;
-#pragma unroll
-                for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
-                for (int k0 = lo + gtid; k0 <= hi; k0 += GT * WIDE_U) {
-                    int32_t ins1[WIDE_U], ins2[WIDE_U], del1[WIDE_U], del2[WIDE_U], misms[WIDE_U];
-#pragma unroll
-                    for (int u = 0; u < WIDE_U; ++u) {
-                        const int k = k0 + GT * u;
-                        ins1[u] = max(getv_l2(m_open1, k - 1), getv_l2(i1, k - 1)) + 1;
-                        ins2[u] = max(getv_l2(m_open2, k - 1), getv_l2(i2, k - 1)) + 1;
-                        del1[u] = max(getv_l2(m_open1, k + 1), getv_l2(d1, k + 1));
-                        del2[u] = max(getv_l2(m_open2, k + 1), getv_l2(d2, k + 1));
-                        misms[u] = getv_l2(m_misms, k) + 1;
-                    }
-                    int32_t mo[WIDE_U];
-#pragma unroll
-                    for (int u = 0; u < WIDE_U; ++u) {
-                        const int k = k0 + GT * u;
-                        const int32_t best = max(max(del1[u], del2[u]), max(misms[u], max(ins1[u], ins2[u])));
-                        mo[u] = (k <= hi && in_matrix(best, k, plen, tlen)) ? best : WF_NULL;
-                        if (k > hi) continue;
-                        if (oI1) oI1[k - lo] = ins1[u];
-                        if (oD1) oD1[k - lo] = del1[u];
-                        if (oI2) oI2[k - lo] = ins2[u];
-                        if (oD2) oD2[k - lo] = del2[u];
-                        const int32_t vals[4] = {ins1[u], del1[u], ins2[u], del2[u]};
-#pragma unroll
-                        for (int c = 0; c < 4; ++c)
-                            if (in_matrix(vals[c], k, plen, tlen))
-                                kmin[c + 1] = min(kmin[c + 1], k), kmax[c + 1] = max(kmax[c + 1], k);
-                        if (mo[u] != WF_NULL) kmin[CM] = min(kmin[CM], k), kmax[CM] = max(kmax[CM], k);
-                    }
-                    extend_n<WIDE_U>(A, PR, pat, txt, k0, GT, mo);
-#pragma unroll
-                    for (int u = 0; u < WIDE_U; ++u) {
-                        const int k = k0 + GT * u;
-                        if (k > hi) break;
-                        if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) reached = true;
-                        oM[k - lo] = mo[u];
-                    }
-                }
-                WidePart &pp = part[it & 1];
-#pragma unroll
-                for (int c = 0; c < 5; ++c) {
-                    const int th = __reduce_max_sync(0xffffffffu, kmax[c]);
-                    const int tl = __reduce_min_sync(0xffffffffu, kmin[c]);
-                    if (lane == 0 && th != INT_MIN) atomicMax(&pp.kmax[c], th), atomicMin(&pp.kmin[c], tl);
-                }
-                if (__any_sync(0xffffffffu, reached) && lane == 0) pp.reached = 1;
-            }
+            plan_compute<true>(A, PR, pat, txt, plan, gtid, GT, part[it & 1]);
             // the leader reserves the next plan's space ahead of need
             if (leader && !W.exhausted && W.nchunks - W.cidx < WIDE_CHUNKS - 1 && !reserve_ok()) {
                 const int64_t len = wide_chunk(A, need_next());

@@ -47,6 +47,8 @@ int64_t al8(int64_t v) { return (v + 7) & ~(int64_t)7; }
 std::atomic<int> g_wide_width{8192};
 std::atomic<int> g_wide_tail{1024};
 std::atomic<int> g_wide_cluster{8};
+// Pairs with pattern + text length from which a pair runs on a whole CTA (aw_set_wfa_long).
+std::atomic<int> g_long_sum{3072};
 
 }  // namespace
 
@@ -177,6 +179,9 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     W.wide_width = wide_clusters > 0 ? std::max(0, g_wide_width.load()) : 0;
     W.wide_width_tail = std::min(W.wide_width, std::max(0, g_wide_tail.load()));
     W.wide_tail_pairs = std::max(1, wide_clusters);
+    W.wide_width_cta = W.wide_width;
+    const int64_t long_sum = W.piggyback ? 0 : g_long_sum.load();
+    std::vector<int32_t> staged;
     // Rounds: every round restarts the pool and runs up to `chunk` pending pairs, largest
     // first; pairs that found the pool exhausted stay pending.  A round that completes
     // nothing halves the chunk (the pairs in flight together share the pool), one that
@@ -192,15 +197,31 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
         while (!pending.empty()) {
             const size_t take = std::min(chunk, pending.size());
             std::vector<int32_t> batch(pending.begin(), pending.begin() + (std::ptrdiff_t)take);
-            WCUDA(cudaMemcpyAsync(al->d_order.p, batch.data(), sizeof(int32_t) * batch.size(), cudaMemcpyHostToDevice,
+            // warp phase: the long pairs (still largest first) ahead of the others, each taken by
+            // a whole CTA before the CTAs' warps take the others one each
+            int32_t n_long = 0;
+            staged.clear();
+            if (phase == 0 && long_sum > 0) {
+                for (int32_t i : batch)
+                    if ((int64_t)plen[i] + tlen[i] >= long_sum) staged.push_back(i);
+                n_long = (int32_t)staged.size();
+                for (int32_t i : batch)
+                    if ((int64_t)plen[i] + tlen[i] < long_sum) staged.push_back(i);
+            } else {
+                staged = batch;
+            }
+            WCUDA(cudaMemcpyAsync(al->d_order.p, staged.data(), sizeof(int32_t) * staged.size(), cudaMemcpyHostToDevice,
                                   al->st));
-            WCUDA(cudaMemsetAsync(al->d_queue.p, 0, 8, al->st));
+            WCUDA(cudaMemsetAsync(al->d_queue.p, 0, 16, al->st));
             WCUDA(cudaMemsetAsync(al->d_head.p, 0, 8, al->st));
-            W.order = al->d_order.as<int32_t>();
-            W.n = (int32_t)batch.size();
+            W.order_long = al->d_order.as<int32_t>();
+            W.n_long = n_long;
+            W.order = al->d_order.as<int32_t>() + n_long;
+            W.n = (int32_t)staged.size() - n_long;
             WCUDA(cudaEventRecord(al->e0, al->st));
             if (phase == 0) {
-                WCUDA(launch_wfa(W, std::min((W.n + 3) / 4, occ * al->sms), al->st));
+                const int ctas = std::max(1, std::min(std::max((W.n + 3) / 4, W.n_long), occ * al->sms));
+                WCUDA(launch_wfa(W, ctas, al->st));
             } else {
                 ++al->last_cluster_launches;
                 WCUDA(launch_wfa_wide(W, std::min(W.n, wide_clusters), cl, al->st));
@@ -301,6 +322,10 @@ int wavefront_gpu_last_launches(const wavefront_aligner_gpu_t *al, int *launches
     if (cluster_launches) *cluster_launches = al->last_cluster_launches;
     if (cluster_pairs) *cluster_pairs = al->last_cluster_pairs;
     return AW_OK;
+}
+
+void aw_set_wfa_long(int min_length_sum) {
+    if (min_length_sum >= 0) g_long_sum.store(min_length_sum);
 }
 
 void aw_set_wfa_wide(int width, int tail_width, int cluster_ctas) {

@@ -37,13 +37,16 @@ struct WfaArgs {
     const WfaPairDev *pairs;
     const int32_t *order;
     int32_t n;
+    const int32_t *order_long;  // pairs each run on a whole CTA first (high memory), n_long of them
+    int32_t n_long;
     uint8_t *pool;
     int64_t pool_bytes;
     unsigned long long *pool_head;
     int64_t *ctab;
     char *ops;
     WfaOutDev *out;
-    int32_t *queue;       // [0] next position of `order`, [1] pairs running on warps
+    int32_t *queue;       // [0] next position of `order`, [1] pairs running on warps,
+                          // [2] next position of `order_long`
     WfaPen pen;
     int singletrack;
     int piggyback;        // medium / low memory: ring of recent scores + packed-CIGAR blocks
@@ -51,6 +54,7 @@ struct WfaArgs {
     int wide_width;       // warp kernel: a pair whose wavefront grows wider stops with WFA_WIDE (0 = never)
     int wide_width_tail;  // the same once every pair has started and at most wide_tail_pairs
     int wide_tail_pairs;  // still run on warps (<= wide_width)
+    int wide_width_cta;   // a pair on a whole CTA whose wavefront grows wider stops with WFA_WIDE
 };
 
 cudaError_t launch_wfa(const WfaArgs &a, int ctas, cudaStream_t st);

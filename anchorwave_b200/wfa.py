@@ -37,6 +37,12 @@ def set_wide(width: int = -1, tail_width: int = -1, cluster_ctas: int = 0) -> No
     lib.aw_set_wfa_wide(int(width), int(tail_width), int(cluster_ctas))
 
 
+def set_long(min_length_sum: int) -> None:
+    """aw_set_wfa_long: pairs whose lengths sum to at least this run first on a whole CTA each
+    (high memory; 0 = every pair on one warp).  Results are identical under every setting."""
+    lib.aw_set_wfa_long(int(min_length_sum))
+
+
 def positive_penalty(p: int) -> int:
     """AnchorWave passes negative penalties; WFA takes their magnitude (WfaAlignment.cpp:298-302)."""
     return -p if p < 0 else p

@@ -240,6 +240,12 @@ int wavefront_gpu_memory(const wavefront_aligner_gpu_t *aligner, int64_t *pair_m
  * stays on one warp; a negative value or cluster_ctas <= 0 keeps that setting.  Defaults:
  * 8192, 1024 and 8.  Process-wide.  No counterpart in the reference (tuning knob). */
 void aw_set_wfa_wide(int width, int tail_width, int cluster_ctas);
+/* High memory: pairs whose pattern and text lengths sum to at least `min_length_sum` run
+ * first, each on all four warps of a CTA (the longest pairs of a batch otherwise set its
+ * duration, one warp each); the others then run one per warp.  0: every pair starts on one
+ * warp.  Default 3072.  A CTA's pair moves to the cluster kernel by the widths of
+ * aw_set_wfa_wide, as a warp's does.  Results are identical.  Process-wide. */
+void aw_set_wfa_long(int min_length_sum);
 /* Kernel launches of the last call (every round and phase) and, of them, the cluster
  * kernel's, with the number of pairs that moved to it. */
 int wavefront_gpu_last_launches(const wavefront_aligner_gpu_t *aligner, int *launches, int *cluster_launches,

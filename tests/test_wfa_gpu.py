@@ -310,3 +310,38 @@ def test_wfa_cluster_kernel_long_pair(gpu, reference):
         assert al.launches()[2] == 1
         al.close()
         assert got[0] == reference.wfa_align(p_, t_, 4, 4, 2, 24, 1, singletrack=stk), stk
+
+
+@pytest.mark.parametrize("singletrack", [False, True])
+def test_wfa_long_pairs_on_whole_ctas(gpu, reference, singletrack):
+    """Long pairs run first on all four warps of a CTA (one planner thread, the diagonals over
+    128 threads): with every pair on a CTA, with none, and with the default length threshold,
+    the results are identical and equal the compiled WFA2-lib's; a CTA's pair that grows too
+    wide still moves to the cluster kernel."""
+    wfa = _wfa()
+    rng = np.random.default_rng(77 + int(singletrack))
+    ps, ts = [], []
+    for i in range(48):
+        L = int(np.exp(rng.uniform(np.log(20), np.log(9000))))
+        q, t = W.divergent_pair(rng, L, 0.0, 0.1, 4.0)
+        if i % 6 == 0:
+            q = q.copy()
+            q[rng.integers(0, len(q), 2)] = 4
+        ps.append(W.to_ascii(t))
+        ts.append(W.to_ascii(q))
+    al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=singletrack)
+    try:
+        wfa.set_long(0)
+        wfa.set_wide(0)
+        warp, _ = al.align_batch(ps, ts)
+        for long_sum, width in ((1, 0), (1, 8192), (8192, 8192), (4000, 512)):
+            wfa.set_long(long_sum)
+            wfa.set_wide(width, min(width, 1024), 8)
+            got, _ = al.align_batch(ps, ts)
+            assert got == warp, (long_sum, width)
+    finally:
+        wfa.set_long(3072)
+        wfa.set_wide(8192, 1024, 8)
+        al.close()
+    for i in range(0, 48, 4):
+        assert warp[i] == reference.wfa_align(ps[i], ts[i], 4, 4, 2, 24, 1, singletrack=singletrack), i
