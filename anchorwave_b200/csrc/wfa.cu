@@ -475,6 +475,108 @@ __device__ void finish_pair(const WfaArgs &A, const WfaPairDev &PR, int idx, con
     A.out[idx] = o;
 }
 
+// One trip of the piggyback compute step over the diagonals kb + g0 + G*u (u < PIG_U) of a
+// score with range [lo, hi], inputs in[] (M[s-x], M[s-o1-e1], I1[s-e1], D1[s-e1], M[s-o2-e2],
+// I2[s-e2], D2[s-e2]) and outputs out[] (ring slots of rcap elements per array).  Each gap cell
+// takes the extension on a tie, M the mismatch, then D2, D1, I2, I1 (the kernel's assignment
+// order); M is extended as it is computed (matches are not recorded in the packed CIGAR; the
+// traceback re-extends them).  Cells whose packed CIGAR holds 15 operations move it into a
+// block from the lane's reserved run; lanes whose run is short reserve LANE_BLOCKS more in one
+// allocation of the warp (`wal`).  Every lane of the warp must call it.  Returns false when
+// the pool is exhausted.
+__device__ __forceinline__ bool pig_trip(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
+                                         const uint8_t *txt, int kb, int g0, int G, int lo, int hi,
+                                         const CompHdr (&in)[7], const CompHdr (&out)[5], int mask, int rcap,
+                                         Alloc &wal, uint32_t &bnext, uint32_t &bend, int (&kmin)[5], int (&kmax)[5],
+                                         bool &reached) {
+    const int plen = PR.plen, tlen = PR.tlen, k_end = tlen - plen, lane = threadIdx.x & 31;
+    const CompHdr &m_misms = in[0], &m_open1 = in[1], &i1 = in[2], &d1 = in[3], &m_open2 = in[4], &i2 = in[5],
+                  &d2 = in[6];
+    const int k0 = kb + g0;
+    Cell C[PIG_U][5];
+#pragma unroll
+    for (int u = 0; u < PIG_U; ++u) {
+        const int k = k0 + G * u;
+        Cell a = getc(A, m_open1, k - 1), b = getc(A, i1, k - 1);
+        Cell g = b.o >= a.o ? b : a;
+        C[u][CI1] = Cell{g.o + 1, (g.pc << 2) | 3u, g.pv};
+        a = getc(A, m_open2, k - 1), b = getc(A, i2, k - 1);
+        g = b.o >= a.o ? b : a;
+        C[u][CI2] = Cell{g.o + 1, (g.pc << 2) | 3u, g.pv};
+        a = getc(A, m_open1, k + 1), b = getc(A, d1, k + 1);
+        g = b.o >= a.o ? b : a;
+        C[u][CD1] = Cell{g.o, (g.pc << 2) | 1u, g.pv};
+        a = getc(A, m_open2, k + 1), b = getc(A, d2, k + 1);
+        g = b.o >= a.o ? b : a;
+        C[u][CD2] = Cell{g.o, (g.pc << 2) | 1u, g.pv};
+        Cell x = getc(A, m_misms, k);
+        x.o += 1;
+        const int32_t best = max(max(C[u][CD1].o, C[u][CD2].o), max(x.o, max(C[u][CI1].o, C[u][CI2].o)));
+        const Cell &src = best == x.o ? x
+                          : best == C[u][CD2].o ? C[u][CD2]
+                          : best == C[u][CD1].o ? C[u][CD1]
+                          : best == C[u][CI2].o ? C[u][CI2]
+                                                : C[u][CI1];
+        C[u][CM] = Cell{in_matrix(best, k, plen, tlen) ? best : WF_NULL, (src.pc << 2) | 2u, src.pv};
+    }
+    {
+        int32_t mo[PIG_U];
+#pragma unroll
+        for (int u = 0; u < PIG_U; ++u) mo[u] = k0 + G * u <= hi ? C[u][CM].o : WF_NULL;
+        extend_n<PIG_U>(A, PR, pat, txt, k0, G, mo);
+#pragma unroll
+        for (int u = 0; u < PIG_U; ++u) {
+            const int k = k0 + G * u;
+            if (k > hi) continue;
+            C[u][CM].o = mo[u];
+            if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) reached = true;
+        }
+    }
+    uint32_t fl = 0;
+#pragma unroll
+    for (int u = 0; u < PIG_U; ++u) {
+        const int k = k0 + G * u;
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            if (k <= hi && (mask & (1 << c)) && C[u][c].pc >= PC_ALMOST_FULL && in_matrix(C[u][c].o, k, plen, tlen))
+                fl |= 1u << (u * 5 + c);
+    }
+    const bool refill = bend - bnext < (uint32_t)__popc(fl);
+    const unsigned rb = __ballot_sync(0xffffffffu, refill);
+    if (rb) {
+        const int64_t bb = warp_alloc(A, wal, (int64_t)__popc(rb) * LANE_BLOCKS * 8, lane);
+        if (bb < 0) return false;
+        if (refill) {
+            bnext = (uint32_t)(bb >> 3) + (uint32_t)__popc(rb & ((1u << lane) - 1u)) * LANE_BLOCKS;
+            bend = bnext + LANE_BLOCKS;
+        }
+    }
+    if (fl) {
+        uint2 *blk = (uint2 *)A.pool;
+#pragma unroll
+        for (int u = 0; u < PIG_U; ++u)
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                if (fl & (1u << (u * 5 + c))) {
+                    blk[bnext] = make_uint2(C[u][c].pc, C[u][c].pv);
+                    C[u][c].pc = 0u, C[u][c].pv = bnext++;
+                }
+    }
+#pragma unroll
+    for (int u = 0; u < PIG_U; ++u) {
+        const int k = k0 + G * u;
+        if (k > hi) break;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            if (!(mask & (1 << c))) continue;
+            int32_t *d = (int32_t *)(A.pool + out[c].off) + (k - lo);
+            d[0] = C[u][c].o, d[rcap] = (int32_t)C[u][c].pc, d[2 * rcap] = (int32_t)C[u][c].pv;
+            if (in_matrix(C[u][c].o, k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
+        }
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------------------
 // Plans and partials shared by the CTA-cooperative mode below and the cluster kernel: the
 // plan of one score (its range, inputs and outputs) and, per CTA, the trimmed ends of each
@@ -488,6 +590,8 @@ struct WidePlan {
 };
 struct WidePart {
     int kmin[5], kmax[5], reached, pad;
+    int retry, pad2;          // a warp found the pool exhausted (CTA-cooperative piggyback mode)
+    unsigned long long used;  // pool bytes of the warps' block reservations (the same)
 };
 
 __device__ __forceinline__ void part_reset(WidePart &p) {
@@ -527,6 +631,26 @@ __device__ __forceinline__ void plan_limits(const CompHdr (&in)[7], int &lo, int
     if (!isnull[1] || !isnull[3]) mask |= 1 << CD1;
     if (!isnull[4] || !isnull[5]) mask |= 1 << CI2;
     if (!isnull[4] || !isnull[6]) mask |= 1 << CD2;
+}
+
+// A warp's trimmed ends and end check, folded into its CTA's partials.
+__device__ __forceinline__ void fold_partials(const int (&kmin)[5], const int (&kmax)[5], bool reached, WidePart &pp) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const int th = __reduce_max_sync(0xffffffffu, kmax[c]);
+        const int tl = __reduce_min_sync(0xffffffffu, kmin[c]);
+        if (lane == 0 && th != INT_MIN) atomicMax(&pp.kmax[c], th), atomicMin(&pp.kmin[c], tl);
+    }
+    if (__any_sync(0xffffffffu, reached) && lane == 0) pp.reached = 1;
+}
+
+// First array of component c at score sc in the piggyback rings: M's last SR scores, then
+// I1/D1's last R1, then I2/D2's last R2, three arrays (offsets, packed CIGARs, links) each.
+__device__ __forceinline__ int64_t pig_slot(int c, int sc, int SR, int R1, int R2) {
+    if (c == CM) return (int64_t)(sc % SR) * 3;
+    if (c <= CD1) return 3 * (int64_t)(SR + (sc % R1) * 2 + (c - CI1));
+    return 3 * (int64_t)(SR + 2 * R1 + (sc % R2) * 2 + (c - CI2));
 }
 
 // One thread's diagonals lo + g0 + G*u of a planned score (high memory): the compute step,
@@ -595,13 +719,7 @@ __device__ __forceinline__ void plan_compute(const WfaArgs &A, const WfaPairDev 
             oM[k - lo] = mo[u];
         }
     }
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-        const int th = __reduce_max_sync(0xffffffffu, kmax[c]);
-        const int tl = __reduce_min_sync(0xffffffffu, kmin[c]);
-        if (lane == 0 && th != INT_MIN) atomicMax(&pp.kmax[c], th), atomicMin(&pp.kmin[c], tl);
-    }
-    if (__any_sync(0xffffffffu, reached) && lane == 0) pp.reached = 1;
+    fold_partials(kmin, kmax, reached, pp);
 }
 
 // Thread-0 bump allocation for the CTA-cooperative mode.
@@ -622,12 +740,15 @@ __device__ int64_t cta_alloc(const WfaArgs &A, Alloc &al, int64_t bytes) {
     return r;
 }
 
-// CTA-cooperative mode (high memory): one long pair on all threads of a CTA.  Thread 0 plans
+// CTA-cooperative mode: one long pair on all threads of a CTA.  Thread 0 plans
 // every score (the headers in the CTA's header ring and the pool, the allocations) and all
 // threads compute and extend the diagonals lo + tid + NT*u; two CTA barriers per score.  A
 // pair whose wavefront grows too wide stops with WFA_WIDE for the cluster kernel.  The cell arithmetic, the limits, the trimming and the backtrace are the warp's.
+// In the piggyback modes every warp reserves its own block runs; no pair moves to the
+// cluster kernel.
+template <bool PIG>
 __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan &plan, WidePart &part) {
-    const int tid = threadIdx.x, NT = blockDim.x;
+    const int tid = threadIdx.x, NT = blockDim.x, lane = tid & 31;
     const WfaPen P = A.pen;
     const WfaPairDev PR = A.pairs[idx];
     const int plen = PR.plen, tlen = PR.tlen;
@@ -640,6 +761,13 @@ __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan 
     const int R = (P.e1 > P.e2 ? P.e1 : P.e2) + 1, ring_cap = plen + tlen + 8;
     int64_t ring = -1;
     Alloc al{0, 0, true, 0};
+    // piggyback rings (thread 0) and every warp's block reservations
+    const int SR = A.max_score_scope, R1 = P.e1 + 1, R2 = P.e2 + 1;
+    const int64_t ring_arrays = 3 * (int64_t)(SR + 2 * R1 + 2 * R2);
+    int rcap = 32;
+    int64_t rbase = -1;
+    Alloc wal{0, 0, true, 0};
+    uint32_t bnext = 0, bend = 0;
     auto set_hdr = [&](int sc, const CompHdr (&o)[5]) {
         ScoreHdr *OH = hdr_ptr(A, ctab, sc);
         for (int c = 0; c < 5; ++c) OH->c[c] = o[c];
@@ -678,6 +806,23 @@ __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan 
             int lo, hi, mask;
             plan_limits(in, lo, hi, mask);
             const int width = hi - lo + 1;
+            if constexpr (PIG) {
+                if (width > rcap) {
+                    const int nc = max(2 * rcap, (width + 3) & ~3);
+                    const int64_t nb = cta_alloc(A, al, ring_arrays * nc * 4);
+                    if (nb < 0) {
+                        status = WFA_RETRY;
+                        break;
+                    }
+                    rcap = nc, rbase = nb;
+                }
+                for (int c = 0; c < 5; ++c)
+                    plan.out[c] = (mask & (1 << c)) ? CompHdr{lo, hi, lo, rcap, rbase + pig_slot(c, s, SR, R1, R2) * rcap * 4}
+                                                     : NUL;
+                for (int j = 0; j < 7; ++j) plan.in[j] = in[j];
+                plan.op = WOP_COMPUTE, plan.lo = lo, plan.hi = hi, plan.mask = mask;
+                return;
+            }
             // a wavefront too wide for the CTA: the cluster kernel re-runs the pair (past
             // wide_width_cta always; past wide_width_tail in the call's tail, checked every 32
             // scores: every pair started and few still running)
@@ -719,19 +864,28 @@ __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan 
     if (tid == 0) {
         atomicAdd(A.queue + 1, 1);  // pairs running
         part_reset(part);
-        if (A.singletrack) {
+        part.retry = 0, part.used = 0;
+        if (!PIG && A.singletrack) {
             ring = cta_alloc(A, al, (int64_t)R * 4 * ring_cap * 4);
             if (ring < 0) status = WFA_RETRY;
         }
+        if (PIG) {
+            rbase = cta_alloc(A, al, ring_arrays * rcap * 4);
+            if (rbase < 0) status = WFA_RETRY;
+        }
         const int64_t h0 = status == 0 ? cta_alloc(A, al, (int64_t)sizeof(ScoreHdr) * HDR_CHUNK) : -1;
-        const int64_t d0 = h0 >= 0 ? cta_alloc(A, al, 16) : -1;
+        const int64_t d0 = h0 < 0 ? -1 : PIG ? rbase : cta_alloc(A, al, 16);  // piggyback: slot 0 of M
         if (status == 0 && d0 < 0) status = WFA_RETRY;
         if (status == 0) {
             // M[0] = {0} on diagonal 0, extended
             const int32_t o0 = (int32_t)lcp1(A, PR, pat, txt, 0, 0);
             ctab[0] = h0;
             *(int32_t *)(A.pool + d0) = o0;
-            const CompHdr o[5] = {CompHdr{0, 0, 0, 0, d0}, NUL, NUL, NUL, NUL};
+            if (PIG) {
+                ((uint32_t *)(A.pool + d0))[rcap] = 0u;
+                ((uint32_t *)(A.pool + d0))[2 * rcap] = BT_NULL;  // the start (0, 0)
+            }
+            const CompHdr o[5] = {CompHdr{0, 0, 0, PIG ? rcap : 0, d0}, NUL, NUL, NUL, NUL};
             set_hdr(0, o);
             if (tlen - plen == 0 && o0 >= tlen) end_score = 0;
         }
@@ -740,9 +894,24 @@ __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan 
     }
     __syncthreads();
     while (plan.op == WOP_COMPUTE) {
-        plan_compute<false>(A, PR, pat, txt, plan, tid, NT, part);
+        if constexpr (PIG) {
+            int kmin[5], kmax[5];
+            bool reached = false, ok = true;
+#pragma unroll
+            for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
+            for (int kb = plan.lo; kb <= plan.hi && ok; kb += NT * PIG_U)
+                ok = pig_trip(A, PR, pat, txt, kb, tid, NT, plan.lo, plan.hi, plan.in, plan.out, plan.mask,
+                              plan.out[CM].pad, wal, bnext, bend, kmin, kmax, reached);
+            fold_partials(kmin, kmax, reached, part);
+            if (!ok && lane == 0) part.retry = 1;
+        } else {
+            plan_compute<false>(A, PR, pat, txt, plan, tid, NT, part);
+        }
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && part.retry) {
+            status = WFA_RETRY;
+            plan.op = WOP_DONE;
+        } else if (tid == 0) {
             CompHdr out[5];
             for (int c = 0; c < 5; ++c) {
                 out[c] = plan.out[c];
@@ -763,8 +932,10 @@ __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan 
         }
         __syncthreads();
     }
+    if (PIG && lane == 0) atomicAdd(&part.used, (unsigned long long)wal.used);
+    __syncthreads();
     if (tid == 0) {
-        finish_pair<false>(A, PR, idx, pat, txt, ctab, HR, status, end_score, s, al.used);
+        finish_pair<PIG>(A, PR, idx, pat, txt, ctab, HR, status, end_score, s, al.used + (int64_t)part.used);
         atomicSub(A.queue + 1, 1);
     }
     __syncthreads();
@@ -785,7 +956,7 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
     const int lane = threadIdx.x & 31;
     const WfaPen P = A.pen;
     extern __shared__ ScoreHdr hring_all[];
-    if constexpr (!PIG) {
+    {
         // the long pairs first, each on the whole CTA (warp 0's header ring serves the
         // planner; the warps take their own rings afterwards)
         __shared__ WidePlan cplan;
@@ -797,7 +968,7 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
             const int pi = cpi;
             __syncthreads();
             if (pi >= A.n_long) break;
-            cta_pair(A, A.order_long[pi], HdrRing{hring_all, rs}, cplan, cpart);
+            cta_pair<PIG>(A, A.order_long[pi], HdrRing{hring_all, rs}, cplan, cpart);
         }
     }
     const HdrRing HR{hring_all + (threadIdx.x >> 5) * rs, rs};
@@ -820,11 +991,6 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
         // e2+1 (the only scores the compute step reads them from); grown by reallocation
         const int SR = A.max_score_scope, R1 = P.e1 + 1, R2 = P.e2 + 1;
         const int64_t ring_arrays = 3 * (int64_t)(SR + 2 * R1 + 2 * R2);
-        auto pig_slot = [&](int c, int sc) -> int64_t {  // first array of component c at score sc
-            if (c == CM) return (int64_t)(sc % SR) * 3;
-            if (c <= CD1) return 3 * (int64_t)(SR + (sc % R1) * 2 + (c - CI1));
-            return 3 * (int64_t)(SR + 2 * R1 + (sc % R2) * 2 + (c - CI2));
-        };
         int rcap = 0;
         int64_t rbase = -1;
         if constexpr (PIG) {
@@ -987,7 +1153,7 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
                 }
                 for (int c = 0; c < 5; ++c)
                     if (alloc_c[c])
-                        out[c] = CompHdr{lo, hi, lo, rcap, rbase + pig_slot(c, s) * rcap * 4};
+                        out[c] = CompHdr{lo, hi, lo, rcap, rbase + pig_slot(c, s, SR, R1, R2) * rcap * 4};
             } else {
                 const int64_t wb = (((int64_t)width * 4) + 15) & ~(int64_t)15;
                 int nstore = 1;
@@ -1021,99 +1187,16 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
 #pragma unroll
             for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
             if constexpr (PIG) {
-                // PIG_U diagonals per lane at a time; each gap cell takes the extension on
-                // a tie, M the mismatch, then D2, D1, I2, I1 (the kernel's assignment order).
-                // Every lane runs every trip (the block reservation below is warp-wide).
+                // PIG_U diagonals per lane at a time (every lane runs every trip: the block
+                // reservation is warp-wide)
+                const CompHdr in7[7] = {m_misms, m_open1, i1, d1, m_open2, i2, d2};
+                int mask = 0;
+                for (int c = 0; c < 5; ++c) mask |= alloc_c[c] ? 1 << c : 0;
                 for (int kb = lo; kb <= hi; kb += 32 * PIG_U) {
-                    const int k0 = kb + lane;
-                    Cell C[PIG_U][5];
-#pragma unroll
-                    for (int u = 0; u < PIG_U; ++u) {
-                        const int k = k0 + 32 * u;
-                        Cell a = getc(A, m_open1, k - 1), b = getc(A, i1, k - 1);
-                        Cell g = b.o >= a.o ? b : a;
-                        C[u][CI1] = Cell{g.o + 1, (g.pc << 2) | 3u, g.pv};
-                        a = getc(A, m_open2, k - 1), b = getc(A, i2, k - 1);
-                        g = b.o >= a.o ? b : a;
-                        C[u][CI2] = Cell{g.o + 1, (g.pc << 2) | 3u, g.pv};
-                        a = getc(A, m_open1, k + 1), b = getc(A, d1, k + 1);
-                        g = b.o >= a.o ? b : a;
-                        C[u][CD1] = Cell{g.o, (g.pc << 2) | 1u, g.pv};
-                        a = getc(A, m_open2, k + 1), b = getc(A, d2, k + 1);
-                        g = b.o >= a.o ? b : a;
-                        C[u][CD2] = Cell{g.o, (g.pc << 2) | 1u, g.pv};
-                        Cell x = getc(A, m_misms, k);
-                        x.o += 1;
-                        const int32_t best = max(max(C[u][CD1].o, C[u][CD2].o), max(x.o, max(C[u][CI1].o, C[u][CI2].o)));
-                        const Cell &src = best == x.o ? x
-                                          : best == C[u][CD2].o ? C[u][CD2]
-                                          : best == C[u][CD1].o ? C[u][CD1]
-                                          : best == C[u][CI2].o ? C[u][CI2]
-                                                                : C[u][CI1];
-                        C[u][CM] = Cell{in_matrix(best, k, plen, tlen) ? best : WF_NULL, (src.pc << 2) | 2u, src.pv};
-                    }
-                    // the extension of M[s] (fused, as outside the piggyback modes): matches are
-                    // not recorded in the packed CIGAR; the traceback re-extends them
-                    {
-                        int32_t mo[PIG_U];
-#pragma unroll
-                        for (int u = 0; u < PIG_U; ++u) mo[u] = k0 + 32 * u <= hi ? C[u][CM].o : WF_NULL;
-                        extend_n<PIG_U>(A, PR, pat, txt, k0, 32, mo);
-#pragma unroll
-                        for (int u = 0; u < PIG_U; ++u) {
-                            const int k = k0 + 32 * u;
-                            if (k > hi) continue;
-                            C[u][CM].o = mo[u];
-                            if (k == k_end && mo[u] != WF_NULL && mo[u] >= tlen) fused_reached = true;
-                        }
-                    }
-                    // cells whose packed CIGAR holds 15 operations move it into a block,
-                    // taken from the lane's reserved run; lanes whose run is short reserve
-                    // LANE_BLOCKS more in one warp allocation
-                    uint32_t fl = 0;
-#pragma unroll
-                    for (int u = 0; u < PIG_U; ++u) {
-                        const int k = k0 + 32 * u;
-#pragma unroll
-                        for (int c = 0; c < 5; ++c)
-                            if (k <= hi && alloc_c[c] && C[u][c].pc >= PC_ALMOST_FULL && in_matrix(C[u][c].o, k, plen, tlen))
-                                fl |= 1u << (u * 5 + c);
-                    }
-                    const bool refill = bend - bnext < (uint32_t)__popc(fl);
-                    const unsigned rb = __ballot_sync(0xffffffffu, refill);
-                    if (rb) {
-                        const int64_t bb = warp_alloc(A, al, (int64_t)__popc(rb) * LANE_BLOCKS * 8, lane);
-                        if (bb < 0) {
-                            status = WFA_RETRY;
-                            break;
-                        }
-                        if (refill) {
-                            bnext = (uint32_t)(bb >> 3) + (uint32_t)__popc(rb & ((1u << lane) - 1u)) * LANE_BLOCKS;
-                            bend = bnext + LANE_BLOCKS;
-                        }
-                    }
-                    if (fl) {
-                        uint2 *blk = (uint2 *)A.pool;
-#pragma unroll
-                        for (int u = 0; u < PIG_U; ++u)
-#pragma unroll
-                            for (int c = 0; c < 5; ++c)
-                                if (fl & (1u << (u * 5 + c))) {
-                                    blk[bnext] = make_uint2(C[u][c].pc, C[u][c].pv);
-                                    C[u][c].pc = 0u, C[u][c].pv = bnext++;
-                                }
-                    }
-#pragma unroll
-                    for (int u = 0; u < PIG_U; ++u) {
-                        const int k = k0 + 32 * u;
-                        if (k > hi) break;
-#pragma unroll
-                        for (int c = 0; c < 5; ++c) {
-                            if (!alloc_c[c]) continue;
-                            int32_t *d = (int32_t *)(A.pool + out[c].off) + (k - lo);
-                            d[0] = C[u][c].o, d[rcap] = (int32_t)C[u][c].pc, d[2 * rcap] = (int32_t)C[u][c].pv;
-                            if (in_matrix(C[u][c].o, k, plen, tlen)) kmin[c] = min(kmin[c], k), kmax[c] = max(kmax[c], k);
-                        }
+                    if (!pig_trip(A, PR, pat, txt, kb, lane, 32, lo, hi, in7, out, mask, rcap, al, bnext, bend, kmin, kmax,
+                                  fused_reached)) {
+                        status = WFA_RETRY;
+                        break;
                     }
                 }
                 if (status != 0) break;

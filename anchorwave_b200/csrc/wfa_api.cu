@@ -180,7 +180,7 @@ static int run_batch(wavefront_aligner_gpu *al, int n, const char *const *patter
     W.wide_width_tail = std::min(W.wide_width, std::max(0, g_wide_tail.load()));
     W.wide_tail_pairs = std::max(1, wide_clusters);
     W.wide_width_cta = W.wide_width;
-    const int64_t long_sum = W.piggyback ? 0 : g_long_sum.load();
+    const int64_t long_sum = g_long_sum.load();
     std::vector<int32_t> staged;
     // Rounds: every round restarts the pool and runs up to `chunk` pending pairs, largest
     // first; pairs that found the pool exhausted stay pending.  A round that completes

@@ -312,14 +312,15 @@ def test_wfa_cluster_kernel_long_pair(gpu, reference):
         assert got[0] == reference.wfa_align(p_, t_, 4, 4, 2, 24, 1, singletrack=stk), stk
 
 
-@pytest.mark.parametrize("singletrack", [False, True])
-def test_wfa_long_pairs_on_whole_ctas(gpu, reference, singletrack):
+@pytest.mark.parametrize("singletrack,memory_mode", [(False, 0), (True, 0), (False, 1), (False, 2)])
+def test_wfa_long_pairs_on_whole_ctas(gpu, reference, singletrack, memory_mode):
     """Long pairs run first on all four warps of a CTA (one planner thread, the diagonals over
-    128 threads): with every pair on a CTA, with none, and with the default length threshold,
-    the results are identical and equal the compiled WFA2-lib's; a CTA's pair that grows too
-    wide still moves to the cluster kernel."""
+    128 threads; in the piggyback modes every warp reserves its own block runs): with every
+    pair on a CTA, with none, and with the default length threshold, the results are
+    identical and equal the compiled WFA2-lib's in the same mode; in high memory a CTA's pair
+    that grows too wide still moves to the cluster kernel."""
     wfa = _wfa()
-    rng = np.random.default_rng(77 + int(singletrack))
+    rng = np.random.default_rng(77 + int(singletrack) + 3 * memory_mode)
     ps, ts = [], []
     for i in range(48):
         L = int(np.exp(rng.uniform(np.log(20), np.log(9000))))
@@ -329,7 +330,7 @@ def test_wfa_long_pairs_on_whole_ctas(gpu, reference, singletrack):
             q[rng.integers(0, len(q), 2)] = 4
         ps.append(W.to_ascii(t))
         ts.append(W.to_ascii(q))
-    al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=singletrack)
+    al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=singletrack, memory_mode=memory_mode)
     try:
         wfa.set_long(0)
         wfa.set_wide(0)
@@ -344,4 +345,5 @@ def test_wfa_long_pairs_on_whole_ctas(gpu, reference, singletrack):
         wfa.set_wide(8192, 1024, 8)
         al.close()
     for i in range(0, 48, 4):
-        assert warp[i] == reference.wfa_align(ps[i], ts[i], 4, 4, 2, 24, 1, singletrack=singletrack), i
+        assert warp[i] == reference.wfa_align(ps[i], ts[i], 4, 4, 2, 24, 1, singletrack=singletrack,
+                                              memory_mode=memory_mode), i
