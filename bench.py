@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--long-banded-max", type=int, default=1_000_000)
     ap.add_argument("--long-banded-indel", type=int, default=50_000, help="longest of the long indels")
     ap.add_argument("--wfa-pairs", type=int, default=16384, help="pairs of the batched WFA workload (0 skips it)")
+    ap.add_argument("--wfa-long-pairs", type=int, default=3,
+                    help="single long divergent WFA intervals timed alone (0 skips them)")
     ap.add_argument("--no-selector-summary", action="store_true",
                     help="skip the selector sequence-pass measurement")
     ap.add_argument("--wfa-pool-gb", type=float, default=0.0,
@@ -495,6 +497,62 @@ def wfa_measurement(npairs: int, rank: int, cpu: bool, pool_gb: float = 0.0):
     return out
 
 
+# Long divergent intervals of the kind AnchorWave's selector routes to SingletrackWfa
+# (interval length, divergence): the latency of one interval alone, the cluster kernel's case.
+WFA_LONG_PAIRS = ((12_000, 0.15), (24_000, 0.12), (40_000, 0.08))
+
+
+def wfa_long_measurement(npairs: int, rank: int, cpu: bool):
+    """Single long divergent intervals through the Singletrack WFA (high memory, penalties
+    x=4, o1=4, e1=2, o2=24, e2=1), one call each: the device time of the call (a pair whose
+    wavefronts outgrow a warp or a CTA moves to the 8-CTA cluster kernel) and, for the first,
+    the same call with every pair kept on one warp; beside them the reference's WFA2 code on
+    one host thread on the same interval (status, score and operation string compared)."""
+    import time
+
+    import numpy as np
+
+    from anchorwave_b200 import wfa
+    from anchorwave_b200 import workloads as W
+    rng = np.random.default_rng(50 + rank)
+    ref = None
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        try:
+            ref = oracle.Reference()
+        except FileNotFoundError:
+            ref = None
+    out = []
+    for j, (length, d) in enumerate(WFA_LONG_PAIRS[:npairs]):
+        q, t = W.divergent_pair(rng, length, d, d, 4.0)
+        p_, t_ = W.to_ascii(t), W.to_ascii(q)
+        al = wfa.WfaAligner(4, 4, 2, 24, 1, singletrack=True, max_memory_abort=4 << 30)
+        al.align_batch([p_], [t_])
+        (res,), ms = al.align_batch([p_], [t_])
+        moved = al.launches()[2]
+        rec = {"length": length, "divergence": d, "status": res[0], "score": res[1], "device_ms": ms,
+               "on_cluster_kernel": bool(moved)}
+        if j == 0:
+            wfa.set_long(0)
+            wfa.set_wide(0)
+            try:
+                _, ms1 = al.align_batch([p_], [t_])
+            finally:
+                wfa.set_long(3072)
+                wfa.set_wide(8192, 1024, 8)
+            rec["one_warp_device_ms"] = ms1
+        al.close()
+        if ref is not None:
+            t0 = time.perf_counter()
+            r = ref.wfa_align(p_, t_, 4, 4, 2, 24, 1, singletrack=True)
+            rs = time.perf_counter() - t0
+            rec["cpu_reference"] = {"seconds": rs, "threads": 1, "identical": tuple(r) == tuple(res)}
+            rec["vs_cpu_reference"] = rs / (ms * 1e-3)
+        out.append(rec)
+    return out
+
+
 def selector_summary_measurement(ps, rank: int, cpu: bool):
     """The selector's sequence pass (summarizeSequencePair: k-mer sketches at k = 9, 15, 21,
     composition, entropy, fingerprints) over the intervals of the headline workload, through
@@ -852,6 +910,7 @@ def main():
         rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max, args.long_banded_indel,
         tuning)
     wfa_res = (wfa_measurement(args.wfa_pairs, rank, cpu_on, args.wfa_pool_gb) if args.wfa_pairs > 0 else None)
+    wfa_long = wfa_long_measurement(args.wfa_long_pairs, rank, cpu_on) if args.wfa_long_pairs > 0 else None
     summary_res = (None if args.no_selector_summary else selector_summary_measurement(ps, rank, cpu_on))
 
     if rank != 0:
@@ -904,6 +963,7 @@ def main():
         "serving": serving,
         "long_banded": long_banded,
         "wfa": wfa_res,
+        "wfa_long_intervals": wfa_long,
         "selector_summary": summary_res,
         "gpu_launches": launches * args.steps,
         "clocks": clocks,
@@ -968,6 +1028,12 @@ def compact_summary(line):
                 out["wfa"][nm] = {"pairs_per_s": wf[nm]["pairs_per_s"], "vs_ref": wf[nm].get("vs_cpu_reference")}
                 par[f"wfa_{nm}"] = {"pairs_checked": get(wf, nm, "cpu_reference", "pairs"),
                                     "identical": get(wf, nm, "cpu_reference", "status_score_cigar_identical")}
+    wl = line.get("wfa_long_intervals")
+    if wl:
+        out["wfa_long"] = [{"kb": r["length"] // 1000, "ms": r["device_ms"], "vs_ref": r.get("vs_cpu_reference")}
+                           for r in wl]
+        par["wfa_long"] = all(get(r, "cpu_reference", "identical") for r in wl) if all(
+            "cpu_reference" in r for r in wl) else None
     ss = line.get("selector_summary")
     if ss:
         out["selector_pass"] = {"bases_per_s": ss.get("e2e_bases_per_s"), "vs_ref": ss.get("vs_cpu_reference")}
