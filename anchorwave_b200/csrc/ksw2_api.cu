@@ -761,6 +761,13 @@ static int plan_finish(aw_ksw_plan_t *pl, float *ms) {
         AW_CUDA(cudaEventElapsedTime(&t0, B->ev_k[3 * k], B->ev_k[3 * k + 1]));
         AW_CUDA(cudaEventElapsedTime(&t1, B->ev_k[3 * k + 1], B->ev_k[3 * k + 2]));
         dp += t0, bt += t1;
+        const int kb = k - (int)pl->waves.size();
+        if (kb >= 0 && getenv("AW_VERBOSE")) {
+            const BandWave &BW = pl->band.waves[kb];
+            fprintf(stderr, "[aw_b200] band wave %d: %d pairs, %d units, traceback %.1f GB, %d recompute rounds; "
+                            "DP %.1f ms, traceback and rounds %.1f ms\n",
+                    kb, BW.npair, BW.nunit, BW.tb_bytes / 1e9, BW.nround, t0, t1);
+        }
     }
     pl->dp_ms = dp;
     pl->bt_ms = bt;

@@ -652,15 +652,16 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
     warm.upload()
     warm.execute()
     warm.close()
-    # the autotuner picks the banded kernel's columns per lane (4, 8, or the per-batch rule) on
-    # the four smallest pairs of this workload that reach the end of the band, score-only (the DP
-    # pass the setting affects)
+    # the autotuner picks the banded kernel's columns per lane (4, 8, or the per-batch rule) on a
+    # seeded random eighth of this workload's pairs, score-only (the DP pass the setting affects).
+    # A sample of the smallest pairs is chain-bound where the whole workload is work-bound, and
+    # picked 4 columns, which made the whole workload 20% slower than 8.
     from anchorwave_b200 import autotune
     t_tune = time.perf_counter()
-    reachable = sorted((i for i in range(len(ps)) if reach[i]), key=lambda i: pair_cells[i])
-    pick = reachable[:4]
+    pick = sorted(np.random.default_rng(7 + rank).choice(len(ps), size=max(1, len(ps) // 8), replace=False).tolist())
     cols, trials = autotune.tune_band([ps.queries[i] for i in pick], [ps.targets[i] for i in pick],
-                                      [ps.band[i] for i in pick], mat, 4, 2, 24, 1, flag=0x01, sample=4, reps=1)
+                                      [ps.band[i] for i in pick], mat, 4, 2, 24, 1, flag=0x01, sample=len(pick),
+                                      reps=1)
     if tuning is not None:
         tuning["band_kernel"] = {"columns_per_lane": cols, "trials_ms": {str(t["columns"]): t["ms"] for t in trials},
                                  "seconds": time.perf_counter() - t_tune, "sample_pairs": len(pick)}
