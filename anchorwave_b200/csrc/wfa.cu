@@ -944,7 +944,7 @@ __device__ void cta_pair(const WfaArgs &A, int idx, const HdrRing &HR, WidePlan 
 // Build-time tuning of the warp kernel: CTAs per SM the registers are sized for (4 warps
 // each), and diagonals per lane in flight in the high-memory compute step.
 #ifndef AW_WFA_MINB
-#define AW_WFA_MINB 3
+#define AW_WFA_MINB 4
 #endif
 #ifndef AW_WFA_WARP_U
 #define AW_WFA_WARP_U 4
