@@ -653,6 +653,11 @@ __device__ __forceinline__ int64_t pig_slot(int c, int sc, int SR, int R1, int R
     return 3 * (int64_t)(SR + 2 * R1 + (sc % R2) * 2 + (c - CI2));
 }
 
+// Diagonals per thread in flight in the CTA-cooperative compute step (build-time tuning).
+#ifndef AW_WFA_CTA_U
+#define AW_WFA_CTA_U 2
+#endif
+
 // One thread's diagonals lo + g0 + G*u of a planned score (high memory): the compute step,
 // the fused extension of M, the stores, and this thread's trimmed ends and end check, folded
 // per warp into the CTA's partials.  `ld_l2` reads the inputs through L2 (other CTAs wrote them).
@@ -673,7 +678,7 @@ __device__ __forceinline__ void plan_compute(const WfaArgs &A, const WfaPairDev 
     bool reached = false;
 #pragma unroll
     for (int c = 0; c < 5; ++c) kmin[c] = INT_MAX, kmax[c] = INT_MIN;
-    constexpr int U = 4;
+    constexpr int U = L2 ? 4 : AW_WFA_CTA_U;
     for (int k0 = lo + g0; k0 <= hi; k0 += G * U) {
         int32_t ins1[U], ins2[U], del1[U], del2[U], misms[U];
 #pragma unroll
