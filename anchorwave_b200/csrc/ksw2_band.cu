@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         uint2 *bnd_me = A.bnd + St.bnd_off;
         int32_t *prog_me = A.progress + PROG_STRIDE * (P.strip0 + s);
         uint8_t *tbp = CIGAR ? A.tb + St.tb_off : nullptr;
+        const bool store_tb = CIGAR && (!P.ckpt || A.store_ckpt);  // this strip's traceback is kept
         BandRes *R = A.res + un.x;
         // lane constants of the closed-form bounds: floor16 and the block end of the lane's columns
         const int F16 = col0 & ~15, XB = (col0 & g.bmask) + B - 1;
@@ -295,7 +296,21 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
             const bool warp_fast = __all_sync(FULL, fast || !active);
             uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;  // traceback bytes of this lane-step
             if (active) {
-                if (warp_fast) {
+                if (warp_fast && ARGMAX && !store_tb) {
+                    // no traceback is kept for this strip (a recomputed pair's first pass, or a
+                    // pair whose band empties): the cells without their state bytes
+                    const uint32_t sel = qc * 0x1111u + 0x8880u;
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        int d = 0;
+                        const int sc = prmt_sx(rlo[c], rhi[c], sel);
+                        cell<false, RIGHT>(sc, xs, vs, x2s, ut[c], yt[c], y2t[c], d, S);
+                        H[c] += vs;
+                    }
+                    lastfast = j;
+                    carry = pack3(xs, vs, x2s, qc);
+                    Hcarry = H[C - 1];
+                } else if (warp_fast) {
                     const uint32_t sel = qc * 0x1111u + 0x8880u;
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
@@ -427,7 +442,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                     Hcarry = Hf;
                 }
                 if (src_lane) ring[warp][k & 15][lane] = carry;
-                if (CIGAR && j >= jlo && (!P.ckpt || A.store_ckpt)) {
+                if (store_tb && j >= jlo) {
                     uint8_t *dst = tbp + ((int64_t)(j - jlo + lane) * 32 + lane) * CB;
                     if (C == 8) {
                         if (ST) __stcs(reinterpret_cast<uint4 *>(dst), make_uint4(w0, w1, w2, w3));
