@@ -144,6 +144,9 @@ struct BandArgs {
     int block, generic;
     int store_ckpt;  // 1: store the traceback of recomputed pairs too (their group passes)
     const unsigned long long *deadline;  // null: no deadline
+    // recompute rounds: the pairs' walk states; a round's strips stop at the row the walk has
+    // reached (it only moves up and left), strips of a finished walk compute nothing
+    const BandWalkState *walk;
 };
 
 constexpr uint64_t WAIT_NS = 20ull * 1000 * 1000 * 1000;  // bounded wait on the left strip
@@ -173,7 +176,14 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         const BandPairDev P = A.pairs[un.x];
         const int s = un.y;
         const BandStripDev St = A.strips[P.strip0 + s];
-        const int jstart = St.jstart, jlo = St.jlo, jend = St.jend;
+        // the last row this pass needs: the strip's last band row, or in a recompute round the
+        // walk's row (the same limit for every strip of the pair, producers included)
+        int wlim = INT_MAX;
+        if (A.walk) {
+            const BandWalkState wk = A.walk[un.x];
+            wlim = wk.done ? -1 : wk.j;
+        }
+        const int jstart = St.jstart, jlo = St.jlo, jend = min(St.jend, wlim);
         if (jend < jlo) continue;  // nothing of this strip is computed
         volatile int32_t *stop_word = &A.res[un.x].stopped;
         if (A.deadline && *stop_word) continue;  // the pair stopped at the deadline
@@ -190,8 +200,8 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         int32_t *prog_prod = nullptr;
         if (s > 0) {
             const BandStripDev Pr = A.strips[P.strip0 + s - 1];
-            if (Pr.jend >= Pr.jlo) {
-                prod_lo = Pr.jlo, prod_hi = Pr.jend;
+            if (min(Pr.jend, wlim) >= Pr.jlo) {
+                prod_lo = Pr.jlo, prod_hi = min(Pr.jend, wlim);
                 bnd_prod = A.bnd + Pr.bnd_off;
                 prog_prod = A.progress + PROG_STRIDE * (P.strip0 + s - 1);
             }
@@ -1090,6 +1100,7 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
     a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
     a.store_ckpt = 0;
     a.deadline = D.deadline;
+    a.walk = nullptr;
     return band_launch_units(bp, a, flag, ctas, st);
 }
 
@@ -1164,6 +1175,7 @@ cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, cons
         a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
         a.store_ckpt = 1;
         a.deadline = D.deadline;
+        a.walk = D.walk;
         if ((e = band_launch_units(bp, a, flag, ctas, st)) != cudaSuccess) return e;
         if (bp.nc == 4) ksw_band_round_walk_kernel<4><<<R.ngroup, 32, 0, st>>>(b, gd);
         else ksw_band_round_walk_kernel<8><<<R.ngroup, 32, 0, st>>>(b, gd);
