@@ -86,6 +86,9 @@ def parse():
     ap.add_argument("--long-banded-min", type=int, default=100_000)
     ap.add_argument("--long-banded-max", type=int, default=1_000_000)
     ap.add_argument("--long-banded-indel", type=int, default=50_000, help="longest of the long indels")
+    ap.add_argument("--long-banded-budget-gb", type=float, default=0.0,
+                    help="traceback budget of the long banded sample in GB (0: the library default); a small "
+                         "budget makes its pairs recompute their tracebacks in rounds")
     ap.add_argument("--wfa-pairs", type=int, default=16384, help="pairs of the batched WFA workload (0 skips it)")
     ap.add_argument("--wfa-long-pairs", type=int, default=3,
                     help="single long divergent WFA intervals timed alone (0 skips them)")
@@ -626,7 +629,7 @@ def cigar_check(res, q, t, mis=4, o1=4, e1=2, o2=24, e2=1):
 
 
 def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 100_000, lmax: int = 1_000_000,
-                            long_max: int = 50_000, tuning=None):
+                            long_max: int = 50_000, budget_gb: float = 0.0, tuning=None):
     """The long-interval banded and Singletrack workload (target length U(lmin, lmax), 30% of
     the query replaced by repeat structure, 3% substitutions, 5-20 long indels of U(1,
     long_max), w = 10% of the shorter length): one execution of the whole set per traceback,
@@ -666,6 +669,9 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
         tuning["band_kernel"] = {"columns_per_lane": cols, "trials_ms": {str(t["columns"]): t["ms"] for t in trials},
                                  "seconds": time.perf_counter() - t_tune, "sample_pairs": len(pick)}
     results = {}
+    if budget_gb > 0:
+        ksw2.set_traceback_budget(int(budget_gb * 1e9))
+        out["traceback_budget_bytes"] = int(budget_gb * 1e9)
     for name, flag in (("banded", 0), ("singletrack", 0x1000)):
         plan = ksw2.KswPlan(ps.queries, ps.targets, mat, 4, 2, 24, 1, w=ps.band, flag=flag)
         plan.upload()
@@ -694,6 +700,8 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
                      "cigars_rescoring_to_score": rescored}
         ksw2.release_thread_buffers()
     ksw2.set_band_columns(0)
+    if budget_gb > 0:
+        ksw2.set_traceback_budget(0)
     if cpu:
         from concurrent.futures import ThreadPoolExecutor
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -909,6 +917,7 @@ def main():
     serving = serving_measurement(args.serve_requests, rank, tuning) if args.serve_requests > 0 else None
     long_banded = None if args.no_long_banded else long_banded_measurement(
         rank, cpu_on, args.long_banded_pairs, args.long_banded_min, args.long_banded_max, args.long_banded_indel,
+        args.long_banded_budget_gb,
         tuning)
     wfa_res = (wfa_measurement(args.wfa_pairs, rank, cpu_on, args.wfa_pool_gb) if args.wfa_pairs > 0 else None)
     wfa_long = wfa_long_measurement(args.wfa_long_pairs, rank, cpu_on) if args.wfa_long_pairs > 0 else None
