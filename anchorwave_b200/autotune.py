@@ -60,26 +60,35 @@ def tune(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray], mat, q, e
 
 
 def tune_band(queries: Sequence[np.ndarray], targets: Sequence[np.ndarray], bands: Sequence[int], mat, q, e, q2,
-              e2, flag: int = 0, sample: int = 8, reps: int = 1, seed: int = 0) -> Tuple[int, List[Dict]]:
+              e2, flag: int = 0, sample: int = 8, reps: int = 1, seed: int = 0,
+              budget: int = 0) -> Tuple[int, List[Dict]]:
     """Banded kernel: times the sample under 4 and 8 columns per lane and under the per-batch
-    rule (0); returns (columns, trials) and installs the winner."""
+    rule (0); returns (columns, trials) and installs the winner.  `budget` > 0: the traceback
+    budget of the trials (a share of the whole batch's, so that the sample's pairs recompute
+    their tracebacks in rounds as the batch's do)."""
     idx = _sample(len(queries), sample, seed)
     qs = [queries[i] for i in idx]
     ts = [targets[i] for i in idx]
     ws = [int(bands[i]) for i in idx]
     trials = []
     best = None
-    for i, cols in enumerate((0,) + BAND_COLUMNS):
-        ksw2.set_band_columns(cols)
-        plan = ksw2.KswPlan(qs, ts, mat, q, e, q2, e2, w=ws, flag=flag)
-        plan.upload()
-        if i == 0:
-            plan.execute()  # warm-up: the device buffers, once for all settings
-        ms = min(plan.execute() for _ in range(reps))
-        plan.close()
-        trials.append({"columns": cols, "ms": ms})
-        if best is None or ms < best[0]:
-            best = (ms, cols)
+    if budget > 0:
+        ksw2.set_traceback_budget(budget)
+    try:
+        for i, cols in enumerate((0,) + BAND_COLUMNS):
+            ksw2.set_band_columns(cols)
+            plan = ksw2.KswPlan(qs, ts, mat, q, e, q2, e2, w=ws, flag=flag)
+            plan.upload()
+            if i == 0:
+                plan.execute()  # warm-up: the device buffers, once for all settings
+            ms = min(plan.execute() for _ in range(reps))
+            plan.close()
+            trials.append({"columns": cols, "ms": ms})
+            if best is None or ms < best[0]:
+                best = (ms, cols)
+    finally:
+        if budget > 0:
+            ksw2.set_traceback_budget(0)
     ksw2.release_thread_buffers()
     ksw2.set_band_columns(best[1])
     return best[1], trials

@@ -655,13 +655,14 @@ def long_banded_measurement(rank: int, cpu: bool, npairs: int = 64, lmin: int = 
     warm.upload()
     warm.execute()
     warm.close()
-    # the autotuner picks the banded kernel's columns per lane (4, 8, or the per-batch rule) on a
-    # seeded random eighth of this workload's pairs, score-only (the DP pass the setting affects).
-    # A sample of the smallest pairs is chain-bound where the whole workload is work-bound, and
-    # picked 4 columns, which made the whole workload 20% slower than 8.
+    # the autotuner picks the banded kernel's columns per lane (4, 8, or the per-batch rule) on the
+    # four pairs with the most band cells, score-only: the batch's largest pairs hold most of its
+    # cells and run first, together, in its first wave.  Samples of small or random pairs (alone,
+    # or with a traceback budget scaled to them) are chain-bound where the whole workload is
+    # work-bound, and picked 4 columns, which made the whole workload 20-25% slower than 8.
     from anchorwave_b200 import autotune
     t_tune = time.perf_counter()
-    pick = sorted(np.random.default_rng(7 + rank).choice(len(ps), size=max(1, len(ps) // 8), replace=False).tolist())
+    pick = sorted(sorted(range(len(ps)), key=lambda i: -pair_cells[i])[:4])
     cols, trials = autotune.tune_band([ps.queries[i] for i in pick], [ps.targets[i] for i in pick],
                                       [ps.band[i] for i in pick], mat, 4, 2, 24, 1, flag=0x01, sample=len(pick),
                                       reps=1)
