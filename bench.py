@@ -220,8 +220,9 @@ def sig(x, digits=4):
 
 
 def run_reference_arm(args):
-    rank, world, local, pg = dist_init(args.gpus)
-    if rank != 0:
+    # under torchrun rank 0 alone times the reference's CPU code; the others exit without work
+    # (no process group: no rank waits on another)
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -827,6 +828,13 @@ def main():
     if args.impl == "reference":
         return run_reference_arm(args)
     rank, world, local, pg = dist_init(args.gpus)
+    if world > 1:
+        # replicas on N GPUs: the line measures the headline step (and its e2e, plain per-call
+        # sample, roofline and clocks) on every rank; the single-GPU sub-measurements and the
+        # host-CPU reference legs belong to the 1-GPU line, so that no rank waits minutes at the
+        # final barrier for another's extra work
+        args.serve_requests = args.plain_pairs = args.wfa_pairs = args.wfa_long_pairs = 0
+        args.no_long_banded = args.no_selector_summary = args.no_cpu_baseline = True
     import numpy as np
 
     from anchorwave_b200 import _lib, ksw2
@@ -926,6 +934,7 @@ def main():
 
     if rank != 0:
         barrier(pg)
+        pg.destroy_process_group()
         return 0
 
     hbm_peak, hbm_kind = load_peaks()
@@ -984,9 +993,13 @@ def main():
             line["cpu_baseline"] = cpu_baseline(ps, args.cpu_budget, res_dev)
         except FileNotFoundError as e:
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if world > 1:
+        line["sub_measurements"] = "on the 1-GPU line (replicas measure the headline step)"
     line["summary"] = compact_summary(line)
     print(json.dumps(line))
     barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
     return 0
 
 
