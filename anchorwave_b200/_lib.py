@@ -25,7 +25,7 @@ class KswExtz(C.Structure):
 EXPORTS = [
     "ksw_extd2_gpu", "ksw_extd2_singletrack_gpu", "ksw_extd2_singletrack_sse_gpu", "aw_ksw_extd2_batch",
     "aw_ksw_plan_new", "aw_ksw_plan_upload", "aw_ksw_plan_execute", "aw_ksw_plan_download",
-    "aw_ksw_plan_stats", "aw_ksw_plan_timing", "aw_ksw_plan_graph", "aw_ksw_plan_free",
+    "aw_ksw_plan_stats", "aw_ksw_plan_routes", "aw_ksw_plan_timing", "aw_ksw_plan_graph", "aw_ksw_plan_free",
     "aw_set_traceback_budget", "aw_set_tuning", "aw_set_band_columns", "aw_set_full_pair_routing",
     "aw_set_wfa_wide", "aw_set_wfa_long", "wavefront_gpu_last_launches", "aw_release_thread_buffers",
     "aw_ksw_set_deadline", "aw_ksw_set_stop_antidiagonal", "aw_last_error", "aw_device_count",
@@ -111,6 +111,8 @@ def _load(path: str = LIB_PATH):
     lib.aw_ksw_plan_download.restype = i32
     lib.aw_ksw_plan_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)]
     lib.aw_ksw_plan_stats.restype = i32
+    lib.aw_ksw_plan_routes.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    lib.aw_ksw_plan_routes.restype = i32
     lib.aw_ksw_plan_timing.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.aw_ksw_plan_timing.restype = i32
     lib.aw_ksw_plan_free.argtypes = [vp]

@@ -235,13 +235,14 @@ static bool full_path_ok(const Params &P, int qlen, int tlen, int w) {
 }
 
 // The banded strip kernel (ksw2_band.cu) restates the reference's padding-lane
-// semantics, so it takes any band and the Singletrack traceback; it shares the
-// strip kernel's scoring restrictions (no z-drop or max tracking: with mat <= 0
+// semantics, so it takes any band and the Singletrack traceback (both entries: the AVX
+// one and ksw_extd2_singletrack_sse with its 16-byte blocks and end rules); it shares
+// the strip kernel's scoring restrictions (no z-drop or max tracking: with mat <= 0
 // every H is <= 0, so ez->max stays 0 and max_t/max_q stay -1).
 static bool band_path_ok(const Params &P, int qlen, int tlen) {
     if (exact_stop_enabled()) return false;
     const int allowed = AW_EZ_SCORE_ONLY | AW_EZ_RIGHT | AW_EZ_GENERIC_SC | AW_EZ_REV_CIGAR |
-                        AW_EZ_SEMIGLOBAL_END | AW_EZ_SINGLETRACK;
+                        AW_EZ_SEMIGLOBAL_END | AW_EZ_SINGLETRACK | AW_EZ_SSE_SINGLETRACK;
     if (P.flag & ~allowed) return false;
     if (P.zdrop >= 0) return false;
     if (P.max_sc > 0 || P.mat[0] < P.max_sc) return false;
@@ -497,8 +498,10 @@ static int plan_build(aw_ksw_plan_t *pl, int n, const int *qlen, const int *tlen
     }
     if (!pl->band_ids.empty()) {
         std::vector<int32_t> refused;
-        if (band_plan_build(pl->band, pl->band_ids, pl->qlen, pl->tlen, pl->w, pl->pairs, P.flag, exact_block(),
-                            budget, band_columns(pl), &refused)) {
+        // ksw_extd2_singletrack_sse works on 16-byte blocks whatever the build's width
+        const bool sse_st = (P.flag & AW_EZ_SINGLETRACK) && (P.flag & AW_EZ_SSE_SINGLETRACK);
+        if (band_plan_build(pl->band, pl->band_ids, pl->qlen, pl->tlen, pl->w, pl->pairs, P.flag,
+                            sse_st ? 16 : exact_block(), budget, band_columns(pl), &refused)) {
             set_error("pair traceback exceeds the HBM traceback budget");
             return AW_E_NOMEM;
         }
@@ -949,6 +952,16 @@ int aw_ksw_plan_stats(const aw_ksw_plan_t *pl, int64_t *cells, int64_t *tb_bytes
     if (tb_bytes) *tb_bytes = pl->tb_total;
     if (waves) *waves = (int)pl->waves.size();
     if (launches) *launches = pl->launches;
+    return AW_OK;
+}
+
+int aw_ksw_plan_routes(const aw_ksw_plan_t *pl, int *strip_pairs, int *banded_pairs, int *exact_pairs) {
+    if (!pl) return AW_E_INVAL;
+    int n[4] = {0, 0, 0, 0};
+    for (int r : pl->route) ++n[r];
+    if (strip_pairs) *strip_pairs = n[1];
+    if (banded_pairs) *banded_pairs = n[3];
+    if (exact_pairs) *exact_pairs = n[2];
     return AW_OK;
 }
 

@@ -46,7 +46,6 @@ namespace aw {
 
 namespace {
 
-constexpr int C = KSW_COLS;
 constexpr unsigned FULL = 0xffffffffu;
 
 struct Geom {
@@ -117,11 +116,14 @@ __device__ __forceinline__ void cell(int s, int &xs, int &vs, int &x2s, int &ut,
     vs = vn;
 }
 
+// The Singletrack tracks (v, u) instead of the state bytes: the Singletrack entries of
+// the AVX builds (blocks of 32 or 64 bytes), and ksw_extd2_singletrack_sse (16-byte blocks).
+bool singletrack_tracks(int flag, int block) {
+    return (flag & AW_EZ_SINGLETRACK) && (block > 16 || (flag & AW_EZ_SSE_SINGLETRACK));
+}
+
 __device__ __forceinline__ unsigned long long end_key(int v, int pos) {
     return ((unsigned long long)((uint32_t)v ^ 0x80000000u) << 32) | (uint32_t)pos;
-}
-__device__ __forceinline__ void best_merge(int &v, int &p, int ov, int op) {
-    if (ov > v || (ov == v && op > p)) v = ov, p = op;
 }
 
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -142,6 +144,9 @@ struct BandArgs {
     BandRes *res;
     KswScore sc;
     int block, generic;
+    // ksw_extd2_singletrack_sse's end rules: strict ">" for mqe/mte (the earliest position
+    // wins a tie; minimap2/ksw2_singletrack.cpp:583-586)
+    int sse_st;
     int store_ckpt;  // 1: store the traceback of recomputed pairs too (their group passes)
     const unsigned long long *deadline;  // null: no deadline
     // recompute rounds: the pairs' walk states; a round's strips stop at the row the walk has
@@ -431,9 +436,11 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
                             if (inBand) {
                                 H[c] = hn;
                                 // end tracking straight into the pair's record (rare cells; the
-                                // packed keys make the ">=" later-wins rule an unsigned max)
-                                if (re && t == tm1) atomicMax(&R->mte_key, end_key(hn, j));
-                                if (j == qm1) atomicMax(&R->mqe_key, end_key(hn, t));
+                                // packed keys make the ">=" later-wins rule an unsigned max, and
+                                // the strict earlier-wins rule one on the mirrored position)
+                                const int pm = A.sse_st ? INT_MAX : 0;
+                                if (re && t == tm1) atomicMax(&R->mte_key, end_key(hn, pm ^ j));
+                                if (j == qm1) atomicMax(&R->mqe_key, end_key(hn, pm ^ t));
                                 if (j == qm1 && t == tm1) R->score = hn, R->has_score = 1;
                             }
                             if (ARGMAX) {
@@ -580,9 +587,13 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
     o.max = 0, o.max_q = -1, o.max_t = -1, o.reach_end = 0, o.stopped = 0, o.n_cigar = 0;
     o.score = R.has_score ? R.score : AW_NEG_INF;
     o.mqe = R.mqe_key ? (int)((uint32_t)(R.mqe_key >> 32) ^ 0x80000000u) : AW_NEG_INF;
-    o.mqe_t = R.mqe_key ? (int)(uint32_t)R.mqe_key : -1;
+    // ksw_extd2_singletrack_sse: positions stored mirrored (its strict ">"), and
+    // mte_q = r - en with en rounded up to its 16-byte block (minimap2/ksw2_singletrack.cpp:583-586)
+    const bool sse_st = (flag & AW_EZ_SINGLETRACK) && (flag & AW_EZ_SSE_SINGLETRACK);
+    const int pm = sse_st ? INT_MAX : 0;
+    o.mqe_t = R.mqe_key ? pm ^ (int)(uint32_t)R.mqe_key : -1;
     o.mte = R.mte_key ? (int)((uint32_t)(R.mte_key >> 32) ^ 0x80000000u) : AW_NEG_INF;
-    o.mte_q = R.mte_key ? (int)(uint32_t)R.mte_key : -1;
+    o.mte_q = R.mte_key ? (pm ^ (int)(uint32_t)R.mte_key) - (sse_st ? ((tlen + 15) & ~15) - tlen : 0) : -1;
     o.zdropped = P.rb < g.nd ? 1 : 0;
     if (R.stopped) {
         // stopped at the deadline: no score and no traceback (ksw2_extd2_sse.c:136-139, :400-409)
@@ -612,7 +623,9 @@ __global__ void __launch_bounds__(32 * FIN_WARPS) ksw_band_finish_kernel(BtArgs 
     auto en16 = [&](int r) { return (g.en0(r) & ~15) + 15; };
     WarpCig cg{A.cig + P.cig_off, 0, 0, 0};
     if (cigar && ST) {
-        if (!o.zdropped && !(flag & (AW_EZ_EXTZ_ONLY | AW_EZ_SEMIGLOBAL_END))) {
+        // ksw_extd2_singletrack_sse reconstructs whatever the EXTZ/SEMIGLOBAL flags
+        // (minimap2/ksw2_singletrack.cpp:606-615)
+        if (!o.zdropped && (sse_st || !(flag & (AW_EZ_EXTZ_ONLY | AW_EZ_SEMIGLOBAL_END)))) {
             const uint8_t *qs = A.qcodes + P.qoff, *ts = A.tcodes + P.toff;
             const int o1 = -A.sc.q, g1 = -A.sc.e, o2 = -A.sc.q2, g2 = -A.sc.e2;
             // track value (0 = v, 1 = u), the matrix-edge difference, or NEG_INF outside the stored band
@@ -774,7 +787,7 @@ void *kernel_ptr() {
 
 void *band_kernel_for(int flag, int block) {
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY), right = !!(flag & AW_EZ_RIGHT);
-    const bool st = cigar && block > 16 && (flag & AW_EZ_SINGLETRACK);
+    const bool st = cigar && singletrack_tracks(flag, block);
     if (st) return kernel_ptr<true, false, true>();
     if (cigar && right) return kernel_ptr<true, true, false>();
     if (cigar) return kernel_ptr<true, false, false>();
@@ -829,7 +842,7 @@ int band_plan_build(BandPlan &bp, const std::vector<int32_t> &ids, const std::ve
     bp.nc = nc == 4 ? 4 : 8;
     const int SW = 32 * bp.nc;  // strip width
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY);
-    const bool st = cigar && block > 16 && (flag & AW_EZ_SINGLETRACK);
+    const bool st = cigar && singletrack_tracks(flag, block);
     const int CB = st ? 2 * bp.nc : bp.nc;  // traceback bytes per lane-step
     const int B = block;
     struct PairGeo {
@@ -1098,6 +1111,7 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
     a.sc = S;
     a.block = bp.block;
     a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
+    a.sse_st = (flag & AW_EZ_SINGLETRACK) && (flag & AW_EZ_SSE_SINGLETRACK) ? 1 : 0;
     a.store_ckpt = 0;
     a.deadline = D.deadline;
     a.walk = nullptr;
@@ -1106,7 +1120,7 @@ cudaError_t band_launch_dp(const BandPlan &bp, int k, const BandDev &D, const ui
 
 cudaError_t band_launch_units(const BandPlan &bp, const BandArgs &a, int flag, int ctas, cudaStream_t st) {
     const bool cigar = !(flag & AW_EZ_SCORE_ONLY), right = !!(flag & AW_EZ_RIGHT);
-    const bool stk = cigar && bp.block > 16 && (flag & AW_EZ_SINGLETRACK);
+    const bool stk = cigar && singletrack_tracks(flag, bp.block);
     const int grid = std::max(1, std::min(ctas, (a.n_units + 7) / 8));
 #define AW_BAND_LAUNCH(NCV)                                                                   \
     if (stk) ksw_band_kernel<true, false, true, NCV><<<grid, 256, 0, st>>>(a);               \
@@ -1134,7 +1148,7 @@ cudaError_t band_launch_finish(const BandPlan &bp, int k, const BandDev &D, cons
     memcpy(b.mat, mat, (size_t)m * m);
     b.m = m, b.flag = flag, b.block = bp.block;
     const int grid = (W.npair + FIN_WARPS - 1) / FIN_WARPS;
-    const bool stk = b.block > 16 && (flag & AW_EZ_SINGLETRACK) && !(flag & AW_EZ_SCORE_ONLY);
+    const bool stk = singletrack_tracks(flag, b.block) && !(flag & AW_EZ_SCORE_ONLY);
     if (bp.nc == 4) {
         if (stk) ksw_band_finish_kernel<true, 4><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
         else ksw_band_finish_kernel<false, 4><<<grid, 32 * FIN_WARPS, 0, st>>>(b);
@@ -1173,6 +1187,7 @@ cudaError_t band_launch_groups(const BandPlan &bp, int k, const BandDev &D, cons
         a.sc = S;
         a.block = bp.block;
         a.generic = (flag & AW_EZ_GENERIC_SC) ? 1 : 0;
+        a.sse_st = (flag & AW_EZ_SINGLETRACK) && (flag & AW_EZ_SSE_SINGLETRACK) ? 1 : 0;
         a.store_ckpt = 1;
         a.deadline = D.deadline;
         a.walk = D.walk;

@@ -664,7 +664,7 @@ __device__ __forceinline__ int64_t pig_slot(int c, int sc, int SR, int R1, int R
 template <bool L2>
 __device__ __forceinline__ void plan_compute(const WfaArgs &A, const WfaPairDev &PR, const uint8_t *pat,
                                              const uint8_t *txt, const WidePlan &Q, int g0, int G, WidePart &pp) {
-    const int plen = PR.plen, tlen = PR.tlen, k_end = tlen - plen, lane = threadIdx.x & 31;
+    const int plen = PR.plen, tlen = PR.tlen, k_end = tlen - plen;
     const int lo = Q.lo, hi = Q.hi, mask = Q.mask;
     const InHdr m_misms = in_hdr(A, Q.in[0]), m_open1 = in_hdr(A, Q.in[1]), i1 = in_hdr(A, Q.in[2]),
                 d1 = in_hdr(A, Q.in[3]), m_open2 = in_hdr(A, Q.in[4]), i2 = in_hdr(A, Q.in[5]),
@@ -1300,7 +1300,6 @@ __global__ void __launch_bounds__(128, AW_WFA_MINB) wfa_kernel(WfaArgs A, int rs
 // diagonals differs, so the results are identical.  Offsets written by other CTAs are read
 // through L2 (ld.global.cg), after the barrier's release/acquire.
 constexpr int WIDE_NT = 384;
-constexpr int WIDE_U = 4;
 constexpr int WIDE_CHUNKS = 8;  // reserve chunks a planner keeps track of (a ring)
 
 // A reserve chunk announced by the leader: for pair `tag`, the planners' chunk number `seq`
@@ -1515,7 +1514,6 @@ __global__ void __launch_bounds__(WIDE_NT, 1) wfa_wide_kernel(WfaArgs A, int rs)
         if (op == WOP_EXIT) break;
         const int pidx = pstart[(np - 1) & 1].seq;
         const WfaPairDev PR = A.pairs[pidx];
-        const int plen = PR.plen, tlen = PR.tlen, k_end = tlen - plen;
         const uint8_t *pat = A.pat + PR.poff, *txt = A.txt + PR.toff;
         while (op == WOP_COMPUTE) {
             // ---- 1. this thread's diagonals of the planned score

@@ -228,6 +228,13 @@ class KswPlan:
               "aw_ksw_plan_stats")
         return {"cells": cells.value, "tb_bytes": tb.value, "waves": waves.value, "launches": launches.value}
 
+    def routes(self):
+        """Pairs per kernel: {"strip": full-matrix strip kernel, "banded": banded strip kernel,
+        "exact": exact anti-diagonal kernel}."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(lib.aw_ksw_plan_routes(self.h, C.byref(a), C.byref(b), C.byref(c)), "aw_ksw_plan_routes")
+        return {"strip": a.value, "banded": b.value, "exact": c.value}
+
     def close(self):
         if self.h:
             lib.aw_ksw_plan_free(self.h)

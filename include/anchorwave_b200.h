@@ -112,6 +112,11 @@ int aw_ksw_plan_download(aw_ksw_plan_t *plan, ksw_extz_t *ez);
 /* Device-side statistics of the plan: cells, traceback bytes, waves, launches. */
 int aw_ksw_plan_stats(const aw_ksw_plan_t *plan, int64_t *cells, int64_t *tb_bytes, int *waves,
                       int *launches_per_execute);
+/* How the plan routes its pairs: the full-matrix strip kernel, the banded strip kernel
+ * (banded calls, Singletrack calls of either entry, long full-width pairs) and the exact
+ * anti-diagonal kernel (z-drop, approximate max, extension-only, parameters beyond the
+ * strip kernels' magnitude bound).  Pairs with no device work count in none. */
+int aw_ksw_plan_routes(const aw_ksw_plan_t *plan, int *strip_pairs, int *banded_pairs, int *exact_pairs);
 /* CUDA-event times (ms) of the last execute, summed over waves: the DP phase (the
  * concurrent strip-kernel launches) and the traceback phase (backtrack kernel). */
 int aw_ksw_plan_timing(const aw_ksw_plan_t *plan, float *dp_ms, float *bt_ms);

@@ -60,3 +60,48 @@ def test_sse_singletrack_vs_reference_and_batch(gpu):
                                flag=oracle.KSW_EZ_SINGLETRACK | 0x4000)
     for q, t, w, b in zip(qs, ts, ws, got):
         assert b.key() == ksw2.ksw_extd2_singletrack_sse(q, t, mat, *PEN[0], w=w).key()
+
+
+def _band_cases(seed, n):
+    """Pairs of 300 bp-12 kb that take the banded strip kernel: no z-drop, every flag it
+    serves, bands from empty-before-the-end to full width, and low-complexity pairs."""
+    rng = np.random.default_rng(seed)
+    flags = [0, oracle.KSW_EZ_SEMIGLOBAL_END, oracle.KSW_EZ_SCORE_ONLY, oracle.KSW_EZ_REV_CIGAR,
+             oracle.KSW_EZ_RIGHT | oracle.KSW_EZ_GENERIC_SC,
+             oracle.KSW_EZ_SEMIGLOBAL_END | oracle.KSW_EZ_SCORE_ONLY]
+    out = []
+    for it in range(n):
+        L = int(np.exp(rng.uniform(np.log(300), np.log(12000))))
+        if it % 5 == 4:
+            unit = W.random_dna(rng, int(rng.integers(1, 5)))
+            t = np.tile(unit, L // len(unit) + 1)[:L]
+            q = t[: max(1, L - int(rng.integers(0, 40)))].copy()
+        else:
+            q, t = W.divergent_pair(rng, L, 0.01, 0.2, 4.0)
+        w = [-1, L // 10, L // 3, 0, 7][it % 5]
+        out.append((q, t, flags[it % len(flags)], w, PEN[it % 2]))
+    return out
+
+
+def test_sse_singletrack_banded_kernel_vs_oracle(gpu, restatement):
+    """The SSE Singletrack entry's pairs run on the banded strip kernel (16-byte blocks, the
+    strict end rules, reconstruction whatever the flags): identical to the restatement."""
+    from anchorwave_b200 import ksw2
+    mat = oracle.anchorwave_matrix(-4)
+    cases = _band_cases(21, 36)
+    for flag in sorted({c[2] for c in cases}):
+        for pen in PEN[:2]:
+            sub = [c for c in cases if c[2] == flag and c[4] == pen]
+            if not sub:
+                continue
+            plan = ksw2.KswPlan([c[0] for c in sub], [c[1] for c in sub], mat, *pen,
+                                w=[c[3] for c in sub], flag=flag | oracle.KSW_EZ_SINGLETRACK | 0x4000)
+            assert plan.routes()["exact"] == 0, (hex(flag), plan.routes())
+            plan.upload()
+            plan.execute()
+            got = plan.download()
+            plan.close()
+            for (q, t, _, w, _), g in zip(sub, got):
+                o = restatement.ksw_extd2(q.tobytes(), t.tobytes(), mat, *pen, w=w,
+                                          flag=flag | oracle.KSW_EZ_SINGLETRACK, block=16)
+                assert g.key() == o.key(), (len(q), len(t), w, hex(flag), pen)
