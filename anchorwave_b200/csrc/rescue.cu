@@ -23,6 +23,8 @@
 namespace {
 
 constexpr int kCompleted = 0, kTimeLimit = 1, kNotCertified = 2, kFailed = 3;  // Ksw2CertifiedStatus
+// band cells an interval's run-ahead round may take (several narrow bands of a long interval)
+constexpr double kAheadCells = 4e9;
 
 // encodeKswSequence (alignSlidingWindow.cpp:645-660)
 int encode(const std::string &s, std::vector<uint8_t> &out) {
@@ -263,17 +265,36 @@ int aw_align_score_certified_batch(int n, const char *const *query, const int64_
             r.fallback = requested < std::min(max_band, doubled) ? requested : -1;
             r.active = true;
         }
-        for (size_t step = 0; rc == AW_OK; ++step) {
+        // Untimed calls run ahead: a round takes an interval's next bands while their band
+        // cells stay within kAheadCells together (always at least one band) and folds the
+        // results in band order, dropping those after the certifying one, so every interval
+        // ends in the state the band-by-band loop reaches.  A long interval at narrow bands is
+        // bound by its strip chain, not by its cells, so the bands taken together cost about
+        // one round.  Timed calls keep one band per round (the deadline then stops the same
+        // attempts as the reference's loop would reach).
+        std::vector<size_t> next(n, 0);
+        while (rc == AW_OK) {
             std::vector<Job> jobs;
-            for (int i : todo)
-                if (C[i].active && !C[i].done && step < C[i].bands.size())
-                    jobs.push_back(Job{i, Q[i], D[i], (int)C[i].bands[step]});
+            for (int i : todo) {
+                const Cert &r = C[i];
+                if (!r.active || r.done) continue;
+                double cells = 0.0;
+                for (size_t b = next[i]; b < r.bands.size(); ++b) {
+                    const double c = (double)std::max(qlen[i], rlen[i]) * (2.0 * (double)r.bands[b] + 1.0);
+                    if (b > next[i] && (timed || cells + c > kAheadCells)) break;
+                    cells += c;
+                    jobs.push_back(Job{i, Q[i], D[i], (int)r.bands[b]});
+                }
+            }
             if (jobs.empty()) break;
             std::vector<ksw_extz_t> res;
             rc = run_round(jobs, mis, o1, e1, o2, e2, 0, res);
             if (rc == AW_OK)
-                for (size_t k = 0; k < jobs.size(); ++k)
-                    take_band(C[jobs[k].id], res[k], Q[jobs[k].id], D[jobs[k].id], jobs[k].band, mis, o1, e1, o2, e2);
+                for (size_t k = 0; k < jobs.size(); ++k) {
+                    const int i = jobs[k].id;
+                    ++next[i];
+                    if (!C[i].done) take_band(C[i], res[k], Q[i], D[i], jobs[k].band, mis, o1, e1, o2, e2);
+                }
             free_ez(res);
         }
         if (rc == AW_OK) {

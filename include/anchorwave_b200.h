@@ -155,7 +155,9 @@ typedef struct {
  * intervals at once, called from the executor at :1835: the unbanded score-only optimum of
  * every interval in one batch, then round by round the next band of every interval not yet
  * certified in one banded batch, until its re-scored alignment reaches the optimum; the
- * skipped smallest band runs only on failure.  Every interval gets the result a call of its
+ * skipped smallest band runs only on failure.  Untimed calls let a round take an interval's
+ * next few bands (up to 4e9 band cells together) and fold their results in band order, so
+ * the narrow bands of a long interval, each bound by its strip chain, cost one round.  Every interval gets the result a call of its
  * own would give (the selector's chained traceback, used when a selection plan is passed,
  * stays with the caller).  Sequences are ASCII; initial_band_width / maximum_band_width hold
  * interval i's bands (the selection plan's ksw2CertifiedInitialBandWidth and
