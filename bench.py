@@ -388,15 +388,16 @@ def serving_measurement(nreq: int, rank: int, tuning=None, plain_sample: int = 4
     rng = np.random.default_rng(2024)
     sample = sorted(rng.choice(len(reqs), size=min(plain_sample, len(reqs)), replace=False).tolist())
     # the autotuner picks the worker slots and the micro-batch size for the lowest p99 at 80% of
-    # the saturated rate of the default setting, on a 3,000-request sample of the trace
+    # the saturated rate of the default setting, each setting serving the whole trace
     from anchorwave_b200 import autotune
     dt0, _, _ = run(None)
     log(f"default setting saturated: {dt0:.1f} s")
     t_tune = time.perf_counter()
     (cfg["slots"], cfg["max_batch"]), trials = autotune.tune_serving(
-        reqs, routes, mat, 4, 2, 24, 1, rate=SERVE_LOAD * len(reqs) / dt0, sample=3000, hbm_budget=SERVE_HBM_BUDGET)
+        reqs, routes, mat, 4, 2, 24, 1, rate=SERVE_LOAD * len(reqs) / dt0, sample=len(reqs),
+        hbm_budget=SERVE_HBM_BUDGET)
     if tuning is not None:
-        tuning["serving"] = {"slots": cfg["slots"], "max_batch": cfg["max_batch"], "sample_requests": 3000,
+        tuning["serving"] = {"slots": cfg["slots"], "max_batch": cfg["max_batch"], "sample_requests": len(reqs),
                              "seconds": time.perf_counter() - t_tune,
                              "trials": [{k: (round(v, 1) if isinstance(v, float) else v) for k, v in t.items()}
                                         for t in trials]}
