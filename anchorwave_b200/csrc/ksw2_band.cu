@@ -155,6 +155,10 @@ struct BandArgs {
 };
 
 constexpr uint64_t WAIT_NS = 20ull * 1000 * 1000 * 1000;  // bounded wait on the left strip
+// rows per publication of a strip's boundary column: the strip on the right starts a row once
+// the PUB rows from it are published (lane 31 finishes row j 31 steps after lane 0), so a hop
+// between strips costs strip width + 31 + PUB lane-steps
+constexpr int PUB = 8;
 
 // NC target columns per lane (strips of 32*NC columns): 8 for throughput, 4 for a shorter
 // pipeline lag between strips when few long pairs run.
@@ -236,6 +240,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
         uint32_t carry = 0, qchunk = 0;
         int Hcarry = AW_NEG_INF;
         uint2 bchunk = make_uint2(init_pack, (uint32_t)AW_NEG_INF);
+        int seen = INT_MIN;  // lane 0: the left strip's progress count last read
         bool failed = false;
         const int nsteps = jend - jstart + 32;
         for (int k = 0; k < nsteps; ++k) {
@@ -252,35 +257,40 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
             if ((k & 31) == 0) {
                 const int J = jstart + k, jr = J + lane;
                 qchunk = (jr >= 0 && jr < qlen) ? qs[jr] : 0u;
-                if (prog_prod) {
-                    // rows J..J+31 of the left strip: published rows, or (past its last
-                    // row) its final H with the initial x/v/x2
-                    const int need = J + 31 > prod_hi ? prod_hi + 2 : J + 32;
-                    if (J + 31 >= prod_lo && lane == 0) {
-                        // one poller per warp with back-off; the bound and the error flag
-                        // (another warp gave up) are checked every 32 polls
-                        cuda::atomic_ref<int32_t, cuda::thread_scope_device> pr(*prog_prod);
-                        if (pr.load(cuda::memory_order_acquire) < need) {
-                            const uint64_t t0 = globaltimer();
-                            unsigned ns = 32, polls = 0;
-                            while (pr.load(cuda::memory_order_acquire) < need) {
-                                __nanosleep(ns);
-                                ns = ns < 1024 ? ns * 2 : ns;
-                                if (A.deadline && *stop_word) break;  // the left strip stopped
-                                if ((++polls & 31) == 0 &&
-                                    (globaltimer() - t0 > WAIT_NS || *(volatile int32_t *)A.error)) {
-                                    failed = true;
-                                    break;
-                                }
+            }
+            if (prog_prod && (k & (PUB - 1)) == 0) {
+                // rows J..J+PUB-1 of the left strip (published rows, or past its last row its
+                // final H with the initial x/v/x2), loaded by the lanes that hold them in the
+                // 32-row chunk the step shuffles from (lane L holds row jstart + (k & ~31) + L)
+                const int J = jstart + k, jr = jstart + (k & ~31) + lane;
+                const int need = J + PUB - 1 > prod_hi ? prod_hi + 2 : J + PUB;
+                if (J + PUB - 1 >= prod_lo && lane == 0 && seen < need) {
+                    // one poller per warp with back-off; the bound and the error flag
+                    // (another warp gave up) are checked every 32 polls
+                    cuda::atomic_ref<int32_t, cuda::thread_scope_device> pr(*prog_prod);
+                    seen = pr.load(cuda::memory_order_acquire);
+                    if (seen < need) {
+                        const uint64_t t0 = globaltimer();
+                        unsigned ns = 32, polls = 0;
+                        while ((seen = pr.load(cuda::memory_order_acquire)) < need) {
+                            __nanosleep(ns);
+                            ns = ns < 1024 ? ns * 2 : ns;
+                            if (A.deadline && *stop_word) break;  // the left strip stopped
+                            if ((++polls & 31) == 0 &&
+                                (globaltimer() - t0 > WAIT_NS || *(volatile int32_t *)A.error)) {
+                                failed = true;
+                                break;
                             }
                         }
                     }
-                    failed = __shfl_sync(FULL, failed, 0);
-                    if (failed) {
-                        if (lane == 0) atomicExch(A.error, 1);
-                        break;
-                    }
-                    if (A.deadline && __shfl_sync(FULL, lane == 0 ? *stop_word : 0, 0)) break;
+                }
+                failed = __shfl_sync(FULL, failed, 0);
+                if (failed) {
+                    if (lane == 0) atomicExch(A.error, 1);
+                    break;
+                }
+                if (A.deadline && __shfl_sync(FULL, lane == 0 ? *stop_word : 0, 0)) break;
+                if ((lane & ~(PUB - 1)) == (k & 31)) {
                     if (jr >= prod_lo && jr <= prod_hi) bchunk = __ldcg(bnd_prod + (jr - prod_lo));
                     else if (jr > prod_hi) bchunk = make_uint2(init_pack, __ldcg(bnd_prod + (prod_hi - prod_lo + 1)).y);
                     else bchunk = make_uint2(init_pack, (uint32_t)AW_NEG_INF);
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(256, 2) ksw_band_kernel(BandArgs A) {
             }
             if (lane == 31 && !last_strip) {
                 const int jj = jstart + k - 31;
-                if (jj >= jlo && jj <= jend && (((jj - jlo) & 31) == 31 || jj == jend)) {
+                if (jj >= jlo && jj <= jend && (((jj - jlo) & (PUB - 1)) == PUB - 1 || jj == jend)) {
                     if (jj == jend) bnd_me[jend - jlo + 1] = make_uint2(init_pack, (uint32_t)Hcarry);
                     // the release store orders this lane's boundary writes before the count
                     cuda::atomic_ref<int32_t, cuda::thread_scope_device> pw(*prog_me);
