@@ -48,7 +48,7 @@ std::atomic<int> g_wide_width{8192};
 std::atomic<int> g_wide_tail{1024};
 std::atomic<int> g_wide_cluster{8};
 // Pairs with pattern + text length from which a pair runs on a whole CTA (aw_set_wfa_long).
-std::atomic<int> g_long_sum{3072};
+std::atomic<int> g_long_sum{1536};
 
 }  // namespace
 

@@ -544,7 +544,7 @@ def wfa_long_measurement(npairs: int, rank: int, cpu: bool):
             try:
                 _, ms1 = al.align_batch([p_], [t_])
             finally:
-                wfa.set_long(3072)
+                wfa.set_long(1536)
                 wfa.set_wide(8192, 1024, 8)
             rec["one_warp_device_ms"] = ms1
         al.close()

@@ -250,7 +250,7 @@ void aw_set_wfa_wide(int width, int tail_width, int cluster_ctas);
 /* High memory: pairs whose pattern and text lengths sum to at least `min_length_sum` run
  * first, each on all four warps of a CTA (the longest pairs of a batch otherwise set its
  * duration, one warp each); the others then run one per warp.  0: every pair starts on one
- * warp.  Default 3072.  A CTA's pair moves to the cluster kernel by the widths of
+ * warp.  Default 1536.  A CTA's pair moves to the cluster kernel by the widths of
  * aw_set_wfa_wide, as a warp's does.  Results are identical.  Process-wide. */
 void aw_set_wfa_long(int min_length_sum);
 /* Kernel launches of the last call (every round and phase) and, of them, the cluster

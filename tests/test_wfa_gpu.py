@@ -341,7 +341,7 @@ def test_wfa_long_pairs_on_whole_ctas(gpu, reference, singletrack, memory_mode):
             got, _ = al.align_batch(ps, ts)
             assert got == warp, (long_sum, width)
     finally:
-        wfa.set_long(3072)
+        wfa.set_long(1536)
         wfa.set_wide(8192, 1024, 8)
         al.close()
     for i in range(0, 48, 4):
